@@ -1,0 +1,448 @@
+"""Benchmark of the adaptive SpMV / SpMSpV engine on B200.
+
+Workload (one "step"): the 1,048,576 x 1,048,576 Zipf-row matrix (nnz
+16,777,216, row lengths Zipf(1.5) scaled to mean 16, values U(-1,1), seed 2)
+multiplied by a sparse x at each density of the sweep 1e-5, 1e-4, 1e-3, 1e-2,
+1e-1, 1.0 (positions uniform without replacement, values U(-1,1)); each call
+goes through the adaptive engine (selector + chosen kernel).  Synthetic data
+of the benchmark's shape: no dataset is involved.
+
+Metric: effective GB/s = compulsory bytes of the cheapest formulation of each
+call (min of the CSC SpMSpV traffic 16*x_nnz + 8*bin_len + 4*m and the SpMV
+traffic 4(m+1) + 8*nnz + 4n + 4m), summed over the sweep, divided by the summed
+device time.  `value` has inputs resident in HBM; `e2e` adds, per call, the
+host->device copy of x (pinned) and the device->host copy of y.
+
+--impl reference times the reference's CPU path (its serial routines,
+restated in the oracle and parallelised with OpenMP over all host threads)
+on the same sweep.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(ROOT, "spmspv-adaptive_b200")
+for _p in (ROOT, PKG):
+    if _p not in sys.path:
+        sys.path.insert(0, _p)
+
+import numpy as np  # noqa: E402
+
+METRIC = "SpMSpV/SpMV effective HBM GB/s vs x density; batched BFS GTEPS vs plain"
+WORKLOAD = ("zipf-1M density sweep: 1,048,576^2 CSR+CSC, nnz 16,777,216, Zipf(1.5) rows "
+            "(mean 16, cap 10,000), x density 1e-5..1.0, adaptive kernel per call")
+DENSITIES = (1e-5, 1e-4, 1e-3, 1e-2, 1e-1, 1.0)
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def eff_bytes(m, n, nnz, x_nnz, bin_len):
+    csc = 16 * x_nnz + 8 * bin_len + 4 * m
+    spmv = 4 * (m + 1) + 8 * nnz + 4 * n + 4 * m
+    return min(csc, spmv)
+
+
+def spmv_bytes(m, n, nnz):
+    return 4 * (m + 1) + 8 * nnz + 4 * n + 4 * m
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_{os.getpid()}.csv")
+
+    def __enter__(self):
+        try:
+            os.makedirs(os.path.dirname(self.path), exist_ok=True)
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index),
+                 "--query-gpu=clocks.sm,clocks.max.sm,clocks_event_reasons.active,"
+                 "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=self.f, stderr=subprocess.DEVNULL)
+            time.sleep(0.3)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            time.sleep(0.25)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+            self.f.close()
+
+    def summary(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
+        rows = []
+        with open(self.path) as f:
+            for ln in f:
+                parts = [p.strip() for p in ln.split(",")]
+                if len(parts) >= 7:
+                    rows.append(parts)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = [float(r[0]) for r in rows if r[0].replace(".", "").isdigit()]
+        mx = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[3 + i] == "Active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
+                "samples": len(rows)}
+
+
+def dist_init(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        backend = "gloo" if args.impl == "reference" else "nccl"
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
+    return world, rank, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def allmax(v, world):
+    if world == 1:
+        return v
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([v], dtype=torch.float64,
+                     device="cuda" if dist.get_backend() == "nccl" else "cpu")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def make_inputs():
+    from spmx import gen
+    A = gen.zipf_1m(seed=2)
+    xs = []
+    for d in DENSITIES:
+        k = gen.density_nnz(A.n, d)
+        key, val = gen.sparse_vector(A.n, k, dist="uniform", seed=1000 + k)
+        xs.append((d, key, val))
+    return A, xs
+
+
+# ---------------------------------------------------------------------------
+# reference arm: the reference's CPU routines on all host threads
+# ---------------------------------------------------------------------------
+def run_reference(args, world, rank):
+    if rank != 0:
+        return 0
+    import oracle.oracle as orc
+    A, xs = make_inputs()
+    colptr, row, cval = A.to_csc()
+    threads = orc.raw.cpu_threads()
+    m, n, nnz = A.m, A.n, A.nnz
+    y = np.zeros(m, np.float32)
+    P = lambda a: a.ctypes.data  # noqa: E731
+    binl = [int(orc.vec_features(colptr, key)[0]) for _, key, _ in xs]
+    tot_bytes = sum(eff_bytes(m, n, nnz, len(k), b) for (_, k, _), b in zip(xs, binl))
+    dense = [orc.sparse2dense_bits(n, k, v)[0] for _, k, v in xs]
+
+    def step():
+        t = 0.0
+        for (d, key, val), xd in zip(xs, dense):
+            t0 = time.perf_counter()
+            if d >= 1.0:
+                orc.raw.cpu_spmv_omp(m, P(A.rowptr), P(A.col), P(A.val), P(xd), P(y), 1.0)
+            else:
+                orc.raw.cpu_spmspv_csc_omp(m, P(colptr), P(row), P(cval), len(key), P(key),
+                                           P(val), P(y))
+            t += time.perf_counter() - t0
+        return t
+
+    for _ in range(args.warmup):
+        step()
+    ts = [step() for _ in range(args.steps)]
+    sec = sum(ts) / len(ts)
+    gbs = tot_bytes / sec / 1e9
+    line = {"metric": METRIC, "value": gbs, "unit": "GB/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": sec * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic", "impl": "reference",
+            "config": {"workload": WORKLOAD, "parallelism": "replicas" if args.gpus > 1 else "single"},
+            "cpu_baseline": {"value": gbs, "unit": "GB/s", "cores": threads, "kind": "port",
+                             "sample": "the full 6-density sweep per step: SpmSpvCSCHost for "
+                                       "sparse x and serialspmv for dense x (oracle restatement, "
+                                       "OpenMP over all host threads)"},
+            "e2e": {"value": gbs, "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ---------------------------------------------------------------------------
+# our arm
+# ---------------------------------------------------------------------------
+def run_ours(args, world, rank, local):
+    import torch
+    import spmx
+    from spmx import abi
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    stream = torch.cuda.current_stream(dev)
+    A, xs = make_inputs()
+    m, n, nnz = A.m, A.n, A.nnz
+
+    def d(a):
+        return torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+
+    rp, cl, vl = d(A.rowptr), d(A.col), d(A.val)
+    h = spmx.SpmspvHandle(m, n, nnz, stream=stream)
+    h.InputCSR(nnz, rp, cl, vl)
+    h.ToCSC()
+    h.holaPreprocess()
+    h.allocPreBuffer()
+    xdense = torch.zeros(n, device=dev)
+    bits = torch.zeros((n + 31) // 32, dtype=torch.int32, device=dev)
+    h.set_x(xdense)
+    h.set_bitvector(bits, (n + 31) // 32)
+    y = torch.empty(m, device=dev)
+    dx = [(dd, d(k), d(v), len(k)) for dd, k, v in xs]
+    binl = []
+    for dd, kd, vd, k in dx:
+        h.set_sparse_x(kd, vd, k)
+        binl.append(h.computeBinlenVer2())
+    ebytes = [eff_bytes(m, n, nnz, k, b) for (_, _, _, k), b in zip(dx, binl)]
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)  # 256 MiB > L2
+
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+          for _ in dx]
+    chosen = [None] * len(dx)
+
+    def step(record):
+        times = []
+        for i, (dd, kd, vd, k) in enumerate(dx):
+            flush.fill_(float(i))
+            h.set_sparse_x(kd, vd, k)
+            s, e = ev[i]
+            s.record(stream)
+            chosen[i] = h.run_adaptive(1.0, y)
+            e.record(stream)
+        stream.synchronize()
+        return [ev[i][0].elapsed_time(ev[i][1]) for i in range(len(dx))]
+
+    for _ in range(max(args.warmup, 3)):
+        step(False)
+    h.check_device_error()
+    barrier(world)
+    torch.cuda.synchronize(dev)
+    per = np.zeros(len(dx))
+    l0 = abi.lib.spmx_launch_count()
+    with Clocks(local) as clk:
+        for _ in range(args.steps):
+            per += np.array(step(True))
+    launches = abi.lib.spmx_launch_count() - l0
+    torch.cuda.synchronize(dev)
+    barrier(world)
+    h.check_device_error()
+    per /= args.steps
+    step_ms = float(per.sum())
+    step_ms_max = allmax(step_ms, world)
+    total_bytes = float(sum(ebytes))
+    value = world * total_bytes / (step_ms_max * 1e-3) / 1e9
+
+    # --- roofline: the LB (Hola) SpMV on the dense x, the dominant call ---
+    h.set_sparse_x(dx[-1][1], dx[-1][2], dx[-1][3])
+    h.sparse2dense()
+    rs, re_ = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    kt = []
+    for it in range(args.warmup + args.steps):
+        flush.fill_(1.0)
+        rs.record(stream)
+        h.holaspmv(1.0, y)
+        re_.record(stream)
+        stream.synchronize()
+        if it >= args.warmup:
+            kt.append(rs.elapsed_time(re_))
+    k_ms = statistics.mean(kt)
+    sb = spmv_bytes(m, n, nnz)
+    peak, peak_kind = peaks()
+    achieved = sb / (k_ms * 1e-3) / 1e9
+    traffic = None
+    tp = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tp):
+        with open(tp) as f:
+            traffic = json.load(f).get("hola_spmv_zipf1m")
+
+    # --- e2e through the public API with host buffers ---
+    pin_k = [torch.from_numpy(np.ascontiguousarray(k)).pin_memory() for _, k, _ in xs]
+    pin_v = [torch.from_numpy(np.ascontiguousarray(v)).pin_memory() for _, _, v in xs]
+    kbuf = torch.empty(n, dtype=torch.int32, device=dev)
+    vbuf = torch.empty(n, dtype=torch.float32, device=dev)
+    yhost = torch.empty(m, dtype=torch.float32).pin_memory()
+    h2d = sum(8 * len(k) for _, k, _ in xs)
+    d2h = 4 * m * len(xs)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+    def e2e_step():
+        tot = 0.0
+        for i in range(len(xs)):
+            k = len(xs[i][1])
+            flush.fill_(2.0)
+            e0.record(stream)
+            kbuf[:k].copy_(pin_k[i], non_blocking=True)
+            vbuf[:k].copy_(pin_v[i], non_blocking=True)
+            h.set_sparse_x(kbuf, vbuf, k)
+            h.run_adaptive(1.0, y)
+            yhost.copy_(y, non_blocking=True)
+            e1.record(stream)
+            stream.synchronize()
+            tot += e0.elapsed_time(e1)
+        return tot
+
+    for _ in range(max(args.warmup, 3)):
+        e2e_step()
+    barrier(world)
+    e2e_ms = statistics.mean([e2e_step() for _ in range(args.steps)])
+    e2e_ms = allmax(e2e_ms, world)
+    e2e_val = world * total_bytes / (e2e_ms * 1e-3) / 1e9
+
+    # --- BFS on R-MAT scale 14 (plain), bit-exact check against the oracle ---
+    bfs = run_bfs_plain(torch, dev, stream, args) if rank == 0 and not args.no_bfs else None
+
+    line = None
+    if rank == 0:
+        cpu = cpu_baseline(A, xs, binl) if not args.no_cpu else None
+        sweep = [{"density": dd, "x_nnz": k, "bin_len": b, "kernel": abi.KERNEL_NAMES[c],
+                  "ms": float(t), "eff_gbs": eb / (t * 1e-3) / 1e9}
+                 for (dd, _, _, k), b, c, t, eb in zip(dx, binl, chosen, per, ebytes)]
+        line = {
+            "metric": METRIC, "value": value, "unit": "GB/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": step_ms_max,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic",
+            "config": {"workload": WORKLOAD, "l2": "flushed (256 MiB write) before every timed call",
+                       "parallelism": f"replicas x{world}" if world > 1 else "single"},
+            "roofline": {"bound": "hbm", "kernel": "hola (fixed-nnz-per-CTA) SpMV, dense x",
+                         "achieved": achieved, "peak": peak, "peak_kind": peak_kind,
+                         "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
+                         "bytes_per_launch": sb, "ms_per_launch": k_ms},
+            "e2e": {"value": e2e_val, "unit": "GB/s", "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms},
+            "gpu_launches": int(launches // max(args.steps, 1)),
+            "clocks": clk.summary(),
+            "sweep": sweep,
+            "cpu_baseline": cpu,
+            "bfs": bfs,
+        }
+        print(json.dumps(line), flush=True)
+    h.Destroy()
+    return 0
+
+
+def run_bfs_plain(torch, dev, stream, args):
+    import spmx
+    from spmx import gen
+    import oracle.oracle as orc
+    g = gen.rmat(14, 16, seed=1)
+    rp = torch.from_numpy(g.rowptr).to(dev)
+    cl = torch.from_numpy(g.col).to(dev)
+    h = spmx.SpmspvHandle(g.m, g.n, g.nnz, stream=stream)
+    h.InputCSR(g.nnz, rp, cl, None)
+    lv = torch.empty(g.n, dtype=torch.int32, device=dev)
+    s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    for _ in range(3):
+        h.bfs(0, lv)
+    ts = []
+    for _ in range(max(args.steps, 5)):
+        s.record(stream)
+        depth = h.bfs(0, lv)
+        e.record(stream)
+        stream.synchronize()
+        ts.append(s.elapsed_time(e))
+    ref, _ = orc.bfs_queue(g.n, g.rowptr, g.col, 0)
+    got = lv.cpu().numpy()
+    reached = ref >= 0
+    # Graph500 convention: undirected input edges inside the source's component
+    edges = int(np.diff(g.rowptr)[reached].sum()) // 2
+    ms = statistics.median(ts)
+    h.Destroy()
+    return {"graph": "rmat scale 14, edge factor 16, seed 1, source 0",
+            "ms": ms, "gteps": edges / (ms * 1e-3) / 1e9, "depth": depth,
+            "bit_exact": bool(np.array_equal(got, ref)), "edges": edges}
+
+
+def cpu_baseline(A, xs, binl):
+    """The reference's serial CPU routines (restated), one core, one sweep."""
+    import oracle.oracle as orc
+    colptr, row, cval = A.to_csc()
+    m, n, nnz = A.m, A.n, A.nnz
+    y = np.zeros(m, np.float32)
+    P = lambda a: a.ctypes.data  # noqa: E731
+    dense = [orc.sparse2dense_bits(n, k, v)[0] for _, k, v in xs]
+    best = None
+    for _ in range(3):
+        t = 0.0
+        for (d, key, val), xd in zip(xs, dense):
+            t0 = time.perf_counter()
+            if d >= 1.0:
+                orc.raw.cpu_spmv_serial(m, P(A.rowptr), P(A.col), P(A.val), P(xd), P(y), 1.0)
+            else:
+                orc.raw.cpu_spmspv_csc_serial(m, P(colptr), P(row), P(cval), len(key), P(key),
+                                              P(val), P(y))
+            t += time.perf_counter() - t0
+        best = t if best is None else min(best, t)
+    tot = sum(eff_bytes(m, n, nnz, len(k), b) for (_, k, _), b in zip(xs, binl))
+    return {"value": tot / best / 1e9, "unit": "GB/s", "cores": 1, "kind": "port",
+            "sample": "one full 6-density sweep (best of 3): SpmSpvCSCHost for sparse x, "
+                      "serialspmv for dense x, oracle restatement, single thread",
+            "ms": best * 1e3}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-bfs", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    world, rank, local = dist_init(args)
+    try:
+        if args.impl == "reference":
+            rc = run_reference(args, world, rank)
+        else:
+            rc = run_ours(args, world, rank, local)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+    return rc
+
+
+if __name__ == "__main__":
+    sys.exit(main())

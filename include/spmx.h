@@ -1,0 +1,313 @@
+/*
+ * spmx.h — C ABI of the B200-native adaptive SpMV / SpMSpV engine.
+ *
+ * Every entry point is `extern "C"`, takes plain pointers and sizes, returns an
+ * int status (SPMX_SUCCESS == 0) and never exits the process.  Pointers named
+ * d_* are device pointers; everything else is host memory.  Index type is
+ * int32, value type is float32 (the reference's SpmspvHandle<int, unsigned,
+ * float> instantiation).
+ *
+ * Each declaration names the reference interface it replaces, as a path inside
+ * hpc-research-2020/spmspv-adaptive, abbreviated:
+ *   H    = hice-spmspv/hice/la/include/spmspv/csc-spmspv/spmspv.h
+ *   DEV  = hice-spmspv/hice/la/include/spmspv/csc-spmspv/detail/device/
+ *   TEST = hice-spmspv/hice/la/test/
+ *
+ * Ownership follows the reference: CSR arrays and x buffers are caller-owned
+ * device memory; CSC built by spmx_to_csc, Hola / CSR5 tables and scratch are
+ * handle-owned.  Unlike the reference, a CSC passed with spmx_input_csc is
+ * borrowed and never freed by the handle (H:2870-2876 frees it regardless).
+ *
+ * Streams: all work of a handle is issued on one stream (spmx_set_stream,
+ * default: the legacy default stream).  Entry points do not synchronise unless
+ * a HOST output pointer (e.g. `int* ynnz`) is non-NULL; device-side counts are
+ * always also available through spmx_get_device_counts.
+ */
+#ifndef SPMX_H_
+#define SPMX_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes: the reference's SPMSPV_* values are kept (common.h:11-26) */
+#define SPMX_SUCCESS                   0
+#define SPMX_UNKNOWN_FORMAT           -1
+#define SPMX_UNSUPPORTED_CSR_SPMV     -2
+#define SPMX_UNSUPPORTED_VALUE_TYPE   -3
+#define SPMX_UNSUPPORTED_CSR_SPMSPV   -4
+#define SPMX_UNSUPPORTED_COO_SPMSPV   -5
+#define SPMX_FORMAT_ERR_HOLA_SPMV     -6
+#define SPMX_MAT_FORMAT_ERR          -13
+#define SPMX_VEC_FORMAT_ERR          -14
+/* additions */
+#define SPMX_ERR_INVALID_VALUE       -20  /* bad argument (size, NULL, range)   */
+#define SPMX_ERR_CUDA                -21  /* a CUDA runtime call failed          */
+#define SPMX_ERR_TIMEOUT             -22  /* a bounded device wait gave up       */
+#define SPMX_ERR_OOB                 -23  /* device bounds check tripped         */
+#define SPMX_ERR_ALLOC               -24  /* device allocation failed            */
+#define SPMX_ERR_NOT_READY           -25  /* missing input / preprocess step     */
+#define SPMX_ERR_NO_DEVICE           -26  /* no CUDA device visible              */
+
+/* ---- vector type codes, as in set_vector_type (H:979): 0 sparse, 1 dense, 2 bitarray */
+#define SPMX_VEC_SPARSE   0
+#define SPMX_VEC_DENSE    1
+#define SPMX_VEC_BITARRAY 2
+
+/* ---- SpMV back-ends for spmx_spmv / spmx_spmspv (set_spmv_type, H:1767) */
+#define SPMX_SPMV_HOLA 0
+#define SPMX_SPMV_CSR5 1
+
+/* ---- CSC SpMSpV work distributions and write-backs (H:1824-2201) */
+#define SPMX_CSC_NAIVE     0  /* group of threads per x nonzero            */
+#define SPMX_CSC_LB_MERGE  1  /* merge-path partition over (x entries, nnz) */
+#define SPMX_CSC_LB_TWOLAYER 2/* fixed nnz per CTA, block-start table      */
+#define SPMX_CSC_BUCKET    3  /* row-block buckets, no global atomics      */
+#define SPMX_WB_ATOMIC     0  /* dense y via atomics (+ optional compaction)*/
+#define SPMX_WB_SORT       1  /* (row,val) pairs -> sort -> reduce_by_key   */
+
+/* ---- the eight adaptive kernels, in the reference's three-stage tree order
+ *      (TEST/new_test_app.cu:406-456): solution x workload x write-back      */
+#define SPMX_K_CSC_NAIVE_SORT    0
+#define SPMX_K_CSC_NAIVE_ATOMIC  1
+#define SPMX_K_CSC_LB_SORT       2
+#define SPMX_K_CSC_LB_ATOMIC     3
+#define SPMX_K_CSR_NAIVE_SPMSPV  4
+#define SPMX_K_CSR_LB_SPMSPV     5
+#define SPMX_K_NAIVE_SPMV        6
+#define SPMX_K_LB_SPMV           7
+#define SPMX_NUM_KERNELS         8
+
+/* number of entries of the feature vector written by spmx_features; the order
+ * is the reference's 23-feature schema (model/1-test_dtree.py:63):
+ * m,n,nnz,maxRow,minRow,avgRow,range,stdRow,edge_equlity,gini,x_nnz,bin_len,
+ * max,min,xnnz/n,bin_len/nnz,xnnz_range,GM1,GM2,GM3,GM1/GM2,GM2/GM3,GM1/GM3 */
+#define SPMX_NUM_FEATURES 23
+
+typedef struct spmx_handle_s* spmx_handle_t;
+
+/* ======================= lifecycle ======================================= */
+/* SpmspvHandle(m, n, nnz) — H:91-141 */
+int spmx_create(int m, int n, int nnz, spmx_handle_t* out);
+/* Destroy() — H:2866-2887 (frees only handle-owned memory) */
+int spmx_destroy(spmx_handle_t h);
+/* no reference counterpart (the reference uses stream 0 everywhere) */
+int spmx_set_stream(spmx_handle_t h, void* cuda_stream);
+/* warmup() — H:347 */
+int spmx_warmup(spmx_handle_t h);
+/* number of kernels the library has launched so far (all handles); no
+ * reference counterpart */
+unsigned long long spmx_launch_count(void);
+/* thread-local text of the last error; never NULL */
+const char* spmx_last_error_string(void);
+/* sticky device error word of the handle (bounded waits, bounds checks);
+ * reading it synchronises the handle's stream and clears it */
+int spmx_check_device_error(spmx_handle_t h);
+
+/* ======================= matrix input ==================================== */
+/* InputCSR(nnz, csr_row, csr_col, csr_val) — H:356-366; csr_row = row pointer
+ * [m+1], csr_col = column indices [nnz]; d_csr_val may be NULL (pattern only,
+ * used by BFS) */
+int spmx_input_csr(spmx_handle_t h, int nnz, const int* d_csr_row,
+                   const int* d_csr_col, const float* d_csr_val);
+/* InputCSC(nnz, csc_row, csc_col, csc_val) — H:369-379; csc_row = row indices
+ * [nnz], csc_col = column pointer [n+1] (borrowed) */
+int spmx_input_csc(spmx_handle_t h, int nnz, const int* d_csc_row,
+                   const int* d_csc_col, const float* d_csc_val);
+/* ToCSC() — H:384-419 (cusparseScsr2csc there).  Handle-owned CSC with row
+ * indices sorted inside each column (a stable transpose). */
+int spmx_to_csc(spmx_handle_t h);
+/* read access to the handle's CSC (device pointers, valid until destroy) */
+int spmx_get_csc(spmx_handle_t h, const int** d_csc_row, const int** d_csc_col,
+                 const float** d_csc_val);
+
+/* ======================= vectors ========================================= */
+/* set_x — H:985 */
+int spmx_set_x(spmx_handle_t h, float* d_x);
+/* set_sparse_x — H:992-1002 */
+int spmx_set_sparse_x(spmx_handle_t h, int* d_x_key, float* d_x_val, int xnnz);
+/* set_bitvector — H:1005-1011 (num_ints = ceil(n/32)) */
+int spmx_set_bitvector(spmx_handle_t h, int* d_bitvector, int num_ints);
+/* set_sparse_x_dense_x — H:1014-1025 */
+int spmx_set_sparse_x_dense_x(spmx_handle_t h, int* d_x_key, float* d_x_val,
+                              float* d_x_dense, int xnnz);
+/* set_vector_type — H:979 */
+int spmx_set_vector_type(spmx_handle_t h, int code);
+
+/* sparse2dense — H:1240-1268 (memset + scatter) */
+int spmx_sparse2dense(spmx_handle_t h);
+/* sparse2bitarray — H:1271-1308 (dense x and bitarray from sparse x) */
+int spmx_sparse2bitarray(spmx_handle_t h);
+/* dense2sparse — H:1177-1222.  Writes x's key/val buffers from the dense x and
+ * updates the handle's x_nnz (the reference leaves it stale); if xnnz != NULL
+ * the count is also returned to the host (synchronises). */
+int spmx_dense2sparse(spmx_handle_t h, int* xnnz);
+/* bitarray2sparse — H:1311-1351 (same compaction, from the dense x) */
+int spmx_bitarray2sparse(spmx_handle_t h, int* xnnz);
+/* dense2bitarray — H:1373-1388, kernel H:1355.  Sets the bit of every NONZERO entry (the
+ * reference sets bits of zeros, H:1362). */
+int spmx_dense2bitarray(spmx_handle_t h);
+/* dense2sparse_outer — H:1953-1998 (no cudaMalloc per call here) */
+int spmx_dense2sparse_outer(spmx_handle_t h, int m, const float* d_dense,
+                            int* ynnz, int* d_key, float* d_val);
+/* sparse2dense_outer — H:1931-1950 */
+int spmx_sparse2dense_outer(spmx_handle_t h, int ynnz, const int* d_key,
+                            const float* d_val, int m, float* d_dense);
+
+/* ======================= scratch / preprocess ============================= */
+/* allocPreBuffer / deallocPreBuffer — H:1726-1763, H:2849-2864.  Sizes the scratch for the
+ * worst case (bin_len = nnz) so later calls never allocate. */
+int spmx_alloc_pre_buffer(spmx_handle_t h);
+int spmx_dealloc_pre_buffer(spmx_handle_t h);
+/* holaPreprocess / holaPostprocess — H:1654-1672 (block-start table) */
+int spmx_hola_preprocess(spmx_handle_t h);
+int spmx_hola_postprocess(spmx_handle_t h);
+/* setSigma / CSR5Preprocess / CSR5Postprocess — H:1396-1651.  sigma = -1
+ * selects the reference's auto rule (H:1396-1416). */
+int spmx_set_sigma(spmx_handle_t h, int sigma);
+int spmx_csr5_preprocess(spmx_handle_t h);
+int spmx_csr5_postprocess(spmx_handle_t h);
+/* set_spmv_type — H:1767 (0 Hola, 1 CSR5) */
+int spmx_set_spmv_type(spmx_handle_t h, int code);
+
+/* ======================= SpMV / CSR SpMSpV (y = alpha*A*x) =============== */
+/* naivespmv — H:1677-1684, DEV/naivespmv.h:34 */
+int spmx_naivespmv(spmx_handle_t h, float alpha, float* d_y);
+/* holaspmv — H:1687-1698, DEV/holaspmv.h:2070 */
+int spmx_holaspmv(spmx_handle_t h, float alpha, float* d_y);
+/* csr5spmv — H:1586-1605, DEV/csr5_spmv_cuda.h:440 */
+int spmx_csr5spmv(spmx_handle_t h, float alpha, float* d_y);
+/* naivespmspv — H:1701-1706, DEV/naivespmv.h:13 (x gated by the bitarray) */
+int spmx_naivespmspv(spmx_handle_t h, float alpha, float* d_y);
+/* holaspmspv — H:1709-1721, DEV/holaspmv.h:2224 */
+int spmx_holaspmspv(spmx_handle_t h, float alpha, float* d_y);
+/* csr5spmspv — H:1607-1627, DEV/csr5_spmspv.h:450 */
+int spmx_csr5spmspv(spmx_handle_t h, float alpha, float* d_y);
+/* spmv / spmspv dispatch by spmv_type — H:1790-1821 */
+int spmx_spmv(spmx_handle_t h, float alpha, float* d_y);
+int spmx_spmspv(spmx_handle_t h, float alpha, float* d_y);
+
+/* ======================= CSC SpMSpV (y = alpha*A*x, x sparse) ============= */
+/* Generic form.  variant: SPMX_CSC_*, writeback: SPMX_WB_*.
+ *  - atomic: d_y (dense, m) is overwritten; if d_y_key/d_y_val are non-NULL the
+ *    nonzeros of y (entries != 0) are also compacted into them, in row order.
+ *  - sort:   d_y_key/d_y_val receive the rows touched by x's columns, sorted,
+ *    with their sums (zeros kept — reduce_by_key semantics); d_y may be NULL,
+ *    otherwise it is also written densely.
+ *  - bucket: as sort for the sparse output, plus dense d_y if non-NULL.
+ * ynnz (host, may be NULL) receives the output count (synchronises). */
+int spmx_spmspv_csc(spmx_handle_t h, int variant, int writeback, float alpha,
+                    float* d_y, int* d_y_key, float* d_y_val, int* ynnz);
+/* CscBasedNoSortNaiveSpmspv — H:2119-2139 */
+int spmx_csc_naive_atomic(spmx_handle_t h, float alpha, int* ynnz, float* d_y);
+/* CscBasedNoSortNaiveSpmspv_keyval — H:2143-2169 */
+int spmx_csc_naive_atomic_keyval(spmx_handle_t h, float alpha, int* ynnz,
+                                 float* d_y, int* d_y_key, float* d_y_val);
+/* CscBasedSortNaiveSpmspv — H:2172-2201 */
+int spmx_csc_naive_sort(spmx_handle_t h, float alpha, int* ynnz, int* d_y_key,
+                        float* d_y_val);
+/* CscBasedNoSortMergeSpmspv(_keyval) — H:2033-2088 (binlen_ready ignored:
+ * bin_len never leaves the device here) */
+int spmx_csc_merge_atomic(spmx_handle_t h, int binlen_ready, float alpha,
+                          int* ynnz, float* d_y, int* d_y_key, float* d_y_val);
+int spmx_csc_merge_atomic_keyval(spmx_handle_t h, int binlen_ready, float alpha,
+                                 int* ynnz, float* d_y, int* d_y_key,
+                                 float* d_y_val);
+/* CscBasedSortMergeSpmspv — H:2091-2115 */
+int spmx_csc_merge_sort(spmx_handle_t h, int binlen_ready, float alpha,
+                        int* ynnz, float* d_y, int* d_y_key, float* d_y_val);
+/* CscBasedMyNoSortSpmspv(_keyval) / CscBasedSortMySpmspv — H:1824-1878, H:2001-2029 */
+int spmx_csc_twolayer_atomic(spmx_handle_t h, int binlen_ready, float alpha,
+                             int* ynnz, float* d_y, int* d_y_key,
+                             float* d_y_val);
+int spmx_csc_twolayer_atomic_keyval(spmx_handle_t h, int binlen_ready,
+                                    float alpha, int* ynnz, float* d_y,
+                                    int* d_y_key, float* d_y_val);
+int spmx_csc_twolayer_sort(spmx_handle_t h, int binlen_ready, float alpha,
+                           int* ynnz, float* d_y, int* d_y_key, float* d_y_val);
+/* CscBasedBucketSpmspvDriver — DEV/csc_bucket_spmspv.cuh:768-1087 (whose
+ * reduction is disabled in the reference; completed here).  buckets <= 0
+ * selects the tuned/default count. */
+int spmx_csc_bucket(spmx_handle_t h, float alpha, int* ynnz, float* d_y,
+                    int* d_y_key, float* d_y_val, int buckets);
+
+/* ======================= features / selector ============================== */
+/* computeBinlenVer2 — H:2703-2723 (sum of the column lengths of x's keys) */
+int spmx_compute_binlen(spmx_handle_t h, long long* bin_len);
+/* computeGM1/2/3 — H:2727-2752 (needs bin_len) */
+int spmx_compute_gm(spmx_handle_t h, double gm[3]);
+/* computeMatFeture_serial — H:2275-2335, computed on the device:
+ * out = {m, n, nnz, maxRow, minRow, avgRow, range, stdRow, edge_equlity, gini} */
+int spmx_mat_features(spmx_handle_t h, double out[10]);
+/* extractMatFeatureParallel — H:921-976 (stdRow with the int-truncated mean) */
+int spmx_std_row(spmx_handle_t h, float* std_row);
+/* computeVecFeture_serial — H:2338-2361 without the per-call colptr copy:
+ * out = {bin_len, max, min} */
+int spmx_vec_features(spmx_handle_t h, long long out[3]);
+/* full 23-entry feature vector (SPMX_NUM_FEATURES order above) */
+int spmx_features(spmx_handle_t h, double out[SPMX_NUM_FEATURES]);
+/* predictSolution / predictWorkloadDistribution / predictWritingBack —
+ * TEST/new_test_app.cu:121-131 (stubs there); a decision tree here.
+ * kernel_id receives one of SPMX_K_*. */
+int spmx_select(spmx_handle_t h, int* kernel_id);
+/* the selector on a caller-supplied feature vector (host only, no handle, no
+ * GPU): predictSolution / predictWorkloadDistribution / predictWritingBack
+ * combined (TEST/new_test_app.cu:121-131) */
+int spmx_select_features(const double f[SPMX_NUM_FEATURES], int* kernel_id);
+/* the adaptive iteration of TEST/new_test_app.cu:349-465 (#if 0 there):
+ * select, convert x as the chosen kernel needs (s2d / s2a), run it.
+ * d_y (dense, m) always receives y; kernel_used (host, may be NULL). */
+int spmx_run_adaptive(spmx_handle_t h, float alpha, float* d_y, int* kernel_used);
+/* run one of the eight kernels by id (used by the exhaustive timing harness) */
+int spmx_run_kernel(spmx_handle_t h, int kernel_id, float alpha, float* d_y);
+
+/* ======================= BFS (Boolean OR-AND semiring) ==================== */
+/* The SpMSpV-driven BFS the replay loops of TEST/test_application.cu:240-415
+ * and TEST/new_test_app.cu:280-469 stand in for.  Needs a symmetric pattern
+ * (CSR; CSC is taken as the same arrays).  d_levels[n] receives hop counts,
+ * -1 for unreachable; depth (host, may be NULL) the number of levels. */
+int spmx_bfs(spmx_handle_t h, int source, int* d_levels, int* depth);
+
+/* ======================= device counters ================================== */
+/* device pointers to the handle's counters: [0] y_nnz of the last SpMSpV,
+ * [1] bin_len of the last scan, [2] x_nnz after dense2sparse */
+int spmx_get_device_counts(spmx_handle_t h, const int** d_counts);
+
+/* ======================= host-side generators (no GPU) =================== */
+/* Deterministic synthetic inputs (counter-based RNG; identical for any thread
+ * count).  Output arrays are allocated with malloc by the generator and must
+ * be released with spmx_host_free. */
+void spmx_host_free(void* p);
+/* symmetric R-MAT (no vertex permutation), self-loops and duplicates removed,
+ * columns sorted per row */
+int spmx_gen_rmat(int scale, int edge_factor, double a, double b, double c,
+                  uint64_t seed, int* m_out, long long* nnz_out, int** rowptr,
+                  int** col);
+/* m x m, truncated Zipf(s) row lengths on [1, maxlen] scaled to mean `mean`
+ * with stochastic rounding, total nnz fixed to mean*m, distinct uniform
+ * columns per row, values U(-1,1) */
+int spmx_gen_zipf_rows(int m, double s, int mean, int maxlen, uint64_t seed,
+                       long long* nnz_out, int** rowptr, int** col, float** val);
+/* Chung-Lu power law (degree exponent gamma, average expected degree avg),
+ * symmetric pattern, self-loops and duplicates removed, values N(0,1) */
+int spmx_gen_chung_lu(int n, double gamma, double avg, uint64_t seed,
+                      long long* nnz_out, int** rowptr, int** col, float** val);
+/* 2-D 5-point Laplacian on a g x g grid, diagonal 4, off-diagonals
+ * -1 + N(0, sigma^2) */
+int spmx_gen_laplacian(int g, double sigma, uint64_t seed, long long* nnz_out,
+                       int** rowptr, int** col, float** val);
+/* k distinct positions in [0,n) (sorted) into caller buffers, values U(-1,1)
+ * (dist 0) or N(0,1) (dist 1) */
+int spmx_gen_sparse_vector(int n, int k, int dist, uint64_t seed, int* key,
+                           float* val);
+/* host CSR -> CSC (stable; rows sorted within columns); val/cval may be NULL */
+int spmx_host_csr2csc(int m, int n, const int* rowptr, const int* col,
+                      const float* val, int* colptr, int* row, float* cval);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SPMX_H_ */

@@ -1,0 +1,407 @@
+/*
+ * spmx_oracle.c — CPU oracle for the adaptive SpMV / SpMSpV path.
+ *
+ * TEST INFRASTRUCTURE ONLY.  This file is the checker: the tests, the smoke
+ * check and the CPU-baseline leg of the benchmark load it; the product (the
+ * CUDA library) never does.
+ *
+ * Each function restates a CPU routine of hpc-research-2020/spmspv-adaptive
+ * (paths relative to hice-spmspv/hice/la/):
+ *   - serialspmv                 test/test_application.cu:107-116
+ *   - SpmSpvCSCHost              test/test_sort_spmspv.cu:330-375
+ *   - computeMatFeture_serial    include/spmspv/csc-spmspv/spmspv.h:2275-2335
+ *   - extractMatFeature (stdRow) include/spmspv/csc-spmspv/spmspv.h:423-447
+ *   - computeVecFeture_serial    include/spmspv/csc-spmspv/spmspv.h:2338-2361
+ *   - computeGM1/2/3             include/spmspv/csc-spmspv/spmspv.h:2727-2752
+ *   - setSigma (auto rule)       include/spmspv/csc-spmspv/spmspv.h:1396-1416
+ *   - updateFlag/streamCompact   include/spmspv/csc-spmspv/spmspv.h:1122-1175
+ *   - scatter / bitvector        spmspv.h:1226-1308, detail/device/bitvector.h
+ * The reference has no BFS and no adjoint; those oracles are restated from
+ * their definitions (level-synchronous Boolean SpMSpV with a visited mask, in
+ * the loop structure of SpmSpvCSCHost; dx = A^T dy, dvals = dy[row]*x[col]).
+ *
+ * Parity status: the reference ships no golden vectors or fixtures for this
+ * path; the restatements are pinned against the reference's own host code
+ * compiled from its sources (oracle/build_ref.sh -> oracle/_ref) where that
+ * builds, as recorded by tests/test_oracle_pin.py.
+ *
+ * Deliberate departures from the reference, each noted at its function:
+ *   - SpmSpvCSCHost reads x_val into an int (test_sort_spmspv.cu:340); the
+ *     oracle keeps the value.
+ *   - accumulation is FP64 unless the function is marked "faithful".
+ */
+#include <math.h>
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+#include <float.h>
+#include <limits.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+#define EXPORT __attribute__((visibility("default")))
+
+/* ---- SpMV ---------------------------------------------------------------- */
+
+/* serialspmv, faithful: FP32 accumulation, product order x*val*alpha
+ * (test_application.cu:107-116). */
+EXPORT void oracle_serialspmv_f32(int m, const int* rowptr, const int* col,
+                                  const float* val, const float* x, float* y,
+                                  float alpha) {
+  for (int i = 0; i < m; i++) {
+    float sum = 0;
+    for (int j = rowptr[i]; j < rowptr[i + 1]; j++) sum += x[col[j]] * val[j] * alpha;
+    y[i] = sum;
+  }
+}
+
+/* serialspmv in FP64; also returns sum_j |a_ij x_j| per row (the magnitude
+ * that scales the FP32 tolerance).  `bits` (may be NULL) gates x like
+ * naive_spmspv_ker (detail/device/naivespmv.h:13-31). */
+EXPORT void oracle_spmv_f64(int m, const int* rowptr, const int* col,
+                            const float* val, const float* x, const int* bits,
+                            double alpha, double* y, double* absy) {
+#pragma omp parallel for schedule(dynamic, 1024)
+  for (int i = 0; i < m; i++) {
+    double s = 0, a = 0;
+    for (int j = rowptr[i]; j < rowptr[i + 1]; j++) {
+      const int c = col[j];
+      if (bits && !((((const unsigned*)bits)[c >> 5] >> (c & 31)) & 1u)) continue;
+      const double p = (double)val[j] * (double)x[c];
+      s += p;
+      a += fabs(p);
+    }
+    y[i] = alpha * s;
+    if (absy) absy[i] = fabs(alpha) * a;
+  }
+}
+
+/* ---- CSC SpMSpV ------------------------------------------------------------ */
+
+/* SpmSpvCSCHost (test_sort_spmspv.cu:330-375) in FP64 with the x value kept
+ * as a float (the reference truncates it to int).  Writes the dense result
+ * y[m], its magnitude absy[m] and touched[m] (1 if row i appears in any
+ * selected column: the structural output of the sort write-back). */
+EXPORT void oracle_spmspv_csc_f64(int m, const int* colptr, const int* row,
+                                  const float* val, int x_nnz, const int* x_key,
+                                  const float* x_val, double alpha, double* y,
+                                  double* absy, unsigned char* touched) {
+  memset(y, 0, sizeof(double) * (size_t)m);
+  if (absy) memset(absy, 0, sizeof(double) * (size_t)m);
+  if (touched) memset(touched, 0, (size_t)m);
+  for (int i = 0; i < x_nnz; i++) {
+    const int c = x_key[i];
+    const double xv = (double)x_val[i];
+    for (int j = colptr[c]; j < colptr[c + 1]; j++) {
+      const double p = (double)val[j] * xv;
+      y[row[j]] += p;
+      if (absy) absy[row[j]] += fabs(p);
+      if (touched) touched[row[j]] = 1;
+    }
+  }
+  for (int r = 0; r < m; r++) {
+    y[r] *= alpha;
+    if (absy) absy[r] *= fabs(alpha);
+  }
+}
+
+/* The reference's CPU sparse output of SpmSpvCSCHost: entries whose |y| is
+ * not below FLT_EPSILON (IS_FLOAT_ZERO in the test drivers), in row order.  Returns
+ * the count. */
+EXPORT int oracle_sparse_output_flt_eps(int m, const double* y, int* key, float* v) {
+  int k = 0;
+  for (int r = 0; r < m; r++)
+    if (!(fabs(y[r]) < FLT_EPSILON)) { key[k] = r; v[k] = (float)y[r]; k++; }
+  return k;
+}
+
+/* ---- vector format conversions --------------------------------------------- */
+
+/* scatter (spmspv.h:1226-1236) into a zeroed dense vector; sets the bits of
+ * the keys like set_sparse_x_bitvector (bitvector.h).  Either output may be
+ * NULL. */
+EXPORT void oracle_sparse2dense_bits(int n, int x_nnz, const int* key, const float* val,
+                                     float* dense, unsigned* bits) {
+  if (dense) memset(dense, 0, sizeof(float) * (size_t)n);
+  if (bits) memset(bits, 0, sizeof(unsigned) * (size_t)((n + 31) / 32));
+  for (int i = 0; i < x_nnz; i++) {
+    if (dense) dense[key[i]] = val ? val[i] : 1.0f;
+    if (bits) bits[key[i] >> 5] |= 1u << (key[i] & 31);
+  }
+}
+
+/* updateFlagKernel + scan + streamCompactKeyValKernel (spmspv.h:1122-1175):
+ * the entries != 0 in index order.  Returns the count. */
+EXPORT int oracle_dense2sparse(int n, const float* dense, int* key, float* val) {
+  int k = 0;
+  for (int i = 0; i < n; i++)
+    if (dense[i] != 0.0f) { key[k] = i; val[k] = dense[i]; k++; }
+  return k;
+}
+
+/* dense2bitarray with the bit of every NONZERO entry set (the reference's
+ * dense2bitarray_ker tests `!val` and so marks the zeros, spmspv.h:1362). */
+EXPORT void oracle_dense2bitarray(int n, const float* dense, unsigned* bits) {
+  memset(bits, 0, sizeof(unsigned) * (size_t)((n + 31) / 32));
+  for (int i = 0; i < n; i++)
+    if (dense[i] != 0.0f) bits[i >> 5] |= 1u << (i & 31);
+}
+
+/* ---- features ------------------------------------------------------------------- */
+
+/* computeMatFeture_serial (spmspv.h:2275-2335) with exact (FP64 / int64)
+ * accumulation.  out = {m, n, nnz, max, min, avg, range, stdRow,
+ * edge_equlity, gini}.  avg keeps the reference's float division
+ * mat_nnz/(float)m. */
+EXPORT void oracle_mat_features(int m, int n, int nnz, const int* rowptr, double* out) {
+  int mx = 0, mn = INT_MAX;
+  const double avg = m ? (double)((float)nnz / (float)m) : 0.0;
+  double sq = 0, ent = 0;
+  int64_t* hist = NULL;
+  for (int i = 0; i < m; i++) {
+    const int d = rowptr[i + 1] - rowptr[i];
+    sq += (d - avg) * (d - avg);
+    if (d != 0) ent += -((double)d / nnz) * log((double)d / nnz);
+    if (d > mx) mx = d;
+    if (d < mn) mn = d;
+  }
+  /* Gini over sorted degrees: S1 = sum_{j>=1} j*d_(j), S2 = sum_{i<m-1} d_(i)
+   * (spmspv.h:2314-2320), via a counting sort */
+  double gini = 0;
+  if (m > 0) {
+    hist = (int64_t*)calloc((size_t)mx + 1, sizeof(int64_t));
+    for (int i = 0; i < m; i++) hist[rowptr[i + 1] - rowptr[i]]++;
+    int64_t pos = 0;
+    unsigned long long s1 = 0;
+    for (int v = 0; v <= mx; v++) {
+      const int64_t h = hist[v];
+      if (h) s1 += (unsigned long long)v * (unsigned long long)(h * pos + h * (h - 1) / 2);
+      pos += h;
+    }
+    free(hist);
+    const double S2 = (double)nnz - (double)mx;
+    gini = (2.0 * (double)s1) / ((double)m * S2) - (double)(m + 1) / (double)m;
+    if (gini < 0) gini = -gini;
+    if (!isfinite(gini)) gini = 0;
+  }
+  out[0] = m; out[1] = n; out[2] = nnz; out[3] = mx; out[4] = mn; out[5] = avg;
+  out[6] = n ? (double)(mx - mn) / (double)n : 0.0;
+  out[7] = m ? sqrt(sq / m) : 0.0;
+  out[8] = m > 1 ? ent / log((double)m) : 0.0;
+  out[9] = gini;
+}
+
+/* computeMatFeture_serial, faithful: float accumulators exactly as written
+ * (float sum, float sum_gini_1/2, std::sort of degrees).  Kept to document
+ * how far the reference's float sums drift from the exact values. */
+static int cmp_int(const void* a, const void* b) {
+  const int x = *(const int*)a, y = *(const int*)b;
+  return (x > y) - (x < y);
+}
+EXPORT void oracle_mat_features_faithful(int m, int n, int nnz, const int* rowptr,
+                                         float* out) {
+  int max = 0, min = INT_MAX;
+  float sum = 0.0f, sum_gini_1 = 0.0f, sum_gini_2 = 0.0f;
+  double sum_edge = 0.0;
+  const double avg = nnz / (float)m;
+  int* deg = (int*)malloc(sizeof(int) * (size_t)m);
+  for (int i = 0; i < m; i++) {
+    const int num = rowptr[i + 1] - rowptr[i];
+    deg[i] = num;
+    sum += (num - avg) * (num - avg);
+    if (num != 0) sum_edge += -(num / (1.0 * nnz)) * log(num / (1.0 * nnz));
+    if (num > max) max = num;
+    if (num < min) min = num;
+  }
+  const float stdv = sqrtf(sum / m);
+  const float edge = (float)sum_edge * (1.0 / log(m * 1.0));
+  qsort(deg, (size_t)m, sizeof(int), cmp_int);
+  int j = 1;
+  for (int i = 0; i + 1 < m; i++) {
+    sum_gini_1 += 1.0 * j * deg[i + 1];
+    sum_gini_2 += 1.0 * deg[i];
+    j++;
+  }
+  float gini = (2.0 * sum_gini_1) / (m * sum_gini_2) - (m + 1) / (float)m;
+  if (gini < 0) gini *= -1;
+  free(deg);
+  out[0] = (float)max; out[1] = (float)min; out[2] = (float)avg;
+  out[3] = (float)((max - min) / (1.0 * n)); out[4] = stdv; out[5] = edge; out[6] = gini;
+}
+
+/* extractMatFeature (spmspv.h:423-447): stdRow with the mean truncated to
+ * int, accumulated in FP64 here. */
+EXPORT double oracle_std_row_intmean(int m, int nnz, const int* rowptr) {
+  const int avg = (int)(nnz / (float)m);
+  double s = 0;
+  for (int i = 0; i < m; i++) {
+    const int d = rowptr[i + 1] - rowptr[i];
+    s += (double)(d - avg) * (double)(d - avg);
+  }
+  return sqrt(s / m);
+}
+
+/* computeVecFeture_serial (spmspv.h:2338-2361): out = {bin_len, max, min} */
+EXPORT void oracle_vec_features(const int* colptr, int x_nnz, const int* x_key,
+                                long long* out) {
+  long long sum = 0;
+  int mx = 0, mn = INT_MAX;
+  for (int i = 0; i < x_nnz; i++) {
+    const int c = x_key[i];
+    const int num = colptr[c + 1] - colptr[c];
+    sum += num;
+    if (num > mx) mx = num;
+    if (num < mn) mn = num;
+  }
+  out[0] = sum; out[1] = mx; out[2] = mn;
+}
+
+/* computeGM1/2/3 (spmspv.h:2727-2752) with 4-byte indices and values */
+EXPORT void oracle_gm(int m, int nnz, int x_nnz, long long bin_len, double* gm) {
+  const double x = x_nnz, b = (double)bin_len;
+  gm[0] = x * 4 + b * 4 + b * 4 + x * 4 + x * 4 + b * 4;
+  gm[1] = ((double)m + 1) * 4 + b * 4 + (double)nnz * 4 + b * 4 + (double)m * 4;
+  gm[2] = ((double)m + 1) * 4 + (double)nnz * 4 * 3 + (double)m * 4;
+}
+
+/* setSigma auto rule (spmspv.h:1396-1416) */
+EXPORT int oracle_csr5_sigma(int m, int nnz) {
+  const int r = 4, s = 32, t = 256, u = 6;
+  const int nnz_per_row = nnz / m;
+  if (nnz_per_row <= r) return r;
+  if (nnz_per_row <= s) return nnz_per_row;
+  if (nnz_per_row <= t) return s;
+  return u;
+}
+
+/* ---- BFS ------------------------------------------------------------------------ */
+
+/* Level-synchronous BFS as repeated Boolean SpMSpV y = A^T f masked by the
+ * visited set, written in the loop structure of SpmSpvCSCHost (a CSC pass
+ * over the frontier's columns).  levels[n] = hop count, -1 if unreachable.
+ * Returns the number of levels. */
+EXPORT int oracle_bfs_spmspv(int n, const int* colptr, const int* row, int src, int* levels) {
+  int* qbuf = (int*)malloc(sizeof(int) * 2 * (size_t)(n > 0 ? n : 1));
+  int* front = qbuf;
+  int* next = qbuf + (n > 0 ? n : 1);
+  unsigned char* y = (unsigned char*)calloc((size_t)(n > 0 ? n : 1), 1);
+  for (int i = 0; i < n; i++) levels[i] = -1;
+  levels[src] = 0;
+  int nf = 1, level = 0;
+  front[0] = src;
+  while (nf > 0) {
+    /* y = OR over frontier columns (Boolean SpMSpV) */
+    for (int i = 0; i < nf; i++) {
+      const int c = front[i];
+      for (int j = colptr[c]; j < colptr[c + 1]; j++) y[row[j]] = 1;
+    }
+    /* mask by visited, emit the next frontier in row order */
+    int nn = 0;
+    for (int r = 0; r < n; r++) {
+      if (y[r] && levels[r] < 0) { levels[r] = level + 1; next[nn++] = r; }
+      y[r] = 0;
+    }
+    int* t = front; front = next; next = t;
+    nf = nn;
+    if (nf > 0) level++;
+  }
+  free(qbuf); free(y);
+  return level + 1;
+}
+
+/* Plain FIFO-queue BFS, the cross-check of the SpMSpV formulation. */
+EXPORT int oracle_bfs_queue(int n, const int* rowptr, const int* col, int src, int* levels) {
+  int* q = (int*)malloc(sizeof(int) * (size_t)(n > 0 ? n : 1));
+  for (int i = 0; i < n; i++) levels[i] = -1;
+  int head = 0, tail = 0, depth = 0;
+  levels[src] = 0;
+  q[tail++] = src;
+  while (head < tail) {
+    const int u = q[head++];
+    if (levels[u] + 1 > depth) depth = levels[u] + 1;
+    for (int j = rowptr[u]; j < rowptr[u + 1]; j++) {
+      const int v = col[j];
+      if (levels[v] < 0) { levels[v] = levels[u] + 1; q[tail++] = v; }
+    }
+  }
+  free(q);
+  return depth;
+}
+
+/* ---- adjoint of y = A x ------------------------------------------------------ */
+
+/* dx = A^T dy (dense dy) in FP64, with per-entry magnitudes */
+EXPORT void oracle_spmv_t_f64(int m, int n, const int* rowptr, const int* col,
+                              const float* val, const float* dy, double* dx, double* absdx) {
+  memset(dx, 0, sizeof(double) * (size_t)n);
+  if (absdx) memset(absdx, 0, sizeof(double) * (size_t)n);
+  for (int i = 0; i < m; i++)
+    for (int j = rowptr[i]; j < rowptr[i + 1]; j++) {
+      const double p = (double)val[j] * (double)dy[i];
+      dx[col[j]] += p;
+      if (absdx) absdx[col[j]] += fabs(p);
+    }
+}
+
+/* dvals[k] = dy[row_k] * x[col_k] in FP64 */
+EXPORT void oracle_dvals_f64(int m, const int* rowptr, const int* col, const float* dy,
+                             const float* x, double* dvals) {
+  for (int i = 0; i < m; i++)
+    for (int j = rowptr[i]; j < rowptr[i + 1]; j++)
+      dvals[j] = (double)dy[i] * (double)x[col[j]];
+}
+
+/* ---- timed CPU baselines ------------------------------------------------------ */
+
+/* serialspmv (FP32, one core) over the whole matrix */
+EXPORT void cpu_spmv_serial(int m, const int* rowptr, const int* col, const float* val,
+                            const float* x, float* y, float alpha) {
+  oracle_serialspmv_f32(m, rowptr, col, val, x, y, alpha);
+}
+
+/* the same loop split over rows with OpenMP (all host threads) */
+EXPORT void cpu_spmv_omp(int m, const int* rowptr, const int* col, const float* val,
+                         const float* x, float* y, float alpha) {
+#pragma omp parallel for schedule(dynamic, 2048)
+  for (int i = 0; i < m; i++) {
+    float sum = 0;
+    for (int j = rowptr[i]; j < rowptr[i + 1]; j++) sum += x[col[j]] * val[j] * alpha;
+    y[i] = sum;
+  }
+}
+
+/* SpmSpvCSCHost with FP32 accumulation into a dense y (one core) */
+EXPORT void cpu_spmspv_csc_serial(int m, const int* colptr, const int* row, const float* val,
+                                  int x_nnz, const int* x_key, const float* x_val, float* y) {
+  memset(y, 0, sizeof(float) * (size_t)m);
+  for (int i = 0; i < x_nnz; i++) {
+    const int c = x_key[i];
+    const float xv = x_val[i];
+    for (int j = colptr[c]; j < colptr[c + 1]; j++) y[row[j]] += val[j] * xv;
+  }
+}
+
+/* CSC SpMSpV on all host threads: x entries split across threads, each with
+ * atomic float adds into y */
+EXPORT void cpu_spmspv_csc_omp(int m, const int* colptr, const int* row, const float* val,
+                               int x_nnz, const int* x_key, const float* x_val, float* y) {
+  memset(y, 0, sizeof(float) * (size_t)m);
+#pragma omp parallel for schedule(dynamic, 64)
+  for (int i = 0; i < x_nnz; i++) {
+    const int c = x_key[i];
+    const float xv = x_val[i];
+    for (int j = colptr[c]; j < colptr[c + 1]; j++) {
+#pragma omp atomic
+      y[row[j]] += val[j] * xv;
+    }
+  }
+}
+
+EXPORT int cpu_threads(void) {
+#ifdef _OPENMP
+  return omp_get_max_threads();
+#else
+  return 1;
+#endif
+}

@@ -1,0 +1,251 @@
+// Shared device helpers for the spmx kernels: warp/block scans, bounded waits,
+// a decoupled look-back tile scan and the device error word.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace spmx {
+
+constexpr int kWarp = 32;
+
+// Bits of the per-handle device error word.  Kernels never trap: they record
+// the problem here, skip the offending access and return.
+enum DeviceError : int {
+  kDevErrTimeout = 1,  // a bounded wait (look-back, grid barrier) gave up
+  kDevErrOob = 2,      // an index outside its array (bad x key, bad column)
+  kDevErrCapacity = 4, // an internal capacity was exceeded
+};
+
+// Upper bound on spin iterations of any wait; with the back-off below this is
+// on the order of seconds, far beyond any legitimate wait.
+constexpr long long kSpinLimit = 1LL << 24;
+
+__device__ __forceinline__ void flag_error(int* err, int code) {
+  if (err) atomicOr(err, code);
+}
+
+__device__ __forceinline__ unsigned lane_id() { return threadIdx.x & 31u; }
+__device__ __forceinline__ unsigned lanemask_lt() {
+  unsigned m;
+  asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+  return m;
+}
+
+template <class T>
+__device__ __forceinline__ T warp_inclusive_sum(T v) {
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    T t = __shfl_up_sync(0xffffffffu, v, o);
+    if ((int)lane_id() >= o) v += t;
+  }
+  return v;
+}
+
+template <class T>
+__device__ __forceinline__ T warp_sum(T v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+template <class T>
+__device__ __forceinline__ T warp_max(T v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    T t = __shfl_xor_sync(0xffffffffu, v, o);
+    v = t > v ? t : v;
+  }
+  return v;
+}
+
+// Block-wide exclusive sum over NT threads.  `warp_tmp` holds NT/32 entries.
+// Returns the exclusive prefix of the calling thread; *total gets the block sum.
+template <int NT, class T>
+__device__ __forceinline__ T block_exclusive_sum(T v, T* warp_tmp, T* total) {
+  constexpr int NW = NT / 32;
+  const int w = threadIdx.x >> 5;
+  T inc = warp_inclusive_sum(v);
+  if (lane_id() == 31) warp_tmp[w] = inc;
+  __syncthreads();
+  if (w == 0) {
+    T s = (lane_id() < (unsigned)NW) ? warp_tmp[lane_id()] : T(0);
+    T si = warp_inclusive_sum(s);
+    if (lane_id() < (unsigned)NW) warp_tmp[lane_id()] = si - s;
+    if (lane_id() == NW - 1) warp_tmp[NW] = si;
+  }
+  __syncthreads();
+  T ex = warp_tmp[w] + inc - v;
+  *total = warp_tmp[NW];
+  __syncthreads();
+  return ex;
+}
+
+// Block-wide inclusive max-scan of ints over NT threads.
+template <int NT>
+__device__ __forceinline__ int block_inclusive_max(int v, int* warp_tmp) {
+  constexpr int NW = NT / 32;
+  const int w = threadIdx.x >> 5;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    int t = __shfl_up_sync(0xffffffffu, v, o);
+    if ((int)lane_id() >= o) v = max(v, t);
+  }
+  if (lane_id() == 31) warp_tmp[w] = v;
+  __syncthreads();
+  if (w == 0) {
+    int s = (lane_id() < (unsigned)NW) ? warp_tmp[lane_id()] : INT_MIN;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      int t = __shfl_up_sync(0xffffffffu, s, o);
+      if ((int)lane_id() >= o) s = max(s, t);
+    }
+    if (lane_id() < (unsigned)NW) warp_tmp[lane_id()] = s;
+  }
+  __syncthreads();
+  int carry = (w > 0) ? warp_tmp[w - 1] : INT_MIN;
+  __syncthreads();
+  return max(v, carry);
+}
+
+__device__ __forceinline__ unsigned long long ld_volatile_u64(
+    const unsigned long long* p) {
+  return *(const volatile unsigned long long*)p;
+}
+__device__ __forceinline__ void st_volatile_u64(unsigned long long* p,
+                                                unsigned long long v) {
+  *(volatile unsigned long long*)p = v;
+}
+
+// ---------------------------------------------------------------------------
+// Decoupled look-back for a single-pass tile scan of 32-bit sums.
+//
+// Status word (64 bit): [63:34] epoch (30 bits), [33:32] state, [31:0] value.
+// state 1 = tile aggregate available, 2 = inclusive prefix available; a word
+// whose epoch differs from the launch's epoch reads as "not ready", so the
+// status array never needs clearing between launches.  Tiles are handed out in
+// launch order through an atomic ticket, so every predecessor of a tile is
+// already resident and the look-back always terminates; the wait is still
+// bounded and reports kDevErrTimeout instead of hanging.
+// ---------------------------------------------------------------------------
+struct LookbackState {
+  unsigned long long* status;  // one word per tile
+  unsigned* ticket;            // tile ticket, reset by the last tile
+  unsigned epoch;              // 30-bit launch epoch (host increments)
+};
+
+__device__ __forceinline__ unsigned long long lb_pack(unsigned epoch,
+                                                      unsigned state,
+                                                      unsigned value) {
+  return ((unsigned long long)(epoch & 0x3fffffffu) << 34) |
+         ((unsigned long long)(state & 3u) << 32) | (unsigned long long)value;
+}
+
+// Acquire a tile id (call from all threads; uses one smem word).
+__device__ __forceinline__ int lb_acquire_tile(const LookbackState& st,
+                                               int ntiles, int* smem_word) {
+  if (threadIdx.x == 0) {
+    unsigned t = atomicAdd(st.ticket, 1u);
+    // The last tile handed out resets the ticket for the next launch: every
+    // other tile already holds its id, and the grid has exactly ntiles CTAs.
+    if ((int)t == ntiles - 1) atomicExch(st.ticket, 0u);
+    *smem_word = (int)t;
+  }
+  __syncthreads();
+  int t = *smem_word;
+  __syncthreads();
+  return t;
+}
+
+// Called by warp 0 only.  Publishes the tile aggregate, looks back over the
+// predecessors and publishes the inclusive prefix.  Returns the exclusive
+// prefix of the tile (valid in all lanes of warp 0).
+__device__ __forceinline__ unsigned lb_warp_lookback(const LookbackState& st,
+                                                     int tile,
+                                                     unsigned aggregate,
+                                                     int* err) {
+  const unsigned lane = lane_id();
+  if (tile == 0) {
+    if (lane == 0) st_volatile_u64(&st.status[0], lb_pack(st.epoch, 2u, aggregate));
+    return 0u;
+  }
+  if (lane == 0) st_volatile_u64(&st.status[tile], lb_pack(st.epoch, 1u, aggregate));
+  unsigned exclusive = 0;
+  int j = tile - 1;
+  bool timed_out = false;
+  while (true) {
+    int idx = j - (int)lane;
+    unsigned state = 2u, value = 0u;
+    long long spins = 0;
+    while (true) {
+      if (idx >= 0) {
+        unsigned long long w = ld_volatile_u64(&st.status[idx]);
+        unsigned ep = (unsigned)(w >> 34);
+        state = (ep == (st.epoch & 0x3fffffffu)) ? (unsigned)((w >> 32) & 3u) : 0u;
+        value = (unsigned)w;
+      }
+      if (!__any_sync(0xffffffffu, state == 0u)) break;
+      if (++spins > kSpinLimit) { timed_out = true; break; }
+      __nanosleep(32);
+    }
+    if (__any_sync(0xffffffffu, timed_out)) {
+      if (lane == 0) flag_error(err, kDevErrTimeout);
+      exclusive = 0;
+      break;
+    }
+    unsigned pmask = __ballot_sync(0xffffffffu, state == 2u);
+    int first_p = pmask ? (__ffs(pmask) - 1) : 32;
+    unsigned contrib = ((int)lane <= first_p) ? value : 0u;
+    exclusive += warp_sum(contrib);
+    if (pmask) break;
+    j -= 32;
+  }
+  if (lane == 0)
+    st_volatile_u64(&st.status[tile], lb_pack(st.epoch, 2u, exclusive + aggregate));
+  return exclusive;
+}
+
+// ---------------------------------------------------------------------------
+// Grid barrier for cooperative launches (all CTAs co-resident).  Bounded: a
+// CTA that waits too long records kDevErrTimeout, raises the abort word and
+// returns false; callers then leave the kernel.
+// ---------------------------------------------------------------------------
+struct GridBarrier {
+  unsigned* count;
+  unsigned* generation;
+  int* abort_flag;
+};
+
+__device__ __forceinline__ bool grid_sync(const GridBarrier& b, int* err) {
+  __shared__ int s_ok;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int ok = 1;
+    unsigned gen = *(volatile unsigned*)b.generation;
+    __threadfence();
+    unsigned arrived = atomicAdd(b.count, 1u);
+    if (arrived == gridDim.x - 1) {
+      *(volatile unsigned*)b.count = 0u;
+      __threadfence();
+      atomicAdd(b.generation, 1u);
+    } else {
+      long long spins = 0;
+      while (*(volatile unsigned*)b.generation == gen) {
+        if (*(volatile int*)b.abort_flag) { ok = 0; break; }
+        if (++spins > kSpinLimit) {
+          flag_error(err, kDevErrTimeout);
+          atomicExch(b.abort_flag, 1);
+          ok = 0;
+          break;
+        }
+        __nanosleep(64);
+      }
+    }
+    __threadfence();
+    if (*(volatile int*)b.abort_flag) ok = 0;
+    s_ok = ok;
+  }
+  __syncthreads();
+  return s_ok != 0;
+}
+
+}  // namespace spmx

@@ -1,0 +1,313 @@
+// CSC SpMSpV kernels: y = alpha * A * x with x sparse (x_key, x_val).
+//
+// Stage 1, csc_scan_kernel: gathers the length of every selected column
+//   (colptr[k+1]-colptr[k]), scans them into offsets in one pass (decoupled
+//   look-back with status words, bounded waits) and, fused into the same pass,
+//   writes the block-start tables of both load-balanced partitions.  This
+//   replaces scanFuseKernel + DetermineBlockStarts / my_KernelMergePartition
+//   (DEV/scan_kernel.cuh:12-143, DEV/csc_two_layer_load_balance.cuh:576,
+//   DEV/csc_sort_load_balance.cuh:295) whose look-back spins without bound on
+//   `sum[gid-1]==0` (scan_kernel.cuh:99).
+//
+// Stage 2, csc_lb_kernel: persistent CTAs take blocks of 2048 work items.
+//   "twolayer" blocks hold 2048 nonzeros (DEV/csc_two_layer_load_balance_
+//   fuse_reduction_modify.cuh:155); "merge" blocks hold 2048 merge-path items
+//   = nonzeros + column ends (DEV/csc_sort_load_balance_fuse_reduction_
+//   modify.cuh:7), which bounds the number of x entries per block.  Inside a
+//   block the owner entry of every item comes from a max-scan over entry-start
+//   marks in shared memory (no per-item search), and consecutive threads read
+//   consecutive nonzeros of a column.
+//
+// naive: a group of G lanes per x entry walks its column (ExtractFuseKernel,
+//   DEV/csc_sort_spmspv.cuh:98-119, is G = 1).
+#include "kernels.h"
+#include "common.cuh"
+
+namespace spmx {
+
+template <int NT, int VT>
+__global__ void __launch_bounds__(NT)
+csc_scan_kernel(CscArgs a, CscScratch s, LookbackState st, int ntiles, int K) {
+  __shared__ int s_len[NT * VT];
+  __shared__ unsigned s_wtmp[NT / 32 + 1];
+  __shared__ int s_tile;
+  __shared__ unsigned s_prefix;
+  const int tile = lb_acquire_tile(st, ntiles, &s_tile);
+  const int base = tile * NT * VT;
+  const int tid = threadIdx.x;
+#pragma unroll
+  for (int j = 0; j < VT; ++j) {
+    const int i = base + j * NT + tid;
+    int len = 0;
+    if (i < a.x_nnz) {
+      const int key = __ldg(a.x_key + i);
+      int cs = 0;
+      if ((unsigned)key >= (unsigned)a.n) {
+        flag_error(a.err, kDevErrOob);
+      } else {
+        cs = __ldg(a.colptr + key);
+        len = __ldg(a.colptr + key + 1) - cs;
+      }
+      s.colstart[i] = cs;
+    }
+    s_len[j * NT + tid] = len;
+  }
+  __syncthreads();
+  unsigned lens[VT];
+  unsigned sum = 0;
+#pragma unroll
+  for (int j = 0; j < VT; ++j) { lens[j] = (unsigned)s_len[tid * VT + j]; sum += lens[j]; }
+  unsigned total;
+  const unsigned ex = block_exclusive_sum<NT>(sum, s_wtmp, &total);
+  if (tid < 32) {
+    const unsigned p = lb_warp_lookback(st, tile, total, a.err);
+    if (tid == 0) s_prefix = p;
+  }
+  __syncthreads();
+  unsigned prefix = s_prefix + ex;
+#pragma unroll
+  for (int j = 0; j < VT; ++j) {
+    const int i = base + tid * VT + j;
+    if (i < a.x_nnz) {
+      s.off[i] = (int)prefix;
+      const long long p = prefix, len = lens[j];
+      if (len > 0) {
+        for (long long b = (p + K - 1) / K; b * K < p + len; ++b) {
+          if (b < s.tl_cap) s.bstart_tl[b] = i; else flag_error(a.err, kDevErrCapacity);
+        }
+      }
+      const long long lo = p + i, hi = p + len + i + 1;
+      for (long long b = (lo + K - 1) / K; b * K < hi; ++b) {
+        if (b < s.mg_cap) s.bstart_mg[b] = i; else flag_error(a.err, kDevErrCapacity);
+      }
+      prefix += lens[j];
+    }
+  }
+  if (tile == ntiles - 1 && tid == 0) {
+    const long long bl = (long long)s_prefix + total;
+    s.off[a.x_nnz] = (int)bl;
+    a.counts[kCntBinlen] = (int)bl;
+    a.counts[kCntBlocksTL] = (int)((bl + K - 1) / K);
+    a.counts[kCntBlocksMG] = (int)((bl + a.x_nnz + K - 1) / K);
+  }
+}
+
+template <int NT, int VT, bool PAIRS>
+__global__ void __launch_bounds__(NT)
+csc_lb_kernel(CscArgs a, CscScratch s, int variant, float* __restrict__ y,
+              int* __restrict__ prow, float* __restrict__ pval) {
+  constexpr int K = NT * VT;
+  constexpr int CAP = K + 1;
+  __shared__ int s_off[CAP];
+  __shared__ int s_cs[CAP];
+  __shared__ float s_xv[CAP];
+  __shared__ int s_mark[K];
+  __shared__ int s_incl[NT];
+  __shared__ int s_wtmp[NT / 32 + 1];
+  const int tid = threadIdx.x;
+  const int bin_len = a.counts[kCntBinlen];
+  int nblocks = a.counts[variant == 1 ? kCntBlocksMG : kCntBlocksTL];
+  const int* bstart = variant == 1 ? s.bstart_mg : s.bstart_tl;
+  const int cap = variant == 1 ? s.mg_cap : s.tl_cap;
+  if (nblocks > cap) {  // only with duplicate x keys (bin_len > nnz)
+    if (blockIdx.x == 0 && threadIdx.x == 0) flag_error(a.err, kDevErrCapacity);
+    nblocks = cap;
+  }
+  const int x_nnz = a.x_nnz;
+
+  for (int b = blockIdx.x; b < nblocks; b += gridDim.x) {
+    const int i0 = bstart[b];
+    int i1, k0, k1;
+    if (variant == 1) {
+      const long long d0 = (long long)b * K;
+      const long long d1 = min(d0 + K, (long long)bin_len + x_nnz);
+      k0 = (int)(d0 - i0);
+      if (b + 1 < nblocks) { i1 = bstart[b + 1]; k1 = (int)(d1 - i1); }
+      else { i1 = x_nnz - 1; k1 = bin_len; }
+    } else {
+      k0 = b * K;
+      k1 = min(k0 + K, bin_len);
+      i1 = (b + 1 < nblocks) ? bstart[b + 1] : x_nnz - 1;
+    }
+    const int ne = i1 - i0 + 1;
+    const int nk = k1 - k0;
+    if (ne <= CAP) {
+      for (int e = tid; e < ne; e += NT) {
+        s_off[e] = __ldg(s.off + i0 + e);
+        s_cs[e] = __ldg(s.colstart + i0 + e);
+        s_xv[e] = (float)(a.alpha * (double)__ldg(a.x_val + i0 + e));
+      }
+      for (int q = tid; q < K; q += NT) s_mark[q] = -1;
+      __syncthreads();
+      for (int e = tid; e < ne; e += NT) {
+        const int p = s_off[e] - k0;
+        if (p >= 0 && p < nk) atomicMax(&s_mark[p], e);
+      }
+      __syncthreads();
+      int loc[VT];
+      int run = INT_MIN;
+#pragma unroll
+      for (int j = 0; j < VT; ++j) {
+        const int q = tid * VT + j;
+        int v = s_mark[q];
+        if (q == 0) v = max(v, 0);
+        run = max(run, v);
+        loc[j] = run;
+      }
+      const int inc = block_inclusive_max<NT>(run, s_wtmp);
+      s_incl[tid] = inc;
+      __syncthreads();
+      const int carry = tid ? s_incl[tid - 1] : INT_MIN;
+#pragma unroll
+      for (int j = 0; j < VT; ++j) s_mark[tid * VT + j] = max(loc[j], carry);
+      __syncthreads();
+#pragma unroll
+      for (int j = 0; j < VT; ++j) {
+        const int q = j * NT + tid;
+        if (q < nk) {
+          const int e = s_mark[q];
+          const int k = k0 + q;
+          const int pos = s_cs[e] + (k - s_off[e]);
+          const int r = __ldg(a.row + pos);
+          const float v = __ldg(a.val + pos) * s_xv[e];
+          if (PAIRS) {
+            prow[k] = r;
+            pval[k] = v;
+          } else if ((unsigned)r < (unsigned)a.m) {
+            atomicAdd(y + r, v);
+          } else {
+            flag_error(a.err, kDevErrOob);
+          }
+        }
+      }
+    } else {
+      // many empty columns inside one block (twolayer only): search in global
+      for (int q = tid; q < nk; q += NT) {
+        const int k = k0 + q;
+        int lo = i0, hi = i1;  // last i in [i0, i1] with off[i] <= k
+        while (lo < hi) {
+          const int mid = (lo + hi + 1) >> 1;
+          if (__ldg(s.off + mid) <= k) lo = mid; else hi = mid - 1;
+        }
+        const int pos = __ldg(s.colstart + lo) + (k - __ldg(s.off + lo));
+        const int r = __ldg(a.row + pos);
+        const float v = __ldg(a.val + pos) * (float)(a.alpha * (double)__ldg(a.x_val + lo));
+        if (PAIRS) {
+          prow[k] = r;
+          pval[k] = v;
+        } else if ((unsigned)r < (unsigned)a.m) {
+          atomicAdd(y + r, v);
+        } else {
+          flag_error(a.err, kDevErrOob);
+        }
+      }
+    }
+    __syncthreads();
+  }
+}
+
+template <int G>
+__global__ void __launch_bounds__(256)
+csc_naive_kernel(CscArgs a, float* __restrict__ y) {
+  const long long gid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = (int)(gid / G);
+  const int g = (int)(gid % G);
+  if (i >= a.x_nnz) return;
+  const int key = __ldg(a.x_key + i);
+  if ((unsigned)key >= (unsigned)a.n) { if (g == 0) flag_error(a.err, kDevErrOob); return; }
+  const int cs = __ldg(a.colptr + key), ce = __ldg(a.colptr + key + 1);
+  const float xv = (float)(a.alpha * (double)__ldg(a.x_val + i));
+#pragma unroll 4
+  for (int k = cs + g; k < ce; k += G) {
+    const int r = __ldg(a.row + k);
+    if ((unsigned)r < (unsigned)a.m) atomicAdd(y + r, __ldg(a.val + k) * xv);
+    else flag_error(a.err, kDevErrOob);
+  }
+}
+
+template <int G>
+__global__ void __launch_bounds__(256)
+csc_naive_pairs_kernel(CscArgs a, CscScratch s, int* __restrict__ prow,
+                       float* __restrict__ pval) {
+  const long long gid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = (int)(gid / G);
+  const int g = (int)(gid % G);
+  if (i >= a.x_nnz) return;
+  const int cs = __ldg(s.colstart + i);
+  const int o = __ldg(s.off + i);
+  const int len = __ldg(s.off + i + 1) - o;
+  const float xv = (float)(a.alpha * (double)__ldg(a.x_val + i));
+  for (int q = g; q < len; q += G) {
+    prow[o + q] = __ldg(a.row + cs + q);
+    pval[o + q] = __ldg(a.val + cs + q) * xv;
+  }
+}
+
+// --------------------------------------------------------------------------
+int launch_csc_scan(const CscArgs& a, const CscScratch& s, ScanScratch& ls,
+                    int block_items, cudaStream_t st) {
+  constexpr int NT = kCscScanNT, VT = kCscScanVT;
+  const int ntiles = (a.x_nnz + NT * VT - 1) / (NT * VT);
+  if (ntiles <= 0) return 0;
+  if (ntiles > ls.status_len) return -1;
+  LookbackState lbs{ls.status, ls.ticket, ++ls.epoch};
+  note_launch();
+  csc_scan_kernel<NT, VT><<<ntiles, NT, 0, st>>>(a, s, lbs, ntiles, block_items);
+  return 0;
+}
+
+int launch_csc_lb(const CscArgs& a, const CscScratch& s, int variant, float* y,
+                  int* pairs_row, float* pairs_val, int grid, cudaStream_t st) {
+  constexpr int NT = kCscLbNT, VT = kCscLbVT;
+  if (a.x_nnz <= 0 || grid <= 0) return 0;
+  note_launch();
+  if (pairs_row)
+    csc_lb_kernel<NT, VT, true><<<grid, NT, 0, st>>>(a, s, variant, y, pairs_row, pairs_val);
+  else
+    csc_lb_kernel<NT, VT, false><<<grid, NT, 0, st>>>(a, s, variant, y, pairs_row, pairs_val);
+  return 0;
+}
+
+#define SPMX_GROUP_SWITCH(G_, BODY)                                              \
+  switch (G_) {                                                                 \
+    case 1: { constexpr int G = 1; BODY; break; }                               \
+    case 2: { constexpr int G = 2; BODY; break; }                               \
+    case 4: { constexpr int G = 4; BODY; break; }                               \
+    case 8: { constexpr int G = 8; BODY; break; }                               \
+    case 16: { constexpr int G = 16; BODY; break; }                             \
+    case 32: { constexpr int G = 32; BODY; break; }                             \
+    default: return -1;                                                         \
+  }
+
+int launch_csc_naive(const CscArgs& a, int group, float* y, cudaStream_t st) {
+  if (a.x_nnz <= 0) return 0;
+  const long long threads = (long long)a.x_nnz * group;
+  const unsigned grid = (unsigned)((threads + 255) / 256);
+  note_launch();
+  SPMX_GROUP_SWITCH(group, (csc_naive_kernel<G><<<grid, 256, 0, st>>>(a, y)));
+  return 0;
+}
+
+int launch_csc_naive_pairs(const CscArgs& a, const CscScratch& s, int group,
+                           int* pairs_row, float* pairs_val, cudaStream_t st) {
+  if (a.x_nnz <= 0) return 0;
+  const long long threads = (long long)a.x_nnz * group;
+  const unsigned grid = (unsigned)((threads + 255) / 256);
+  note_launch();
+  SPMX_GROUP_SWITCH(group, (csc_naive_pairs_kernel<G><<<grid, 256, 0, st>>>(a, s, pairs_row, pairs_val)));
+  return 0;
+}
+
+}  // namespace spmx
+
+namespace spmx {
+int csc_lb_blocks_per_sm() {
+  int b = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+          &b, csc_lb_kernel<kCscLbNT, kCscLbVT, false>, kCscLbNT, 0) != cudaSuccess) {
+    cudaGetLastError();
+    return 2;
+  }
+  return b > 0 ? b : 1;
+}
+}  // namespace spmx

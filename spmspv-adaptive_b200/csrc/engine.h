@@ -1,0 +1,105 @@
+// The handle behind the C ABI (spmx.h).  Host-side state of one matrix: the
+// borrowed CSR, the CSC (owned after spmx_to_csc), the current x in its
+// sparse / dense / bitarray forms, the scratch of every kernel family, cached
+// features and tuned launch parameters.  Mirrors the members of
+// SpmspvHandle (H:246-344).
+#pragma once
+#include <cuda_runtime.h>
+#include <string>
+#include "spmx.h"
+#include "kernels.h"
+#include "sort.h"
+
+struct spmx_handle_s {
+  int m = 0, n = 0, nnz = 0;
+  int device = 0;
+  int num_sms = 148;
+  cudaStream_t stream = nullptr;
+
+  // CSR (borrowed)
+  const int* rowptr = nullptr;
+  const int* col = nullptr;
+  const float* val = nullptr;
+  bool has_csr = false;
+  // CSC (borrowed via input_csc or owned via to_csc)
+  const int* csc_colptr = nullptr;
+  const int* csc_row = nullptr;
+  const float* csc_val = nullptr;
+  bool has_csc = false;
+  int* own_colptr = nullptr;
+  int* own_row = nullptr;
+  float* own_cval = nullptr;
+
+  // x
+  float* x_dense = nullptr;
+  int* x_key = nullptr;
+  float* x_val = nullptr;
+  int x_nnz = 0;
+  int* bitvec = nullptr;
+  int num_ints = 0;
+  int vec_type = -1;
+  float* own_xdense = nullptr;
+  int* own_bits = nullptr;
+
+  int spmv_type = SPMX_SPMV_HOLA;
+  int sigma = -1;
+
+  // device counters, error word, feature accumulators
+  int* d_counts = nullptr;         // spmx::kCntTotal ints
+  int* d_err = nullptr;            // sticky error bits
+  double* d_facc = nullptr;        // 4 doubles
+  int* d_iacc = nullptr;           // 4 ints
+  unsigned long long* d_u64 = nullptr;  // 4 words
+  int* h_pinned = nullptr;         // 16 ints of pinned host memory
+
+  spmx::ScanScratch ls{};          // look-back status + ticket
+
+  // CSC SpMSpV scratch
+  spmx::CscScratch cs{};
+  bool cs_ready = false;
+  // sort write-back scratch (pairs + radix)
+  unsigned* sk = nullptr;
+  unsigned* sk_alt = nullptr;
+  unsigned* sv = nullptr;
+  unsigned* sv_alt = nullptr;
+  int* shist = nullptr;
+  int* shist_off = nullptr;
+  int* sslot = nullptr;
+  int* sy_key = nullptr;      // internal sparse y (adaptive path)
+  float* sy_val = nullptr;
+  bool sort_ready = false;
+
+  // Hola tables
+  spmx::HolaTables hola{};
+  bool hola_ready = false;
+
+  // tuned parameters
+  int naive_row_group = 0;    // 0 = derive from mean row length
+  int naive_col_group = 0;    // 0 = derive from mean column length
+  int hola_vt = 8;
+  int lb_variant = SPMX_CSC_LB_MERGE;
+  int lb_grid = 0;
+
+  // cached features
+  bool mat_feat_ready = false;
+  double mat_feat[10] = {0};
+  bool std_row_ready = false;
+  float std_row = 0.f;
+  long long bin_len = -1;
+  long long vec_max = 0, vec_min = 0;
+  double gm[3] = {-1, -1, -1};
+
+  // BFS buffers
+  unsigned* bfs_visited = nullptr;
+  unsigned* bfs_front = nullptr;
+  int* bfs_q[2] = {nullptr, nullptr};
+  int* bfs_cnt = nullptr;                  // [0..1] queue counts
+  unsigned long long* bfs_edges = nullptr; // [0..1]
+  int bfs_n = 0;
+};
+
+namespace spmx {
+int set_error(int code, const std::string& msg);
+int dalloc(void** p, size_t bytes, const char* what);
+void dfree(void* p);
+}  // namespace spmx

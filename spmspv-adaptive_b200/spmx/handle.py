@@ -1,0 +1,338 @@
+"""SpmspvHandle: the reference's engine handle, over the spmx C ABI.
+
+Method names, argument meaning and ownership follow SpmspvHandle<int,
+unsigned, float> (hice-spmspv/hice/la/include/spmspv/csc-spmspv/spmspv.h,
+H:88-344): CSR and x buffers are caller-owned device tensors (the handle keeps
+a reference so they outlive it), CSC / Hola / CSR5 tables and scratch belong
+to the handle.  Differences from the reference:
+
+- methods return None and raise SpmxError on failure (the reference returns
+  SPMSPV_* codes, prints, or exits);
+- y_nnz outputs are returned as Python ints;
+- alpha scales the result (y = alpha*A*x), as the reference's CPU
+  serialspmv does; its GPU kernels ignore alpha, which coincides for 1.0.
+
+All tensors must be CUDA tensors: int32 indices, float32 values.  Work runs on
+torch's current CUDA stream at construction time (set_stream changes it).
+"""
+import ctypes
+
+import torch
+
+from . import _lib
+from ._lib import lib, check, c_int, c_ll, c_double, c_float, c_void_p
+
+
+def _ptr(t):
+    if t is None:
+        return None
+    if not isinstance(t, torch.Tensor):
+        raise TypeError("expected a torch tensor")
+    if not t.is_cuda:
+        raise ValueError("expected a CUDA tensor")
+    if not t.is_contiguous():
+        raise ValueError("expected a contiguous tensor")
+    return t.data_ptr()
+
+
+def _i32(t):
+    if t is not None and t.dtype != torch.int32:
+        raise TypeError("index tensors must be int32")
+    return _ptr(t)
+
+
+def _f32(t):
+    if t is not None and t.dtype != torch.float32:
+        raise TypeError("value tensors must be float32")
+    return _ptr(t)
+
+
+class SpmspvHandle:
+    def __init__(self, m, n, nnz, stream=None):
+        h = c_void_p()
+        check(lib.spmx_create(int(m), int(n), int(nnz), ctypes.byref(h)), "create")
+        self._h = h
+        self.m, self.n, self.nnz = int(m), int(n), int(nnz)
+        self._keep = {}
+        s = stream if stream is not None else torch.cuda.current_stream()
+        self.set_stream(s)
+
+    # -- lifecycle -----------------------------------------------------------
+    def set_stream(self, stream):
+        self._stream = stream
+        check(lib.spmx_set_stream(self._h, stream.cuda_stream), "set_stream")
+
+    def warmup(self):
+        check(lib.spmx_warmup(self._h), "warmup")
+
+    def Destroy(self):
+        if getattr(self, "_h", None) is not None and self._h.value:
+            lib.spmx_destroy(self._h)
+            self._h = c_void_p()
+        self._keep = {}
+
+    def __del__(self):
+        try:
+            self.Destroy()
+        except Exception:
+            pass
+
+    def check_device_error(self):
+        check(lib.spmx_check_device_error(self._h), "device")
+
+    @property
+    def raw(self):
+        """The C handle (for callers that use the C ABI directly)."""
+        return self._h
+
+    # -- matrix --------------------------------------------------------------
+    def InputCSR(self, nnz, csr_row, csr_col, csr_val=None):
+        check(lib.spmx_input_csr(self._h, int(nnz), _i32(csr_row), _i32(csr_col), _f32(csr_val)),
+              "InputCSR")
+        self._keep["csr"] = (csr_row, csr_col, csr_val)
+
+    def InputCSC(self, nnz, csc_row, csc_col, csc_val=None):
+        check(lib.spmx_input_csc(self._h, int(nnz), _i32(csc_row), _i32(csc_col), _f32(csc_val)),
+              "InputCSC")
+        self._keep["csc"] = (csc_row, csc_col, csc_val)
+
+    def ToCSC(self):
+        check(lib.spmx_to_csc(self._h), "ToCSC")
+
+    def get_csc(self):
+        """(row[nnz], colptr[n+1], val[nnz] or None) as new tensors."""
+        r, c, v = c_void_p(), c_void_p(), c_void_p()
+        check(lib.spmx_get_csc(self._h, ctypes.byref(r), ctypes.byref(c), ctypes.byref(v)), "get_csc")
+        torch.cuda.synchronize()
+        return (_copy_dev(r.value, self.nnz, torch.int32), _copy_dev(c.value, self.n + 1, torch.int32),
+                _copy_dev(v.value, self.nnz, torch.float32) if v.value else None)
+
+    # -- vectors -------------------------------------------------------------
+    def set_x(self, x):
+        check(lib.spmx_set_x(self._h, _f32(x)), "set_x")
+        self._keep["x"] = x
+
+    def set_sparse_x(self, x_key, x_val, xnnz):
+        check(lib.spmx_set_sparse_x(self._h, _i32(x_key), _f32(x_val), int(xnnz)), "set_sparse_x")
+        self._keep["xs"] = (x_key, x_val)
+
+    def set_bitvector(self, bitvector, num_ints):
+        check(lib.spmx_set_bitvector(self._h, _i32(bitvector), int(num_ints)), "set_bitvector")
+        self._keep["bits"] = bitvector
+
+    def set_sparse_x_dense_x(self, x_key, x_val, x_dense, xnnz):
+        check(lib.spmx_set_sparse_x_dense_x(self._h, _i32(x_key), _f32(x_val), _f32(x_dense),
+                                            int(xnnz)), "set_sparse_x_dense_x")
+        self._keep["xs"] = (x_key, x_val)
+        self._keep["x"] = x_dense
+
+    def set_vector_type(self, code):
+        check(lib.spmx_set_vector_type(self._h, int(code)), "set_vector_type")
+
+    def sparse2dense(self):
+        check(lib.spmx_sparse2dense(self._h), "sparse2dense")
+
+    def sparse2bitarray(self):
+        check(lib.spmx_sparse2bitarray(self._h), "sparse2bitarray")
+
+    def dense2sparse(self):
+        n = c_int()
+        check(lib.spmx_dense2sparse(self._h, ctypes.byref(n)), "dense2sparse")
+        return n.value
+
+    def bitarray2sparse(self):
+        n = c_int()
+        check(lib.spmx_bitarray2sparse(self._h, ctypes.byref(n)), "bitarray2sparse")
+        return n.value
+
+    def dense2bitarray(self):
+        check(lib.spmx_dense2bitarray(self._h), "dense2bitarray")
+
+    def dense2sparse_outer(self, m, d_dense, d_key, d_val):
+        n = c_int()
+        check(lib.spmx_dense2sparse_outer(self._h, int(m), _f32(d_dense), ctypes.byref(n),
+                                          _i32(d_key), _f32(d_val)), "dense2sparse_outer")
+        return n.value
+
+    def sparse2dense_outer(self, ynnz, d_key, d_val, m, d_dense):
+        check(lib.spmx_sparse2dense_outer(self._h, int(ynnz), _i32(d_key), _f32(d_val), int(m),
+                                          _f32(d_dense)), "sparse2dense_outer")
+
+    # -- scratch / preprocess ----------------------------------------------------
+    def allocPreBuffer(self):
+        check(lib.spmx_alloc_pre_buffer(self._h), "allocPreBuffer")
+
+    def deallocPreBuffer(self):
+        check(lib.spmx_dealloc_pre_buffer(self._h), "deallocPreBuffer")
+
+    def holaPreprocess(self):
+        check(lib.spmx_hola_preprocess(self._h), "holaPreprocess")
+
+    def holaPostprocess(self):
+        check(lib.spmx_hola_postprocess(self._h), "holaPostprocess")
+
+    def setSigma(self, sigma):
+        check(lib.spmx_set_sigma(self._h, int(sigma)), "setSigma")
+
+    def CSR5Preprocess(self):
+        check(lib.spmx_csr5_preprocess(self._h), "CSR5Preprocess")
+
+    def CSR5Postprocess(self):
+        check(lib.spmx_csr5_postprocess(self._h), "CSR5Postprocess")
+
+    def set_spmv_type(self, code):
+        check(lib.spmx_set_spmv_type(self._h, int(code)), "set_spmv_type")
+
+    # -- SpMV / CSR SpMSpV ---------------------------------------------------------
+    def naivespmv(self, alpha, y):
+        check(lib.spmx_naivespmv(self._h, float(alpha), _f32(y)), "naivespmv")
+
+    def holaspmv(self, alpha, y):
+        check(lib.spmx_holaspmv(self._h, float(alpha), _f32(y)), "holaspmv")
+
+    def csr5spmv(self, alpha, y):
+        check(lib.spmx_csr5spmv(self._h, float(alpha), _f32(y)), "csr5spmv")
+
+    def naivespmspv(self, alpha, y):
+        check(lib.spmx_naivespmspv(self._h, float(alpha), _f32(y)), "naivespmspv")
+
+    def holaspmspv(self, alpha, y):
+        check(lib.spmx_holaspmspv(self._h, float(alpha), _f32(y)), "holaspmspv")
+
+    def csr5spmspv(self, alpha, y):
+        check(lib.spmx_csr5spmspv(self._h, float(alpha), _f32(y)), "csr5spmspv")
+
+    def spmv(self, alpha, y):
+        check(lib.spmx_spmv(self._h, float(alpha), _f32(y)), "spmv")
+
+    def spmspv(self, alpha, y):
+        check(lib.spmx_spmspv(self._h, float(alpha), _f32(y)), "spmspv")
+
+    # -- CSC SpMSpV (reference names) --------------------------------------------------
+    def spmspv_csc(self, variant, writeback, alpha, y=None, y_key=None, y_val=None, sync=True):
+        n = c_int()
+        check(lib.spmx_spmspv_csc(self._h, int(variant), int(writeback), float(alpha), _f32(y),
+                                  _i32(y_key), _f32(y_val), ctypes.byref(n) if sync else None),
+              "spmspv_csc")
+        return n.value if sync else None
+
+    def CscBasedNoSortNaiveSpmspv(self, alpha, y):
+        n = c_int()
+        check(lib.spmx_csc_naive_atomic(self._h, float(alpha), ctypes.byref(n), _f32(y)),
+              "CscBasedNoSortNaiveSpmspv")
+        return n.value
+
+    def CscBasedNoSortNaiveSpmspv_keyval(self, alpha, y, y_key, y_val):
+        n = c_int()
+        check(lib.spmx_csc_naive_atomic_keyval(self._h, float(alpha), ctypes.byref(n), _f32(y),
+                                               _i32(y_key), _f32(y_val)),
+              "CscBasedNoSortNaiveSpmspv_keyval")
+        return n.value
+
+    def CscBasedSortNaiveSpmspv(self, alpha, y_key, y_val):
+        n = c_int()
+        check(lib.spmx_csc_naive_sort(self._h, float(alpha), ctypes.byref(n), _i32(y_key),
+                                      _f32(y_val)), "CscBasedSortNaiveSpmspv")
+        return n.value
+
+    def _lb(self, fn, name, alpha, y, y_key, y_val):
+        n = c_int()
+        check(fn(self._h, 1, float(alpha), ctypes.byref(n), _f32(y), _i32(y_key), _f32(y_val)), name)
+        return n.value
+
+    def CscBasedNoSortMergeSpmspv(self, IsBinLenComputed, alpha, y, y_key=None, y_val=None):
+        return self._lb(lib.spmx_csc_merge_atomic, "CscBasedNoSortMergeSpmspv", alpha, y, None, None)
+
+    def CscBasedNoSortMergeSpmspv_keyval(self, IsBinLenComputed, alpha, y, y_key, y_val):
+        return self._lb(lib.spmx_csc_merge_atomic_keyval, "CscBasedNoSortMergeSpmspv_keyval",
+                        alpha, y, y_key, y_val)
+
+    def CscBasedSortMergeSpmspv(self, IsBinLenComputed, alpha, y, y_key, y_val):
+        return self._lb(lib.spmx_csc_merge_sort, "CscBasedSortMergeSpmspv", alpha, y, y_key, y_val)
+
+    def CscBasedMyNoSortSpmspv(self, IsBinLenComputed, alpha, y, y_key=None, y_val=None):
+        return self._lb(lib.spmx_csc_twolayer_atomic, "CscBasedMyNoSortSpmspv", alpha, y, None, None)
+
+    def CscBasedMyNoSortSpmspv_keyval(self, IsBinLenComputed, alpha, y, y_key, y_val):
+        return self._lb(lib.spmx_csc_twolayer_atomic_keyval, "CscBasedMyNoSortSpmspv_keyval",
+                        alpha, y, y_key, y_val)
+
+    def CscBasedSortMySpmspv(self, IsBinLenComputed, alpha, y, y_key, y_val):
+        return self._lb(lib.spmx_csc_twolayer_sort, "CscBasedSortMySpmspv", alpha, y, y_key, y_val)
+
+    def CscBasedBucketSpmspv(self, alpha, y=None, y_key=None, y_val=None, buckets=0):
+        n = c_int()
+        check(lib.spmx_csc_bucket(self._h, float(alpha), ctypes.byref(n), _f32(y), _i32(y_key),
+                                  _f32(y_val), int(buckets)), "CscBasedBucketSpmspv")
+        return n.value
+
+    # -- features / selector -------------------------------------------------------------
+    def computeBinlenVer2(self):
+        v = c_ll()
+        check(lib.spmx_compute_binlen(self._h, ctypes.byref(v)), "computeBinlenVer2")
+        return v.value
+
+    def computeGM(self):
+        gm = (c_double * 3)()
+        check(lib.spmx_compute_gm(self._h, gm), "computeGM")
+        return list(gm)
+
+    def computeGM1(self):
+        return self.computeGM()[0]
+
+    def computeGM2(self):
+        return self.computeGM()[1]
+
+    def computeGM3(self):
+        return self.computeGM()[2]
+
+    def computeMatFeture(self):
+        """{m, n, nnz, max, min, avg, range, stdRow, edge_equlity, gini}"""
+        out = (c_double * 10)()
+        check(lib.spmx_mat_features(self._h, out), "computeMatFeture")
+        return list(out)
+
+    def extractMatFeatureParallel(self):
+        v = c_float()
+        check(lib.spmx_std_row(self._h, ctypes.byref(v)), "extractMatFeatureParallel")
+        return v.value
+
+    def computeVecFeture(self):
+        """(bin_len, max, min) of the column lengths of x's keys"""
+        out = (c_ll * 3)()
+        check(lib.spmx_vec_features(self._h, out), "computeVecFeture")
+        return tuple(out)
+
+    def features(self):
+        out = (c_double * _lib.NUM_FEATURES)()
+        check(lib.spmx_features(self._h, out), "features")
+        return dict(zip(_lib.FEATURE_NAMES, list(out)))
+
+    def select(self):
+        k = c_int()
+        check(lib.spmx_select(self._h, ctypes.byref(k)), "select")
+        return k.value
+
+    def run_adaptive(self, alpha, y):
+        k = c_int()
+        check(lib.spmx_run_adaptive(self._h, float(alpha), _f32(y), ctypes.byref(k)), "run_adaptive")
+        return k.value
+
+    def run_kernel(self, kid, alpha, y):
+        check(lib.spmx_run_kernel(self._h, int(kid), float(alpha), _f32(y)), "run_kernel")
+
+    # -- BFS ---------------------------------------------------------------------------
+    def bfs(self, source, levels):
+        d = c_int()
+        check(lib.spmx_bfs(self._h, int(source), _i32(levels), ctypes.byref(d)), "bfs")
+        return d.value
+
+
+def _copy_dev(ptr, count, dtype):
+    """Copy `count` elements at device address `ptr` into a new tensor."""
+    out = torch.empty(count, dtype=dtype, device="cuda")
+    if count:
+        nbytes = count * torch.tensor([], dtype=dtype).element_size()
+        cudart = torch.cuda.cudart()
+        cudart.cudaMemcpy(out.data_ptr(), ptr, nbytes, 3)  # device to device
+    return out
