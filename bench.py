@@ -422,6 +422,62 @@ def cpu_baseline(A, xs, binl):
             "ms": best * 1e3}
 
 
+ONLY = ("hola-spmv", "csr5-spmv", "naive-spmv", "hola-spmspv", "csc-lb-atomic", "csc-naive-atomic",
+        "csc-bucket", "csc-lb-sort", "bfs-rmat14")
+
+
+def run_only(args):
+    """One kernel on the benchmark workload, K+W launches, for profiling
+    (e.g. under ncu -k <kernel>); prints the mean time of the last K."""
+    import torch
+    import spmx
+    dev = torch.device("cuda", 0)
+    stream = torch.cuda.current_stream(dev)
+    if args.only == "bfs-rmat14":
+        print(json.dumps(run_bfs_plain(torch, dev, stream, args)))
+        return 0
+    A, xs = make_inputs()
+    d = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)  # noqa: E731
+    rp, cl, vl = d(A.rowptr), d(A.col), d(A.val)
+    h = spmx.SpmspvHandle(A.m, A.n, A.nnz, stream=stream)
+    h.InputCSR(A.nnz, rp, cl, vl)
+    h.ToCSC()
+    h.holaPreprocess()
+    h.CSR5Preprocess()
+    h.allocPreBuffer()
+    dens = 1.0 if args.only.endswith("spmv") else args.density
+    k = [x for x in xs if abs(x[0] - dens) < 1e-12][0]
+    kd, vd = d(k[1]), d(k[2])
+    h.set_sparse_x(kd, vd, len(k[1]))
+    h.sparse2bitarray()
+    y = torch.empty(A.m, device=dev)
+    yk = torch.empty(A.m, dtype=torch.int32, device=dev)
+    yv = torch.empty(A.m, device=dev)
+    run = {
+        "hola-spmv": lambda: h.holaspmv(1.0, y),
+        "csr5-spmv": lambda: h.csr5spmv(1.0, y),
+        "naive-spmv": lambda: h.naivespmv(1.0, y),
+        "hola-spmspv": lambda: h.holaspmspv(1.0, y),
+        "csc-lb-atomic": lambda: h.spmspv_csc(1, 0, 1.0, y, sync=False),
+        "csc-naive-atomic": lambda: h.spmspv_csc(0, 0, 1.0, y, sync=False),
+        "csc-bucket": lambda: h.CscBasedBucketSpmspv(1.0, y, yk, yv),
+        "csc-lb-sort": lambda: h.spmspv_csc(1, 1, 1.0, None, yk, yv),
+    }[args.only]
+    s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ts = []
+    for it in range(args.warmup + args.steps):
+        s.record(stream)
+        run()
+        e.record(stream)
+        stream.synchronize()
+        if it >= args.warmup:
+            ts.append(s.elapsed_time(e))
+    h.check_device_error()
+    print(json.dumps({"only": args.only, "density": dens, "ms": statistics.mean(ts),
+                      "min_ms": min(ts)}))
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -430,7 +486,11 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-bfs", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--only", choices=ONLY, help="run one kernel (profiling helper)")
+    ap.add_argument("--density", type=float, default=0.1)
     args = ap.parse_args()
+    if args.only:
+        return run_only(args)
     world, rank, local = dist_init(args)
     try:
         if args.impl == "reference":

@@ -170,6 +170,8 @@ int spmx_hola_postprocess(spmx_handle_t h);
 int spmx_set_sigma(spmx_handle_t h, int sigma);
 int spmx_csr5_preprocess(spmx_handle_t h);
 int spmx_csr5_postprocess(spmx_handle_t h);
+/* the sigma in use (after CSR5Preprocess) or that the auto rule would pick */
+int spmx_csr5_sigma(spmx_handle_t h, int* sigma);
 /* set_spmv_type — H:1767 (0 Hola, 1 CSR5) */
 int spmx_set_spmv_type(spmx_handle_t h, int code);
 

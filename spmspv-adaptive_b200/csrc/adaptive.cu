@@ -219,16 +219,33 @@ extern "C" int spmx_features(spmx_handle_t h, double out[SPMX_NUM_FEATURES]) {
 // ---------------------------------------------------------------------------
 // selector and the adaptive iteration
 // ---------------------------------------------------------------------------
+// longest column of the CSC (once per matrix): an upper bound of the longest
+// column any x selects
+static int compute_col_max(spmx_handle_t h) {
+  if (h->col_max >= 0) return SPMX_SUCCESS;
+  if (!h->has_csc) { h->col_max = 0; return SPMX_SUCCESS; }
+  cudaStream_t st = h->stream;
+  SPMX_CUDA(cudaMemsetAsync(h->d_facc, 0, sizeof(double) * 4, st));
+  SPMX_CUDA(cudaMemsetAsync(h->d_iacc, 0, sizeof(int) * 4, st));
+  launch_mat_features(h->n, h->csc_colptr, h->nnz, 0.0, 0.0, h->d_facc, h->d_iacc, st);
+  int iacc[4];
+  SPMX_CUDA(cudaMemcpyAsync(iacc, h->d_iacc, sizeof(iacc), cudaMemcpyDeviceToHost, st));
+  SPMX_CUDA(cudaStreamSynchronize(st));
+  h->col_max = h->n ? iacc[0] : 0;
+  return launch_ok("column features");
+}
+
 extern "C" int spmx_select(spmx_handle_t h, int* kernel_id) {
   SPMX_CHECK_HANDLE(h);
   if (!kernel_id) return set_error(SPMX_ERR_INVALID_VALUE, "kernel_id is NULL");
   SPMX_TRY(compute_mat_features(h));
+  SPMX_TRY(compute_col_max(h));
   double f[SPMX_NUM_FEATURES];
   const double est = h->bin_len >= 0 ? (double)h->bin_len
                                       : (h->n ? (double)h->x_nnz * h->nnz / h->n : 0.0);
-  // the maximum / minimum column length of x are not known without a device
-  // pass; the selector does not use them
-  fill_features(h, est, 0, 0, f);
+  // x's own longest / shortest column need a device pass; the matrix's
+  // longest column bounds the former, the latter is not used
+  fill_features(h, est, h->col_max, 0, f);
   *kernel_id = spmx_select_kernel(f);
   return SPMX_SUCCESS;
 }

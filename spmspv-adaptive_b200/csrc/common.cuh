@@ -80,6 +80,61 @@ __device__ __forceinline__ T block_exclusive_sum(T v, T* warp_tmp, T* total) {
   return ex;
 }
 
+// Segmented scan operator on (flag, value): a set flag starts a new segment.
+// combine(a, b) with a before b: (a.f | b.f, b.f ? b.v : a.v + b.v).
+// Block-wide EXCLUSIVE segmented scan over NT threads; returns the value of
+// the segment still open at the calling thread's start (0 for thread 0).
+// `tmp_f` / `tmp_v` hold NT/32 + 1 entries.
+template <int NT>
+__device__ __forceinline__ double block_exclusive_segscan(bool f, double v, int* tmp_f,
+                                                         double* tmp_v) {
+  constexpr int NW = NT / 32;
+  const int w = threadIdx.x >> 5;
+  const int lane = (int)lane_id();
+  // inclusive within the warp
+  int fi = f;
+  double vi = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int f2 = __shfl_up_sync(0xffffffffu, fi, o);
+    const double v2 = __shfl_up_sync(0xffffffffu, vi, o);
+    if (lane >= o) {
+      vi = fi ? vi : v2 + vi;
+      fi |= f2;
+    }
+  }
+  // exclusive within the warp
+  int fe = __shfl_up_sync(0xffffffffu, fi, 1);
+  double ve = __shfl_up_sync(0xffffffffu, vi, 1);
+  if (lane == 0) { fe = 0; ve = 0.0; }
+  if (lane == 31) { tmp_f[w] = fi; tmp_v[w] = vi; }
+  __syncthreads();
+  if (w == 0) {
+    int gf = lane < NW ? tmp_f[lane] : 0;
+    double gv = lane < NW ? tmp_v[lane] : 0.0;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int f2 = __shfl_up_sync(0xffffffffu, gf, o);
+      const double v2 = __shfl_up_sync(0xffffffffu, gv, o);
+      if (lane >= o) {
+        gv = gf ? gv : v2 + gv;
+        gf |= f2;
+      }
+    }
+    // exclusive over warps
+    int xf = __shfl_up_sync(0xffffffffu, gf, 1);
+    double xv = __shfl_up_sync(0xffffffffu, gv, 1);
+    if (lane == 0) { xf = 0; xv = 0.0; }
+    if (lane < NW) { tmp_f[lane] = xf; tmp_v[lane] = xv; }
+  }
+  __syncthreads();
+  // prefix of earlier warps, then this warp's exclusive part
+  const double wv = tmp_v[w];
+  const double res = fe ? ve : wv + ve;
+  __syncthreads();
+  return res;
+}
+
 // Block-wide inclusive max-scan of ints over NT threads.
 template <int NT>
 __device__ __forceinline__ int block_inclusive_max(int v, int* warp_tmp) {

@@ -22,6 +22,7 @@
 //   DEV/csc_sort_spmspv.cuh:98-119, is G = 1).
 #include "kernels.h"
 #include "common.cuh"
+#include "csc_lb.cuh"
 
 namespace spmx {
 
@@ -96,110 +97,21 @@ template <int NT, int VT, bool PAIRS>
 __global__ void __launch_bounds__(NT)
 csc_lb_kernel(CscArgs a, CscScratch s, int variant, float* __restrict__ y,
               int* __restrict__ prow, float* __restrict__ pval) {
-  constexpr int K = NT * VT;
-  constexpr int CAP = K + 1;
-  __shared__ int s_off[CAP];
-  __shared__ int s_cs[CAP];
-  __shared__ float s_xv[CAP];
-  __shared__ int s_mark[K];
-  __shared__ int s_incl[NT];
-  __shared__ int s_wtmp[NT / 32 + 1];
-  const int tid = threadIdx.x;
-  const int bin_len = a.counts[kCntBinlen];
-  int nblocks = a.counts[variant == 1 ? kCntBlocksMG : kCntBlocksTL];
-  const int* bstart = variant == 1 ? s.bstart_mg : s.bstart_tl;
-  const int cap = variant == 1 ? s.mg_cap : s.tl_cap;
-  if (nblocks > cap) {  // only with duplicate x keys (bin_len > nnz)
-    if (blockIdx.x == 0 && threadIdx.x == 0) flag_error(a.err, kDevErrCapacity);
-    nblocks = cap;
-  }
-  const int x_nnz = a.x_nnz;
-
+  __shared__ LbSmem<NT, VT> sh;
+  const int nblocks = lb_num_blocks(a, s, variant);
   for (int b = blockIdx.x; b < nblocks; b += gridDim.x) {
-    const int i0 = bstart[b];
-    int i1, k0, k1;
-    if (variant == 1) {
-      const long long d0 = (long long)b * K;
-      const long long d1 = min(d0 + K, (long long)bin_len + x_nnz);
-      k0 = (int)(d0 - i0);
-      if (b + 1 < nblocks) { i1 = bstart[b + 1]; k1 = (int)(d1 - i1); }
-      else { i1 = x_nnz - 1; k1 = bin_len; }
-    } else {
-      k0 = b * K;
-      k1 = min(k0 + K, bin_len);
-      i1 = (b + 1 < nblocks) ? bstart[b + 1] : x_nnz - 1;
-    }
-    const int ne = i1 - i0 + 1;
-    const int nk = k1 - k0;
-    if (ne <= CAP) {
-      for (int e = tid; e < ne; e += NT) {
-        s_off[e] = __ldg(s.off + i0 + e);
-        s_cs[e] = __ldg(s.colstart + i0 + e);
-        s_xv[e] = (float)(a.alpha * (double)__ldg(a.x_val + i0 + e));
-      }
-      for (int q = tid; q < K; q += NT) s_mark[q] = -1;
-      __syncthreads();
-      for (int e = tid; e < ne; e += NT) {
-        const int p = s_off[e] - k0;
-        if (p >= 0 && p < nk) atomicMax(&s_mark[p], e);
-      }
-      __syncthreads();
-      int loc[VT];
-      int run = INT_MIN;
-#pragma unroll
-      for (int j = 0; j < VT; ++j) {
-        const int q = tid * VT + j;
-        int v = s_mark[q];
-        if (q == 0) v = max(v, 0);
-        run = max(run, v);
-        loc[j] = run;
-      }
-      const int inc = block_inclusive_max<NT>(run, s_wtmp);
-      s_incl[tid] = inc;
-      __syncthreads();
-      const int carry = tid ? s_incl[tid - 1] : INT_MIN;
-#pragma unroll
-      for (int j = 0; j < VT; ++j) s_mark[tid * VT + j] = max(loc[j], carry);
-      __syncthreads();
-#pragma unroll
-      for (int j = 0; j < VT; ++j) {
-        const int q = j * NT + tid;
-        if (q < nk) {
-          const int e = s_mark[q];
-          const int k = k0 + q;
-          const int pos = s_cs[e] + (k - s_off[e]);
-          const int r = __ldg(a.row + pos);
-          const float v = __ldg(a.val + pos) * s_xv[e];
-          if (PAIRS) {
-            prow[k] = r;
-            pval[k] = v;
-          } else if ((unsigned)r < (unsigned)a.m) {
-            atomicAdd(y + r, v);
-          } else {
-            flag_error(a.err, kDevErrOob);
-          }
-        }
-      }
-    } else {
-      // many empty columns inside one block (twolayer only): search in global
-      for (int q = tid; q < nk; q += NT) {
-        const int k = k0 + q;
-        int lo = i0, hi = i1;  // last i in [i0, i1] with off[i] <= k
-        while (lo < hi) {
-          const int mid = (lo + hi + 1) >> 1;
-          if (__ldg(s.off + mid) <= k) lo = mid; else hi = mid - 1;
-        }
-        const int pos = __ldg(s.colstart + lo) + (k - __ldg(s.off + lo));
-        const int r = __ldg(a.row + pos);
-        const float v = __ldg(a.val + pos) * (float)(a.alpha * (double)__ldg(a.x_val + lo));
-        if (PAIRS) {
-          prow[k] = r;
-          pval[k] = v;
-        } else if ((unsigned)r < (unsigned)a.m) {
-          atomicAdd(y + r, v);
-        } else {
-          flag_error(a.err, kDevErrOob);
-        }
+    const LbBlock bl = lb_block_setup<NT, VT>(a, s, variant, b, nblocks, sh);
+    for (int q = threadIdx.x; q < bl.nk; q += NT) {
+      int k, r;
+      float v;
+      lb_item<NT, VT>(a, s, bl, sh, q, k, r, v);
+      if (PAIRS) {
+        prow[k] = r;
+        pval[k] = v;
+      } else if ((unsigned)r < (unsigned)a.m) {
+        atomicAdd(y + r, v);
+      } else {
+        flag_error(a.err, kDevErrOob);
       }
     }
     __syncthreads();

@@ -13,6 +13,7 @@
 #include "feat.h"
 #include "kernels.h"
 #include "sort.h"
+#include "bucket.h"
 
 namespace spmx {
 
@@ -148,6 +149,8 @@ static void free_sort_scratch(spmx_handle_t h) {
   dfree(h->sk); dfree(h->sk_alt); dfree(h->sv); dfree(h->sv_alt);
   dfree(h->shist); dfree(h->shist_off); dfree(h->sslot);
   dfree(h->sy_key); dfree(h->sy_val);
+  dfree(h->bk_gcount); dfree(h->bk_boff); dfree(h->bk_cursor);
+  h->bk_gcount = h->bk_boff = h->bk_cursor = nullptr;
   h->sk = h->sk_alt = h->sv = h->sv_alt = nullptr;
   h->shist = h->shist_off = h->sslot = nullptr;
   h->sy_key = nullptr;
@@ -162,6 +165,7 @@ static void free_csc_scratch(spmx_handle_t h) {
 }
 
 extern "C" int spmx_hola_postprocess(spmx_handle_t h);
+extern "C" int spmx_csr5_postprocess(spmx_handle_t h);
 
 extern "C" int spmx_destroy(spmx_handle_t h) {
   if (!h) return SPMX_SUCCESS;
@@ -175,6 +179,7 @@ extern "C" int spmx_destroy(spmx_handle_t h) {
   free_csc_scratch(h);
   free_sort_scratch(h);
   spmx_hola_postprocess(h);
+  spmx_csr5_postprocess(h);
   dfree(h->bfs_visited); dfree(h->bfs_front); dfree(h->bfs_q[0]); dfree(h->bfs_q[1]);
   dfree(h->bfs_cnt); dfree(h->bfs_edges);
   delete h;
@@ -267,6 +272,9 @@ static int ensure_sort_scratch(spmx_handle_t h) {
   const size_t ycap = (size_t)std::max(h->m, 1);
   SPMX_TRY(dalloc((void**)&h->sy_key, 4 * ycap, "sparse y keys"));
   SPMX_TRY(dalloc((void**)&h->sy_val, 4 * ycap, "sparse y vals"));
+  SPMX_TRY(dalloc((void**)&h->bk_gcount, 4 * (size_t)kBucketMax, "bucket counts"));
+  SPMX_TRY(dalloc((void**)&h->bk_boff, 4 * (size_t)(kBucketMax + 1), "bucket offsets"));
+  SPMX_TRY(dalloc((void**)&h->bk_cursor, 4 * (size_t)kBucketMax, "bucket cursors"));
   h->sort_ready = true;
   return SPMX_SUCCESS;
 }
@@ -635,6 +643,8 @@ extern "C" int spmx_spmspv(spmx_handle_t h, float alpha, float* y) {
 // ---------------------------------------------------------------------------
 int csc_bucket_impl(spmx_handle_t h, float alpha, float* y, int* ykey, float* yval,
                     int* ynnz, int buckets);
+static int ensure_csc_scratch(spmx_handle_t h);
+static int read_counter(spmx_handle_t h, int slot, int* out);
 
 static CscArgs csc_args(spmx_handle_t h, float alpha) {
   return CscArgs{h->m, h->n, h->csc_colptr, h->csc_row, h->csc_val, h->x_nnz,
@@ -776,4 +786,28 @@ extern "C" int spmx_csc_bucket(spmx_handle_t h, float alpha, int* ynnz, float* y
     return set_error(SPMX_ERR_NOT_READY, "CSC SpMSpV needs the CSC with values");
   if (h->x_nnz == 0) return spmx_spmspv_csc(h, SPMX_CSC_BUCKET, SPMX_WB_SORT, alpha, y, ykey, yval, ynnz);
   return csc_bucket_impl(h, alpha, y, ykey, yval, ynnz, buckets);
+}
+
+// ---------------------------------------------------------------------------
+// bucket-based CSC SpMSpV
+// ---------------------------------------------------------------------------
+int csc_bucket_impl(spmx_handle_t h, float alpha, float* y, int* ykey, float* yval,
+                    int* ynnz, int buckets) {
+  SPMX_TRY(ensure_csc_scratch(h));
+  SPMX_TRY(ensure_sort_scratch(h));
+  int rshift = 0, nb = 0;
+  if (bucket_geometry(h->m, buckets > 0 ? buckets : h->buckets, &rshift, &nb))
+    return set_error(SPMX_ERR_INVALID_VALUE, "too many rows for the bucket method");
+  if (nb > h->ls.status_len) return set_error(SPMX_ERR_INVALID_VALUE, "bucket count exceeds scan capacity");
+  cudaStream_t st = h->stream;
+  const CscArgs a = csc_args(h, alpha);
+  if (launch_csc_scan(a, h->cs, h->ls, kCscLbNT * kCscLbVT, st))
+    return set_error(SPMX_ERR_INVALID_VALUE, "scan capacity");
+  BucketScratch bs{h->bk_gcount, h->bk_boff, h->bk_cursor, (int*)h->sk, (float*)h->sv, h->nnz};
+  if (launch_bucket_spmspv(a, h->cs, bs, SPMX_CSC_LB_MERGE, rshift, nb, y, ykey, yval,
+                           h->d_counts + kCntYnnz, h->ls, h->lb_grid, st))
+    return set_error(SPMX_ERR_INVALID_VALUE, "bucket launch capacity");
+  SPMX_TRY(launch_ok("bucket spmspv"));
+  if (ynnz) SPMX_TRY(read_counter(h, kCntYnnz, ynnz));
+  return SPMX_SUCCESS;
 }

@@ -68,6 +68,13 @@ struct spmx_handle_s {
   int* sy_key = nullptr;      // internal sparse y (adaptive path)
   float* sy_val = nullptr;
   bool sort_ready = false;
+  int* bk_gcount = nullptr;   // bucket histogram / offsets / cursors
+  int* bk_boff = nullptr;
+  int* bk_cursor = nullptr;
+  int buckets = 0;            // 0 = default (256)
+
+  // CSR5 tile tables (csr5.cu)
+  void* csr5 = nullptr;
 
   // Hola tables
   spmx::HolaTables hola{};
@@ -84,6 +91,7 @@ struct spmx_handle_s {
   bool mat_feat_ready = false;
   double mat_feat[10] = {0};
   bool std_row_ready = false;
+  long long col_max = -1;     // longest CSC column (-1 = not computed)
   float std_row = 0.f;
   long long bin_len = -1;
   long long vec_max = 0, vec_min = 0;

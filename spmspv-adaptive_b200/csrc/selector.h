@@ -25,14 +25,17 @@ SPMX_HD inline int select_by_traffic_model(const double* f) {
   const double m = f[0], n = f[1], nnz = f[2];
   const double max_row = f[3], avg_row = f[5] > 0 ? f[5] : 1.0;
   const double x = f[10], bin = f[11];
-  const double bw = 6.5e3;     // bytes per microsecond
+  const double bw = 6.5e6;     // bytes per microsecond (6.5 TB/s)
   const double launch = 2.5;   // microseconds per dependent launch
   const bool skewed = max_row > 8.0 * avg_row + 32.0;
   // CSC SpMSpV, atomic write-back: y memset, scan, gather + atomics
   const double csc_lb = 3 * launch + (4 * m + 16 * x + 8 * bin + 8 * bin) / bw;
+  // f[12] holds the longest column of x (or an upper bound of it): one
+  // group per column serialises on it
   const double avg_col = n > 0 ? nnz / n : 1.0;
-  const double csc_naive = 2 * launch + (4 * m + 12 * x + 16 * bin) / bw *
-                           (avg_col > 64 ? 4.0 : 1.0);
+  const double max_col = f[12] > 0 ? f[12] : avg_col;
+  const bool col_skewed = max_col > 8.0 * avg_col + 64.0;
+  const double csc_naive = 2 * launch + (4 * m + 12 * x + 16 * bin) / bw;
   // sort write-back: scan, read-back, pairs, radix passes, reduce
   const double passes = ceil(log2(m > 2 ? m : 2) / 8.0);
   const double csc_sort = (6 + 3 * passes) * launch + 10.0 +
@@ -45,7 +48,7 @@ SPMX_HD inline int select_by_traffic_model(const double* f) {
   const double spmv = s2d + launch + (4 * (m + 1) + 8 * nnz + 4 * n + 4 * m) / bw;
   double best = csc_lb;
   int k = SPMX_K_CSC_LB_ATOMIC;
-  if (!skewed && csc_naive < best) { best = csc_naive; k = SPMX_K_CSC_NAIVE_ATOMIC; }
+  if (!col_skewed && csc_naive < best) { best = csc_naive; k = SPMX_K_CSC_NAIVE_ATOMIC; }
   if (csc_sort < best) { best = csc_sort; k = SPMX_K_CSC_LB_SORT; }
   if (csr_spmspv < best) { best = csr_spmspv; k = skewed ? SPMX_K_CSR_LB_SPMSPV : SPMX_K_CSR_NAIVE_SPMSPV; }
   if (spmv < best) { best = spmv; k = skewed ? SPMX_K_LB_SPMV : SPMX_K_NAIVE_SPMV; }

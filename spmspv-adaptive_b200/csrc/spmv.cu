@@ -105,8 +105,10 @@ spmv_chunk_kernel(int m, int n, int nnz, const int* __restrict__ rowptr,
                   const int* __restrict__ chunk_row, double* carry,
                   unsigned* arrive, int vec_ok, int* err) {
   constexpr int K = NT * VT;
-  __shared__ double sP[K + 1];
+  __shared__ double sP[K];
   __shared__ double s_wtmp[NT / 32 + 1];
+  __shared__ int s_tf[NT / 32 + 1];
+  __shared__ unsigned s_flag[K / 32];
   const int c = blockIdx.x;
   const int s = c * K;
   const int e = min(s + K, nnz);
@@ -151,24 +153,46 @@ spmv_chunk_kernel(int m, int n, int nnz, const int* __restrict__ rowptr,
     }
   }
 
+  // row-start flags of the rows that begin inside the chunk
+  const int lo = __ldg(chunk_row + c), hi = __ldg(chunk_row + c + 1);
+  for (int i = threadIdx.x; i < K / 32; i += NT) s_flag[i] = 0u;
+  __syncthreads();
+  for (int r = lo + (int)threadIdx.x; r < hi; r += NT) {
+    const int p = __ldg(rowptr + r) - s;
+    if (p < e - s) atomicOr(&s_flag[p >> 5], 1u << (p & 31));
+  }
+  __syncthreads();
+  // segmented scan: every row is summed from its own products only (no
+  // differences of running sums), so all-zero rows stay exactly zero
+  unsigned myf;
+  {
+    const int bit0 = threadIdx.x * VT;
+    const unsigned w = s_flag[bit0 >> 5];
+    myf = (w >> (bit0 & 31)) & ((VT >= 32) ? 0xffffffffu : ((1u << VT) - 1u));
+  }
   double run = 0.0;
 #pragma unroll
-  for (int j = 0; j < VT; ++j) { run += pr[j]; pr[j] = run; }
-  double tot;
-  const double ex = block_exclusive_sum<NT>(run, s_wtmp, &tot);
-  if (threadIdx.x == 0) sP[0] = 0.0;
+  for (int j = 0; j < VT; ++j) {
+    run = ((myf >> j) & 1u) ? pr[j] : run + pr[j];
+    pr[j] = run;
+  }
+  const double carry_in = block_exclusive_segscan<NT>(myf != 0u, run, s_tf, s_wtmp);
+  const int first = myf ? __ffs(myf) - 1 : VT;
 #pragma unroll
-  for (int j = 0; j < VT; ++j) sP[threadIdx.x * VT + j + 1] = ex + pr[j];
+  for (int j = 0; j < VT; ++j) {
+    if (j < first) pr[j] += carry_in;
+    sP[threadIdx.x * VT + j] = pr[j];
+  }
   __syncthreads();
 
-  const int lo = __ldg(chunk_row + c), hi = __ldg(chunk_row + c + 1);
   for (int r = lo + (int)threadIdx.x; r < hi; r += NT) {
     const int a = __ldg(rowptr + r), b = __ldg(rowptr + r + 1);
-    if (b <= e) {
-      y[r] = (float)(alpha * (sP[b - s] - sP[a - s]));
+    if (b == a) {
+      y[r] = 0.f;
+    } else if (b <= e) {
+      y[r] = (float)(alpha * sP[b - 1 - s]);
     } else {
-      split_row_contribute<K>(r, c, 1, sP[e - s] - sP[a - s], rowptr, carry,
-                              arrive, alpha, y);
+      split_row_contribute<K>(r, c, 1, sP[e - 1 - s], rowptr, carry, arrive, alpha, y);
     }
   }
   if (threadIdx.x == 0 && lo > 0) {
@@ -176,8 +200,7 @@ spmv_chunk_kernel(int m, int n, int nnz, const int* __restrict__ rowptr,
     const int endR = __ldg(rowptr + lo);
     if (endR > s) {
       const int stop = min(endR, e);
-      split_row_contribute<K>(R, c, 0, sP[stop - s], rowptr, carry, arrive,
-                              alpha, y);
+      split_row_contribute<K>(R, c, 0, sP[stop - 1 - s], rowptr, carry, arrive, alpha, y);
     }
   }
 }

@@ -83,6 +83,7 @@ _SIGS = {
     "spmx_set_sigma": (c_int, [P, c_int]),
     "spmx_csr5_preprocess": (c_int, [P]),
     "spmx_csr5_postprocess": (c_int, [P]),
+    "spmx_csr5_sigma": (c_int, [P, PI]),
     "spmx_set_spmv_type": (c_int, [P, c_int]),
     "spmx_naivespmv": (c_int, [P, c_float, P]),
     "spmx_holaspmv": (c_int, [P, c_float, P]),

@@ -207,3 +207,29 @@ def test_features(torch_cuda):
         assert h.computeGM() == pytest.approx(orc.gm(A.m, A.nnz, 1000, b).tolist())
         feats = h.features()
         assert feats["bin_len"] == b and feats["x_nnz"] == 1000
+
+
+@pytest.mark.parametrize("mat", ["uniform", "skewed", "long-col"])
+@pytest.mark.parametrize("frac", [0.0005, 0.05, 1.0])
+@pytest.mark.parametrize("buckets", [0, 3, 64])
+def test_csc_bucket(torch_cuda, mat, frac, buckets):
+    """Bucket write-back: dense y and the sorted touched rows (no global atomics)."""
+    torch = torch_cuda
+    A = _matrix(mat)
+    h = make_handle(A, torch, hola=False)
+    k = max(1, int(frac * A.n))
+    key, val = _x(A.n, k, 6)
+    set_sparse(h, key, val, torch)
+    y = torch.full((A.m,), 4.0, device="cuda")
+    yk = torch.empty(A.m, dtype=torch.int32, device="cuda")
+    yv = torch.empty(A.m, device="cuda")
+    ynnz = h.CscBasedBucketSpmspv(0.5, y, yk, yv, buckets)
+    h.check_device_error()
+    colptr, row, cval = A.to_csc()
+    y64, mag, touched = orc.spmspv_csc_f64(A.m, colptr, row, cval, key, val, alpha=0.5)
+    ok, _ = orc.within_tol(y.cpu().numpy(), y64, mag, RTOL)
+    assert ok
+    rows = np.nonzero(touched)[0]
+    assert ynnz == len(rows)
+    assert np.array_equal(yk[:ynnz].cpu().numpy(), rows)
+    assert np.array_equal(yv[:ynnz].cpu().numpy(), y.cpu().numpy()[rows])

@@ -104,3 +104,58 @@ def test_spmv_full_size_zipf(torch_cuda):
         h.check_device_error()
         ok, _ = orc.within_tol(y.cpu().numpy(), y64, mag, RTOL)
         assert ok, kind
+
+
+@pytest.mark.parametrize("name,A", CASES, ids=[c[0] for c in CASES])
+@pytest.mark.parametrize("sigma", [-1, 4, 12, 32])
+def test_csr5_spmv(torch_cuda, name, A, sigma):
+    torch = torch_cuda
+    h = make_handle(A, torch, csc=False, hola=False)
+    h.setSigma(sigma)
+    h.CSR5Preprocess()
+    x = np.random.default_rng(13).uniform(-1, 1, A.n).astype(np.float32)
+    h.set_x(dev(x, torch))
+    for rep in range(2):  # the second call checks the self-resetting counters
+        y = torch.full((A.m,), 7.0, device="cuda")
+        h.csr5spmv(1.25, y)
+        h.check_device_error()
+        y64, mag = orc.spmv_f64(A.rowptr, A.col, A.val, x, alpha=1.25)
+        ok, _ = orc.within_tol(y.cpu().numpy(), y64, mag, RTOL)
+        assert ok, orc.max_scaled_err(y.cpu().numpy(), y64, mag)
+
+
+@pytest.mark.parametrize("name,A", CASES[:3], ids=[c[0] for c in CASES[:3]])
+def test_csr5_spmspv_gated(torch_cuda, name, A):
+    torch = torch_cuda
+    h = make_handle(A, torch, csc=False, hola=False)
+    h.CSR5Preprocess()
+    rng = np.random.default_rng(8)
+    k = max(1, A.n // 40)
+    key = np.sort(rng.choice(A.n, k, replace=False)).astype(np.int32)
+    val = rng.uniform(-1, 1, k).astype(np.float32)
+    kd, vd = dev(key, torch), dev(val, torch)
+    h.set_sparse_x(kd, vd, k)
+    h.sparse2bitarray()
+    y = torch.zeros(A.m, device="cuda")
+    h.csr5spmspv(1.0, y)
+    h.check_device_error()
+    xd, bits = orc.sparse2dense_bits(A.n, key, val)
+    y64, mag = orc.spmv_f64(A.rowptr, A.col, A.val, xd, bits=bits.view(np.int32))
+    ok, _ = orc.within_tol(y.cpu().numpy(), y64, mag, RTOL)
+    assert ok
+
+
+def test_csr5_zipf_full_size(torch_cuda):
+    torch = torch_cuda
+    from spmx import gen
+    A = gen.zipf_1m()
+    h = make_handle(A, torch, csc=False, hola=False)
+    h.CSR5Preprocess()
+    x = np.random.default_rng(2).uniform(-1, 1, A.n).astype(np.float32)
+    h.set_x(dev(x, torch))
+    y = torch.empty(A.m, device="cuda")
+    h.csr5spmv(1.0, y)
+    h.check_device_error()
+    y64, mag = orc.spmv_f64(A.rowptr, A.col, A.val, x)
+    ok, _ = orc.within_tol(y.cpu().numpy(), y64, mag, RTOL)
+    assert ok
