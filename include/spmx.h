@@ -120,6 +120,9 @@ int spmx_input_csc(spmx_handle_t h, int nnz, const int* d_csc_row,
 /* ToCSC() — H:384-419 (cusparseScsr2csc there).  Handle-owned CSC with row
  * indices sorted inside each column (a stable transpose). */
 int spmx_to_csc(spmx_handle_t h);
+/* copy the handle's CSC into caller buffers (row[nnz], colptr[n+1],
+ * val[nnz]; any may be NULL); asynchronous on the handle's stream */
+int spmx_copy_csc(spmx_handle_t h, int* d_row, int* d_colptr, float* d_val);
 /* read access to the handle's CSC (device pointers, valid until destroy) */
 int spmx_get_csc(spmx_handle_t h, const int** d_csc_row, const int** d_csc_col,
                  const float** d_csc_val);
@@ -272,6 +275,17 @@ int spmx_run_kernel(spmx_handle_t h, int kernel_id, float alpha, float* d_y);
  * (CSR; CSC is taken as the same arrays).  d_levels[n] receives hop counts,
  * -1 for unreachable; depth (host, may be NULL) the number of levels. */
 int spmx_bfs(spmx_handle_t h, int source, int* d_levels, int* depth);
+/* 0 (default): the whole traversal in one cooperative persistent launch with
+ * the push/pull choice on the device; 1: one launch per level with the
+ * frontier size read back by the host (the reference's replay-loop shape) */
+int spmx_set_bfs_mode(spmx_handle_t h, int mode);
+/* Batched BFS (no reference counterpart): up to 64 sources (host array) in
+ * one persistent launch, one bit per source per vertex.  layout 0: d_levels
+ * is vertex-major, d_levels[v * nsrc + s]; layout 1: source-major,
+ * d_levels[s * n + v].  depth (host, may be NULL): levels of the deepest
+ * traversal. */
+int spmx_bfs_batched(spmx_handle_t h, const int* srcs, int nsrc, int* d_levels,
+                     int layout, int* depth);
 
 /* ======================= device counters ================================== */
 /* device pointers to the handle's counters: [0] y_nnz of the last SpMSpV,

@@ -301,28 +301,139 @@ extern "C" int spmx_run_adaptive(spmx_handle_t h, float alpha, float* y, int* ke
 // BFS: level-synchronous, direction-optimising (push = CSC SpMSpV, pull =
 // bitmap-gated CSR SpMSpV).  For a symmetric pattern CSR and CSC coincide.
 // ---------------------------------------------------------------------------
+static int bfs_stepped(spmx_handle_t h, int source, int* levels, int* depth);
+
 static int ensure_bfs(spmx_handle_t h) {
   if (h->bfs_n == h->n && h->bfs_visited) return SPMX_SUCCESS;
   dfree(h->bfs_visited); dfree(h->bfs_front); dfree(h->bfs_q[0]); dfree(h->bfs_q[1]);
-  dfree(h->bfs_cnt); dfree(h->bfs_edges);
+  dfree(h->bfs_cnt); dfree(h->bfs_edges); dfree(h->bfs_fb1); dfree(h->bfs_ctrl);
   const size_t words = (size_t)std::max((h->n + 31) / 32, 1);
   SPMX_TRY(dalloc((void**)&h->bfs_visited, 4 * words, "bfs visited"));
   SPMX_TRY(dalloc((void**)&h->bfs_front, 4 * words, "bfs front"));
+  SPMX_TRY(dalloc((void**)&h->bfs_fb1, 4 * words, "bfs front 1"));
   SPMX_TRY(dalloc((void**)&h->bfs_q[0], 4 * (size_t)std::max(h->n, 1), "bfs queue 0"));
   SPMX_TRY(dalloc((void**)&h->bfs_q[1], 4 * (size_t)std::max(h->n, 1), "bfs queue 1"));
   SPMX_TRY(dalloc((void**)&h->bfs_cnt, 4 * 4, "bfs counts"));
   SPMX_TRY(dalloc((void**)&h->bfs_edges, 8 * 4, "bfs edges"));
+  SPMX_TRY(dalloc((void**)&h->bfs_ctrl, sizeof(BfsCtrl), "bfs ctrl"));
   h->bfs_n = h->n;
+  return SPMX_SUCCESS;
+}
+
+static int bfs_check(spmx_handle_t h) {
+  if (!h->has_csr) return set_error(SPMX_ERR_NOT_READY, "BFS needs the (symmetric) CSR pattern");
+  if (h->m != h->n) return set_error(SPMX_ERR_INVALID_VALUE, "BFS needs a square matrix");
+  return SPMX_SUCCESS;
+}
+
+extern "C" int spmx_set_bfs_mode(spmx_handle_t h, int mode) {
+  SPMX_CHECK_HANDLE(h);
+  if (mode != 0 && mode != 1) return set_error(SPMX_ERR_INVALID_VALUE, "BFS mode must be 0 or 1");
+  h->bfs_mode = mode;
+  return SPMX_SUCCESS;
+}
+
+static int bfs_persistent(spmx_handle_t h, int source, int* levels, int* depth) {
+  cudaStream_t st = h->stream;
+  const int n = h->n;
+  const size_t words = (size_t)((n + 31) / 32);
+  SPMX_CUDA(cudaMemsetAsync(levels, 0xff, 4 * (size_t)n, st));
+  SPMX_CUDA(cudaMemsetAsync(h->bfs_visited, 0, 4 * words, st));
+  SPMX_CUDA(cudaMemsetAsync(h->bfs_front, 0, 4 * words, st));
+  SPMX_CUDA(cudaMemsetAsync(h->bfs_fb1, 0, 4 * words, st));
+  BfsPersistentArgs a{n, source, h->num_sms, (long long)h->nnz, h->rowptr, h->col, levels,
+                      h->bfs_visited, h->bfs_front, h->bfs_fb1, h->bfs_q[0], h->bfs_q[1],
+                      (BfsCtrl*)h->bfs_ctrl, h->bfs_alpha, h->bfs_beta, h->d_err};
+  const int rc = launch_bfs_persistent(a, st);
+  if (rc) return set_error(SPMX_ERR_CUDA, std::string("cooperative BFS launch: ") +
+                                              cudaGetErrorString(cudaGetLastError()));
+  if (depth) {
+    int d = 0;
+    SPMX_CUDA(cudaMemcpyAsync(&d, &((BfsCtrl*)h->bfs_ctrl)->depth, sizeof(int),
+                              cudaMemcpyDeviceToHost, st));
+    SPMX_CUDA(cudaStreamSynchronize(st));
+    *depth = d;
+  }
   return SPMX_SUCCESS;
 }
 
 extern "C" int spmx_bfs(spmx_handle_t h, int source, int* levels, int* depth) {
   SPMX_CHECK_HANDLE(h);
-  if (!h->has_csr) return set_error(SPMX_ERR_NOT_READY, "BFS needs the (symmetric) CSR pattern");
-  if (h->m != h->n) return set_error(SPMX_ERR_INVALID_VALUE, "BFS needs a square matrix");
+  SPMX_TRY(bfs_check(h));
   if (source < 0 || source >= h->n) return set_error(SPMX_ERR_INVALID_VALUE, "source out of range");
   if (!levels) return set_error(SPMX_ERR_INVALID_VALUE, "levels is NULL");
   SPMX_TRY(ensure_bfs(h));
+  if (h->bfs_mode == 0) return bfs_persistent(h, source, levels, depth);
+  return bfs_stepped(h, source, levels, depth);
+}
+
+static int ensure_msbfs(spmx_handle_t h) {
+  if (h->ms_n == h->n && h->ms_visit) return SPMX_SUCCESS;
+  dfree(h->ms_visit); dfree(h->ms_front0); dfree(h->ms_front1); dfree(h->ms_next);
+  dfree(h->ms_q0); dfree(h->ms_q1); dfree(h->ms_srcs); dfree(h->ms_ctrl);
+  const size_t n = (size_t)std::max(h->n, 1);
+  SPMX_TRY(dalloc((void**)&h->ms_visit, 8 * n, "msbfs visit"));
+  SPMX_TRY(dalloc((void**)&h->ms_front0, 8 * n, "msbfs front 0"));
+  SPMX_TRY(dalloc((void**)&h->ms_front1, 8 * n, "msbfs front 1"));
+  SPMX_TRY(dalloc((void**)&h->ms_next, 8 * n, "msbfs next"));
+  SPMX_TRY(dalloc((void**)&h->ms_q0, 4 * n, "msbfs queue 0"));
+  SPMX_TRY(dalloc((void**)&h->ms_q1, 4 * n, "msbfs queue 1"));
+  SPMX_TRY(dalloc((void**)&h->ms_srcs, 4 * 64, "msbfs sources"));
+  SPMX_TRY(dalloc((void**)&h->ms_ctrl, sizeof(BfsCtrl), "msbfs ctrl"));
+  h->ms_n = h->n;
+  return SPMX_SUCCESS;
+}
+
+extern "C" int spmx_bfs_batched(spmx_handle_t h, const int* srcs, int nsrc, int* levels,
+                                int layout, int* depth) {
+  SPMX_CHECK_HANDLE(h);
+  SPMX_TRY(bfs_check(h));
+  if (nsrc < 1 || nsrc > 64) return set_error(SPMX_ERR_INVALID_VALUE, "nsrc must be in [1, 64]");
+  if (!srcs || !levels) return set_error(SPMX_ERR_INVALID_VALUE, "NULL argument");
+  if (layout != 0 && layout != 1) return set_error(SPMX_ERR_INVALID_VALUE, "layout must be 0 or 1");
+  for (int s = 0; s < nsrc; ++s)
+    if (srcs[s] < 0 || srcs[s] >= h->n) return set_error(SPMX_ERR_INVALID_VALUE, "source out of range");
+  SPMX_TRY(ensure_msbfs(h));
+  cudaStream_t st = h->stream;
+  const size_t n = (size_t)h->n;
+  const size_t total = n * (size_t)nsrc;
+  int* vmajor = levels;
+  if (layout == 1) {
+    if (h->ms_tmp_len < total) {
+      SPMX_CUDA(cudaStreamSynchronize(st));
+      dfree(h->ms_tmp);
+      h->ms_tmp = nullptr;
+      h->ms_tmp_len = 0;
+      SPMX_TRY(dalloc((void**)&h->ms_tmp, 4 * total, "msbfs levels"));
+      h->ms_tmp_len = total;
+    }
+    vmajor = h->ms_tmp;
+  }
+  SPMX_CUDA(cudaMemcpyAsync(h->ms_srcs, srcs, 4 * (size_t)nsrc, cudaMemcpyHostToDevice, st));
+  SPMX_CUDA(cudaMemsetAsync(vmajor, 0xff, 4 * total, st));
+  SPMX_CUDA(cudaMemsetAsync(h->ms_visit, 0, 8 * n, st));
+  SPMX_CUDA(cudaMemsetAsync(h->ms_front0, 0, 8 * n, st));
+  SPMX_CUDA(cudaMemsetAsync(h->ms_front1, 0, 8 * n, st));
+  SPMX_CUDA(cudaMemsetAsync(h->ms_next, 0, 8 * n, st));
+  MsBfsArgs a{h->n, nsrc, h->num_sms, (long long)h->nnz, h->msbfs_alpha, h->ms_srcs, h->rowptr,
+              h->col, vmajor, h->ms_visit, h->ms_front0, h->ms_front1, h->ms_next, h->ms_q0,
+              h->ms_q1, (BfsCtrl*)h->ms_ctrl, h->d_err};
+  if (launch_msbfs_persistent(a, st))
+    return set_error(SPMX_ERR_CUDA, std::string("cooperative multi-source BFS launch: ") +
+                                        cudaGetErrorString(cudaGetLastError()));
+  if (layout == 1) launch_levels_transpose(h->n, nsrc, vmajor, levels, st);
+  SPMX_TRY(launch_ok("batched bfs"));
+  if (depth) {
+    int d = 0;
+    SPMX_CUDA(cudaMemcpyAsync(&d, &((BfsCtrl*)h->ms_ctrl)->depth, sizeof(int),
+                              cudaMemcpyDeviceToHost, st));
+    SPMX_CUDA(cudaStreamSynchronize(st));
+    *depth = d;
+  }
+  return SPMX_SUCCESS;
+}
+
+static int bfs_stepped(spmx_handle_t h, int source, int* levels, int* depth) {
   cudaStream_t st = h->stream;
   const int n = h->n;
   const size_t words = (size_t)((n + 31) / 32);

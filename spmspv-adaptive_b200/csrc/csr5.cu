@@ -62,7 +62,9 @@ __global__ void csr5_tiles_kernel(int m, int nnz, int sigma, int ntiles,
       if (__ldg(rowptr + mid) <= e0) lo = mid; else hi = mid - 1;
     }
     int r = lo;
-    rk = __ldg(rank + r);
+    // the rank of the row open just before e0: one less when a row starts at
+    // e0 itself (-1 before the first row)
+    rk = __ldg(rank + r) - (__ldg(rowptr + r) == e0 ? 1 : 0);
     for (int j = 0; j < sigma; ++j) {
       const long long e = e0 + j;
       if (e >= nnz) break;
@@ -134,12 +136,18 @@ csr5_spmv_kernel(int m, int n, int ntiles, const int* __restrict__ rowptr,
       if (!seen) {
         head = run;
         seen = true;
-      } else {
+      } else if ((unsigned)rk < (unsigned)m_nz) {
         y[__ldg(nz_rows + rk)] = (float)(alpha * run);  // a row complete inside the lane
+      } else {
+        flag_error(err, kDevErrOob);
       }
       ++rk;
-      // empty rows between the previous non-empty row and this one
-      zero_rows(y, __ldg(nz_rows + rk - 1) + 1, __ldg(nz_rows + rk));
+      if ((unsigned)rk < (unsigned)m_nz) {
+        // empty rows between the previous non-empty row and this one
+        if (rk >= 1) zero_rows(y, __ldg(nz_rows + rk - 1) + 1, __ldg(nz_rows + rk));
+      } else {
+        flag_error(err, kDevErrOob);
+      }
       run = 0.0;
     }
     run += p;
@@ -164,7 +172,7 @@ csr5_spmv_kernel(int m, int n, int ntiles, const int* __restrict__ rowptr,
   const double V0 = __shfl_sync(0xffffffffu, V, 0);
   const unsigned f0 = __shfl_sync(0xffffffffu, flags, 0);
   const int tile_end = (t + 1) * K;
-  if (seen) {
+  if (seen && (unsigned)rk < (unsigned)m_nz) {
     // the last row opened in this lane: its tail plus the heads of the lanes
     // up to the next lane that opens a row (or to the end of the tile)
     const int R = __ldg(nz_rows + rk);
@@ -173,11 +181,11 @@ csr5_spmv_kernel(int m, int n, int ntiles, const int* __restrict__ rowptr,
     else csr5_contribute(R, t, 1, sum, K, rowptr, carry, arrive, alpha, y);
   }
   if (l == 0) {
-    if (!(f0 & 1u)) {
+    const int r0 = __ldg(lane_rank + (size_t)t * 32);
+    if (!(f0 & 1u) && (unsigned)r0 < (unsigned)m_nz) {
       // the row open at the tile start began in an earlier tile: its part here
       // runs through the first lane that opens a row (or the whole tile)
-      const int R = __ldg(nz_rows + __ldg(lane_rank + (size_t)t * 32));
-      csr5_contribute(R, t, 0, V0, K, rowptr, carry, arrive, alpha, y);
+      csr5_contribute(__ldg(nz_rows + r0), t, 0, V0, K, rowptr, carry, arrive, alpha, y);
     }
     if (t == 0) zero_rows(y, 0, __ldg(nz_rows + 0));
     if (t == ntiles - 1) zero_rows(y, __ldg(nz_rows + m_nz - 1) + 1, m);
@@ -249,7 +257,8 @@ static int pick_sigma(int s) {
 
 extern "C" int spmx_csr5_preprocess(spmx_handle_t h) {
   if (!h) return set_error(SPMX_ERR_INVALID_VALUE, "NULL handle");
-  if (!h->has_csr || !h->val) return set_error(SPMX_ERR_NOT_READY, "CSR5 needs the CSR input with values");
+  if (!h->has_csr || (!h->val && h->nnz > 0))
+    return set_error(SPMX_ERR_NOT_READY, "CSR5 needs the CSR input with values");
   spmx_csr5_postprocess(h);
   Csr5Tables* t = new Csr5Tables();
   h->csr5 = t;

@@ -181,7 +181,9 @@ extern "C" int spmx_destroy(spmx_handle_t h) {
   spmx_hola_postprocess(h);
   spmx_csr5_postprocess(h);
   dfree(h->bfs_visited); dfree(h->bfs_front); dfree(h->bfs_q[0]); dfree(h->bfs_q[1]);
-  dfree(h->bfs_cnt); dfree(h->bfs_edges);
+  dfree(h->bfs_cnt); dfree(h->bfs_edges); dfree(h->bfs_fb1); dfree(h->bfs_ctrl);
+  dfree(h->ms_visit); dfree(h->ms_front0); dfree(h->ms_front1); dfree(h->ms_next);
+  dfree(h->ms_q0); dfree(h->ms_q1); dfree(h->ms_srcs); dfree(h->ms_tmp); dfree(h->ms_ctrl);
   delete h;
   return SPMX_SUCCESS;
 }
@@ -345,6 +347,19 @@ extern "C" int spmx_to_csc(spmx_handle_t h) {
   h->csc_val = h->own_cval;
   h->has_csc = true;
   return launch_ok("ToCSC");
+}
+
+extern "C" int spmx_copy_csc(spmx_handle_t h, int* row, int* colptr, float* val) {
+  SPMX_CHECK_HANDLE(h);
+  if (!h->has_csc) return set_error(SPMX_ERR_NOT_READY, "no CSC (call spmx_to_csc)");
+  cudaStream_t st = h->stream;
+  if (row && h->nnz)
+    SPMX_CUDA(cudaMemcpyAsync(row, h->csc_row, 4 * (size_t)h->nnz, cudaMemcpyDeviceToDevice, st));
+  if (colptr)
+    SPMX_CUDA(cudaMemcpyAsync(colptr, h->csc_colptr, 4 * (size_t)(h->n + 1), cudaMemcpyDeviceToDevice, st));
+  if (val && h->csc_val && h->nnz)
+    SPMX_CUDA(cudaMemcpyAsync(val, h->csc_val, 4 * (size_t)h->nnz, cudaMemcpyDeviceToDevice, st));
+  return SPMX_SUCCESS;
 }
 
 extern "C" int spmx_get_csc(spmx_handle_t h, const int** row, const int** colptr,
@@ -575,7 +590,8 @@ extern "C" int spmx_set_spmv_type(spmx_handle_t h, int code) {
 // SpMV / CSR SpMSpV
 // ---------------------------------------------------------------------------
 static int spmv_common(spmx_handle_t h, float alpha, float* y, bool gated, SpmvArgs* a) {
-  if (!h->has_csr || !h->val) return set_error(SPMX_ERR_NOT_READY, "SpMV needs the CSR input with values");
+  if (!h->has_csr || (!h->val && h->nnz > 0))
+    return set_error(SPMX_ERR_NOT_READY, "SpMV needs the CSR input with values");
   if (!h->x_dense) return set_error(SPMX_VEC_FORMAT_ERR, "SpMV needs the dense x (set_x / sparse2dense)");
   if (gated && !h->bitvec) return set_error(SPMX_VEC_FORMAT_ERR, "SpMSpV needs the bitarray (sparse2bitarray)");
   if (!y && h->m > 0) return set_error(SPMX_ERR_INVALID_VALUE, "y is NULL");
@@ -645,6 +661,7 @@ int csc_bucket_impl(spmx_handle_t h, float alpha, float* y, int* ykey, float* yv
                     int* ynnz, int buckets);
 static int ensure_csc_scratch(spmx_handle_t h);
 static int read_counter(spmx_handle_t h, int slot, int* out);
+static int ensure_scan_tiles(spmx_handle_t h, long long tiles);
 
 static CscArgs csc_args(spmx_handle_t h, float alpha) {
   return CscArgs{h->m, h->n, h->csc_colptr, h->csc_row, h->csc_val, h->x_nnz,
@@ -798,7 +815,7 @@ int csc_bucket_impl(spmx_handle_t h, float alpha, float* y, int* ykey, float* yv
   int rshift = 0, nb = 0;
   if (bucket_geometry(h->m, buckets > 0 ? buckets : h->buckets, &rshift, &nb))
     return set_error(SPMX_ERR_INVALID_VALUE, "too many rows for the bucket method");
-  if (nb > h->ls.status_len) return set_error(SPMX_ERR_INVALID_VALUE, "bucket count exceeds scan capacity");
+  SPMX_TRY(ensure_scan_tiles(h, nb));
   cudaStream_t st = h->stream;
   const CscArgs a = csc_args(h, alpha);
   if (launch_csc_scan(a, h->cs, h->ls, kCscLbNT * kCscLbVT, st))

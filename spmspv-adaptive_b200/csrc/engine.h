@@ -97,7 +97,23 @@ struct spmx_handle_s {
   long long vec_max = 0, vec_min = 0;
   double gm[3] = {-1, -1, -1};
 
-  // BFS buffers
+  // BFS buffers (level-stepped and persistent)
+  int bfs_mode = 0;                        // 0 persistent, 1 level-stepped
+  unsigned* bfs_fb1 = nullptr;
+  void* bfs_ctrl = nullptr;                // BfsCtrl
+  // batched (multi-source) BFS buffers
+  unsigned long long* ms_visit = nullptr;
+  unsigned long long* ms_front0 = nullptr;
+  unsigned long long* ms_front1 = nullptr;
+  unsigned long long* ms_next = nullptr;
+  int* ms_q0 = nullptr;
+  int* ms_q1 = nullptr;
+  int* ms_srcs = nullptr;
+  int* ms_tmp = nullptr;                   // vertex-major levels for layout 1
+  size_t ms_tmp_len = 0;
+  void* ms_ctrl = nullptr;
+  int ms_n = 0;
+  double bfs_alpha = 14.0, bfs_beta = 24.0, msbfs_alpha = 12.0;
   unsigned* bfs_visited = nullptr;
   unsigned* bfs_front = nullptr;
   int* bfs_q[2] = {nullptr, nullptr};

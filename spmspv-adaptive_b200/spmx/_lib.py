@@ -64,6 +64,7 @@ _SIGS = {
     "spmx_input_csc": (c_int, [P, c_int, P, P, P]),
     "spmx_to_csc": (c_int, [P]),
     "spmx_get_csc": (c_int, [P, PP, PP, PP]),
+    "spmx_copy_csc": (c_int, [P, P, P, P]),
     "spmx_set_x": (c_int, [P, P]),
     "spmx_set_sparse_x": (c_int, [P, P, P, c_int]),
     "spmx_set_bitvector": (c_int, [P, P, c_int]),
@@ -115,6 +116,8 @@ _SIGS = {
     "spmx_run_adaptive": (c_int, [P, c_float, P, PI]),
     "spmx_run_kernel": (c_int, [P, c_int, c_float, P]),
     "spmx_bfs": (c_int, [P, c_int, P, PI]),
+    "spmx_set_bfs_mode": (c_int, [P, c_int]),
+    "spmx_bfs_batched": (c_int, [P, PI, c_int, P, c_int, PI]),
     "spmx_get_device_counts": (c_int, [P, PP]),
     "spmx_host_free": (None, [P]),
     "spmx_gen_rmat": (c_int, [c_int, c_int, c_double, c_double, c_double, c_u64, PI, PLL, PP, PP]),

@@ -100,12 +100,14 @@ class SpmspvHandle:
         check(lib.spmx_to_csc(self._h), "ToCSC")
 
     def get_csc(self):
-        """(row[nnz], colptr[n+1], val[nnz] or None) as new tensors."""
-        r, c, v = c_void_p(), c_void_p(), c_void_p()
-        check(lib.spmx_get_csc(self._h, ctypes.byref(r), ctypes.byref(c), ctypes.byref(v)), "get_csc")
-        torch.cuda.synchronize()
-        return (_copy_dev(r.value, self.nnz, torch.int32), _copy_dev(c.value, self.n + 1, torch.int32),
-                _copy_dev(v.value, self.nnz, torch.float32) if v.value else None)
+        """(row[nnz], colptr[n+1], val[nnz]) copied into new tensors."""
+        row = torch.empty(self.nnz, dtype=torch.int32, device="cuda")
+        colptr = torch.empty(self.n + 1, dtype=torch.int32, device="cuda")
+        val = torch.empty(self.nnz, dtype=torch.float32, device="cuda")
+        check(lib.spmx_copy_csc(self._h, _ptr(row) if self.nnz else None, _ptr(colptr),
+                                _ptr(val) if self.nnz else None), "copy_csc")
+        self._stream.synchronize()
+        return row, colptr, val
 
     # -- vectors -------------------------------------------------------------
     def set_x(self, x):
@@ -327,12 +329,14 @@ class SpmspvHandle:
         check(lib.spmx_bfs(self._h, int(source), _i32(levels), ctypes.byref(d)), "bfs")
         return d.value
 
+    def set_bfs_mode(self, mode):
+        check(lib.spmx_set_bfs_mode(self._h, int(mode)), "set_bfs_mode")
 
-def _copy_dev(ptr, count, dtype):
-    """Copy `count` elements at device address `ptr` into a new tensor."""
-    out = torch.empty(count, dtype=dtype, device="cuda")
-    if count:
-        nbytes = count * torch.tensor([], dtype=dtype).element_size()
-        cudart = torch.cuda.cudart()
-        cudart.cudaMemcpy(out.data_ptr(), ptr, nbytes, 3)  # device to device
-    return out
+    def bfs_batched(self, sources, levels, layout=1):
+        """Up to 64 sources in one launch; levels is [n*len(sources)] int32
+        (layout 1: source-major [s][v]; layout 0: vertex-major [v][s])."""
+        src = (c_int * len(sources))(*[int(s) for s in sources])
+        d = c_int()
+        check(lib.spmx_bfs_batched(self._h, src, len(sources), _i32(levels), int(layout),
+                                   ctypes.byref(d)), "bfs_batched")
+        return d.value

@@ -57,3 +57,53 @@ def test_bfs_rmat_larger_both_directions(torch_cuda):
     lv, d = _bfs(h, 0, g.n, torch)
     e, ed = orc.bfs_queue(g.n, g.rowptr, g.col, 0)
     assert np.array_equal(lv, e) and d == ed
+
+
+def test_bfs_level_stepped_mode(torch_cuda):
+    torch = torch_cuda
+    from spmx import gen
+    g = gen.rmat(14, 16, seed=1)
+    h = make_handle(g, torch, csc=False, hola=False)
+    h.set_bfs_mode(1)
+    lv, d = _bfs(h, 0, g.n, torch)
+    e, ed = orc.bfs_queue(g.n, g.rowptr, g.col, 0)
+    assert np.array_equal(lv, e) and d == ed
+
+
+@pytest.mark.parametrize("layout", [0, 1])
+def test_batched_bfs_matches_plain_runs(torch_cuda, layout):
+    """64 sources in one launch == 64 single-source traversals, bit for bit."""
+    torch = torch_cuda
+    from spmx import gen
+    g = gen.rmat(14, 16, seed=1)
+    h = make_handle(g, torch, csc=False, hola=False)
+    rng = np.random.default_rng(3)
+    deg = np.diff(g.rowptr)
+    srcs = rng.choice(np.nonzero(deg > 0)[0], 64, replace=False).tolist()
+    srcs[5] = srcs[4]  # a repeated source shares its frontier word
+    srcs[63] = int(np.nonzero(deg == 0)[0][0]) if (deg == 0).any() else srcs[63]
+    lv = torch.empty(64 * g.n, dtype=torch.int32, device="cuda")
+    depth = h.bfs_batched(srcs, lv, layout=layout)
+    h.check_device_error()
+    got = lv.cpu().numpy().reshape((64, g.n) if layout == 1 else (g.n, 64))
+    if layout == 0:
+        got = got.T
+    dmax = 0
+    for s, src in enumerate(srcs):
+        e, ed = orc.bfs_queue(g.n, g.rowptr, g.col, src)
+        assert np.array_equal(got[s], e), s
+        dmax = max(dmax, ed)
+    assert depth == dmax
+
+
+def test_batched_bfs_small_graphs(torch_cuda):
+    torch = torch_cuda
+    g = sym_graph(300, [(i, i + 1) for i in range(299)] + [(0, 150)])
+    h = make_handle(g, torch, csc=False, hola=False)
+    srcs = [0, 299, 150, 77]
+    lv = torch.empty(len(srcs) * g.n, dtype=torch.int32, device="cuda")
+    h.bfs_batched(srcs, lv, layout=1)
+    got = lv.cpu().numpy().reshape(len(srcs), g.n)
+    for s, src in enumerate(srcs):
+        e, _ = orc.bfs_queue(g.n, g.rowptr, g.col, src)
+        assert np.array_equal(got[s], e)
