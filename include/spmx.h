@@ -287,6 +287,18 @@ int spmx_set_bfs_mode(spmx_handle_t h, int mode);
 int spmx_bfs_batched(spmx_handle_t h, const int* srcs, int nsrc, int* d_levels,
                      int layout, int* depth);
 
+/* ======================= adjoint (FP32) ==================================== */
+/* No reference counterpart (the reference has no differentiation).  For
+ * y = A x and an upstream gradient dy[m]: dx[n] = A^T dy and dvals[nnz] =
+ * dy[row_k] * x[col_k] on the CSR pattern, in one pass over the matrix.
+ * Either output may be NULL.  Uses the Hola chunk table (built on demand). */
+int spmx_spmv_backward(spmx_handle_t h, const float* d_x, const float* d_dy,
+                       float* d_dx, float* d_dvals);
+/* the same with a sparse dy (keys = rows); dvals is zero outside dy's rows */
+int spmx_spmv_backward_sparse(spmx_handle_t h, const float* d_x,
+                              const int* d_dy_key, const float* d_dy_val,
+                              int dy_nnz, float* d_dx, float* d_dvals);
+
 /* ======================= device counters ================================== */
 /* device pointers to the handle's counters: [0] y_nnz of the last SpMSpV,
  * [1] bin_len of the last scan, [2] x_nnz after dense2sparse */

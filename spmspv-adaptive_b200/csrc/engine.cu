@@ -655,6 +655,49 @@ extern "C" int spmx_spmspv(spmx_handle_t h, float alpha, float* y) {
 }
 
 // ---------------------------------------------------------------------------
+// adjoint of y = alpha*A*x: dx = alpha*A^T dy, dvals = alpha*dy[row]*x[col]
+// (alpha folded into dy by the caller's choice of dy; here alpha = 1)
+// ---------------------------------------------------------------------------
+extern "C" int spmx_spmv_backward(spmx_handle_t h, const float* x, const float* dy, float* dx,
+                                  float* dvals) {
+  SPMX_CHECK_HANDLE(h);
+  if (!h->has_csr || (!h->val && h->nnz > 0))
+    return set_error(SPMX_ERR_NOT_READY, "backward needs the CSR input with values");
+  if (!dy || (dvals && !x)) return set_error(SPMX_ERR_INVALID_VALUE, "NULL x / dy");
+  if (!h->hola_ready || h->hola.K != 2048) {
+    const int vt = h->hola_vt;
+    h->hola_vt = 8;
+    const int rc = spmx_hola_preprocess(h);
+    h->hola_vt = vt;
+    SPMX_TRY(rc);
+  }
+  cudaStream_t st = h->stream;
+  if (dx) SPMX_CUDA(cudaMemsetAsync(dx, 0, 4 * (size_t)h->n, st));
+  if (launch_spmv_backward(h->m, h->n, h->nnz, h->rowptr, h->col, h->val, x, dy, h->hola, dx,
+                           dvals, h->d_err, st))
+    return set_error(SPMX_ERR_INVALID_VALUE, "backward chunk geometry");
+  return launch_ok("spmv backward");
+}
+
+extern "C" int spmx_spmv_backward_sparse(spmx_handle_t h, const float* x, const int* dy_key,
+                                         const float* dy_val, int dy_nnz, float* dx,
+                                         float* dvals) {
+  SPMX_CHECK_HANDLE(h);
+  if (!h->has_csr || (!h->val && h->nnz > 0))
+    return set_error(SPMX_ERR_NOT_READY, "backward needs the CSR input with values");
+  if (dy_nnz < 0 || dy_nnz > h->m) return set_error(SPMX_ERR_INVALID_VALUE, "dy_nnz must be in [0, m]");
+  if (dy_nnz > 0 && (!dy_key || !dy_val)) return set_error(SPMX_ERR_INVALID_VALUE, "NULL dy");
+  if (dvals && !x) return set_error(SPMX_ERR_INVALID_VALUE, "NULL x");
+  cudaStream_t st = h->stream;
+  if (dx) SPMX_CUDA(cudaMemsetAsync(dx, 0, 4 * (size_t)h->n, st));
+  if (dvals && h->nnz) SPMX_CUDA(cudaMemsetAsync(dvals, 0, 4 * (size_t)h->nnz, st));
+  const int g = pow2_group(h->m ? (double)h->nnz / h->m : 1.0);
+  launch_spmv_backward_sparse(h->m, h->n, h->rowptr, h->col, h->val, x, dy_nnz, dy_key, dy_val,
+                              g, dx, dvals, h->d_err, st);
+  return launch_ok("spmv backward (sparse dy)");
+}
+
+// ---------------------------------------------------------------------------
 // CSC SpMSpV
 // ---------------------------------------------------------------------------
 int csc_bucket_impl(spmx_handle_t h, float alpha, float* y, int* ykey, float* yval,

@@ -37,6 +37,16 @@ int launch_chunk_rows(int m, const int* rowptr, int K, int nchunks,
                       int* chunk_row, cudaStream_t st);
 int hola_chunk_nnz(int vt);
 
+// ---- adjoint.cu
+int launch_spmv_backward(int m, int n, int nnz, const int* rowptr, const int* col,
+                         const float* val, const float* x, const float* dy,
+                         const HolaTables& t, float* dx, float* dvals, int* err,
+                         cudaStream_t st);
+int launch_spmv_backward_sparse(int m, int n, const int* rowptr, const int* col,
+                                const float* val, const float* x, int dy_nnz,
+                                const int* dy_key, const float* dy_val, int group,
+                                float* dx, float* dvals, int* err, cudaStream_t st);
+
 // ---- lookback scratch shared by the single-pass scans
 struct ScanScratch {
   unsigned long long* status;  // tile status words

@@ -119,6 +119,8 @@ _SIGS = {
     "spmx_set_bfs_mode": (c_int, [P, c_int]),
     "spmx_bfs_batched": (c_int, [P, PI, c_int, P, c_int, PI]),
     "spmx_get_device_counts": (c_int, [P, PP]),
+    "spmx_spmv_backward": (c_int, [P, P, P, P, P]),
+    "spmx_spmv_backward_sparse": (c_int, [P, P, P, P, c_int, P, P]),
     "spmx_host_free": (None, [P]),
     "spmx_gen_rmat": (c_int, [c_int, c_int, c_double, c_double, c_double, c_u64, PI, PLL, PP, PP]),
     "spmx_gen_zipf_rows": (c_int, [c_int, c_double, c_int, c_int, c_u64, PLL, PP, PP, PP]),

@@ -323,6 +323,16 @@ class SpmspvHandle:
     def run_kernel(self, kid, alpha, y):
         check(lib.spmx_run_kernel(self._h, int(kid), float(alpha), _f32(y)), "run_kernel")
 
+    # -- adjoint -----------------------------------------------------------------------
+    def spmv_backward(self, x, dy, dx=None, dvals=None):
+        check(lib.spmx_spmv_backward(self._h, _f32(x), _f32(dy), _f32(dx), _f32(dvals)),
+              "spmv_backward")
+
+    def spmv_backward_sparse(self, x, dy_key, dy_val, dy_nnz, dx=None, dvals=None):
+        check(lib.spmx_spmv_backward_sparse(self._h, _f32(x), _i32(dy_key), _f32(dy_val),
+                                            int(dy_nnz), _f32(dx), _f32(dvals)),
+              "spmv_backward_sparse")
+
     # -- BFS ---------------------------------------------------------------------------
     def bfs(self, source, levels):
         d = c_int()
