@@ -239,6 +239,25 @@ int spmx_csc_twolayer_sort(spmx_handle_t h, int binlen_ready, float alpha,
 int spmx_csc_bucket(spmx_handle_t h, float alpha, int* ynnz, float* d_y,
                     int* d_y_key, float* d_y_val, int buckets);
 
+/* No counterpart in the reference.  The load-balanced (merge-path) CSC
+ * SpMSpV with atomic write-back, y = alpha*A*x, for callers that cannot let
+ * the library allocate device memory (a host framework that owns the device
+ * heap through its own allocator; a latency-critical loop in which cudaMalloc
+ * / cudaFree could synchronise the device).  No handle: the caller passes the
+ * CSC (csc_row = row indices [nnz], csc_col = column pointer [n+1]), the sparse
+ * x and the dense output y[m]; all scratch lives in one fixed array of device
+ * global memory (about 8.6 MB on every GPU that loads the library, held until
+ * the process exits).  Limits: x_nnz <= 1,048,576 and nnz + x_nnz <=
+ * 134,217,728; larger calls return SPMX_ERR_INVALID_VALUE without launching.
+ * The first call on a device looks up the array's device address (make it
+ * before any stream capture).  Calls share the array: calls that overlap on
+ * the GPU race, so serialise them (e.g. on one stream).  Nothing is allocated,
+ * no cudaMalloc / cudaFree is called; work is queued on `stream`. */
+int spmx_spmspv_csc_noalloc(int m, int n, int nnz, const int* d_csc_row,
+                            const int* d_csc_col, const float* d_csc_val,
+                            int x_nnz, const int* d_x_key, const float* d_x_val,
+                            float alpha, float* d_y, void* stream);
+
 /* ======================= features / selector ============================== */
 /* computeBinlenVer2 — H:2703-2723 (sum of the column lengths of x's keys) */
 int spmx_compute_binlen(spmx_handle_t h, long long* bin_len);

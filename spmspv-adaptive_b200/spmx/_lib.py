@@ -105,6 +105,7 @@ _SIGS = {
     "spmx_csc_twolayer_atomic_keyval": (c_int, [P, c_int, c_float, PI, P, P, P]),
     "spmx_csc_twolayer_sort": (c_int, [P, c_int, c_float, PI, P, P, P]),
     "spmx_csc_bucket": (c_int, [P, c_float, PI, P, P, P, c_int]),
+    "spmx_spmspv_csc_noalloc": (c_int, [c_int, c_int, c_int, P, P, P, c_int, P, P, c_float, P, P]),
     "spmx_compute_binlen": (c_int, [P, PLL]),
     "spmx_compute_gm": (c_int, [P, PD]),
     "spmx_mat_features": (c_int, [P, PD]),
