@@ -60,6 +60,7 @@ extern "C" {
 /* ---- SpMV back-ends for spmx_spmv / spmx_spmspv (set_spmv_type, H:1767) */
 #define SPMX_SPMV_HOLA 0
 #define SPMX_SPMV_CSR5 1
+#define SPMX_SPMV_TILED 2  /* row-block x column-window tiles (no reference counterpart) */
 
 /* ---- CSC SpMSpV work distributions and write-backs (H:1824-2201) */
 #define SPMX_CSC_NAIVE     0  /* group of threads per x nonzero            */
@@ -175,7 +176,16 @@ int spmx_csr5_preprocess(spmx_handle_t h);
 int spmx_csr5_postprocess(spmx_handle_t h);
 /* the sigma in use (after CSR5Preprocess) or that the auto rule would pick */
 int spmx_csr5_sigma(spmx_handle_t h, int* sigma);
-/* set_spmv_type — H:1767 (0 Hola, 1 CSR5) */
+/* Tiled SpMV format (no reference counterpart; a third back-end for
+ * spmv / spmspv): nonzeros grouped into tiles of rb_rows rows x win columns
+ * (powers of two, rb_rows <= 32768, win <= 65536) so that each CTA's x
+ * accesses stay inside one window cached in L1 while y accumulates in shared
+ * memory; chunk = nonzeros per work unit.  0 selects the defaults. */
+int spmx_tiled_preprocess(spmx_handle_t h, int rb_rows, int win, int chunk);
+int spmx_tiled_postprocess(spmx_handle_t h);
+int spmx_tiledspmv(spmx_handle_t h, float alpha, float* d_y);
+int spmx_tiledspmspv(spmx_handle_t h, float alpha, float* d_y);
+/* set_spmv_type — H:1767 (0 Hola, 1 CSR5, 2 tiled) */
 int spmx_set_spmv_type(spmx_handle_t h, int code);
 
 /* ======================= SpMV / CSR SpMSpV (y = alpha*A*x) =============== */

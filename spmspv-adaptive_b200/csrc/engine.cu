@@ -166,6 +166,8 @@ static void free_csc_scratch(spmx_handle_t h) {
 
 extern "C" int spmx_hola_postprocess(spmx_handle_t h);
 extern "C" int spmx_csr5_postprocess(spmx_handle_t h);
+extern "C" int spmx_tiled_postprocess(spmx_handle_t h);
+int tiled_spmv_impl(spmx_handle_t h, float alpha, float* y, bool gated);
 
 extern "C" int spmx_destroy(spmx_handle_t h) {
   if (!h) return SPMX_SUCCESS;
@@ -180,6 +182,7 @@ extern "C" int spmx_destroy(spmx_handle_t h) {
   free_sort_scratch(h);
   spmx_hola_postprocess(h);
   spmx_csr5_postprocess(h);
+  spmx_tiled_postprocess(h);
   dfree(h->bfs_visited); dfree(h->bfs_front); dfree(h->bfs_q[0]); dfree(h->bfs_q[1]);
   dfree(h->bfs_cnt); dfree(h->bfs_edges); dfree(h->bfs_fb1); dfree(h->bfs_ctrl);
   dfree(h->ms_visit); dfree(h->ms_front0); dfree(h->ms_front1); dfree(h->ms_next);
@@ -580,8 +583,8 @@ extern "C" int spmx_hola_postprocess(spmx_handle_t h) {
 
 extern "C" int spmx_set_spmv_type(spmx_handle_t h, int code) {
   SPMX_CHECK_HANDLE(h);
-  if (code != SPMX_SPMV_HOLA && code != SPMX_SPMV_CSR5)
-    return set_error(SPMX_ERR_INVALID_VALUE, "spmv type must be 0 (Hola) or 1 (CSR5)");
+  if (code != SPMX_SPMV_HOLA && code != SPMX_SPMV_CSR5 && code != SPMX_SPMV_TILED)
+    return set_error(SPMX_ERR_INVALID_VALUE, "spmv type must be 0 (Hola), 1 (CSR5) or 2 (tiled)");
   h->spmv_type = code;
   return SPMX_SUCCESS;
 }
@@ -647,10 +650,12 @@ extern "C" int spmx_csr5spmspv(spmx_handle_t h, float alpha, float* y) {
 
 extern "C" int spmx_spmv(spmx_handle_t h, float alpha, float* y) {
   SPMX_CHECK_HANDLE(h);
+  if (h->spmv_type == SPMX_SPMV_TILED) return tiled_spmv_impl(h, alpha, y, false);
   return h->spmv_type == SPMX_SPMV_HOLA ? spmx_holaspmv(h, alpha, y) : spmx_csr5spmv(h, alpha, y);
 }
 extern "C" int spmx_spmspv(spmx_handle_t h, float alpha, float* y) {
   SPMX_CHECK_HANDLE(h);
+  if (h->spmv_type == SPMX_SPMV_TILED) return tiled_spmv_impl(h, alpha, y, true);
   return h->spmv_type == SPMX_SPMV_HOLA ? spmx_holaspmspv(h, alpha, y) : spmx_csr5spmspv(h, alpha, y);
 }
 

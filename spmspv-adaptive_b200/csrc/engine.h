@@ -73,8 +73,9 @@ struct spmx_handle_s {
   int* bk_cursor = nullptr;
   int buckets = 0;            // 0 = default (256)
 
-  // CSR5 tile tables (csr5.cu)
+  // CSR5 tile tables (csr5.cu) and tiled-SpMV tables (tiled.cu)
   void* csr5 = nullptr;
+  void* tiled = nullptr;
 
   // Hola tables
   spmx::HolaTables hola{};

@@ -38,7 +38,7 @@ ERR_NOT_READY = -25
 ERR_NO_DEVICE = -26
 
 VEC_SPARSE, VEC_DENSE, VEC_BITARRAY = 0, 1, 2
-SPMV_HOLA, SPMV_CSR5 = 0, 1
+SPMV_HOLA, SPMV_CSR5, SPMV_TILED = 0, 1, 2
 CSC_NAIVE, CSC_LB_MERGE, CSC_LB_TWOLAYER, CSC_BUCKET = 0, 1, 2, 3
 WB_ATOMIC, WB_SORT = 0, 1
 (K_CSC_NAIVE_SORT, K_CSC_NAIVE_ATOMIC, K_CSC_LB_SORT, K_CSC_LB_ATOMIC,
@@ -86,6 +86,10 @@ _SIGS = {
     "spmx_csr5_postprocess": (c_int, [P]),
     "spmx_csr5_sigma": (c_int, [P, PI]),
     "spmx_set_spmv_type": (c_int, [P, c_int]),
+    "spmx_tiled_preprocess": (c_int, [P, c_int, c_int, c_int]),
+    "spmx_tiled_postprocess": (c_int, [P]),
+    "spmx_tiledspmv": (c_int, [P, c_float, P]),
+    "spmx_tiledspmspv": (c_int, [P, c_float, P]),
     "spmx_naivespmv": (c_int, [P, c_float, P]),
     "spmx_holaspmv": (c_int, [P, c_float, P]),
     "spmx_csr5spmv": (c_int, [P, c_float, P]),

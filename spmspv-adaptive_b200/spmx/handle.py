@@ -182,6 +182,18 @@ class SpmspvHandle:
     def CSR5Postprocess(self):
         check(lib.spmx_csr5_postprocess(self._h), "CSR5Postprocess")
 
+    def tiledPreprocess(self, rb_rows=0, win=0, chunk=0):
+        check(lib.spmx_tiled_preprocess(self._h, int(rb_rows), int(win), int(chunk)), "tiledPreprocess")
+
+    def tiledPostprocess(self):
+        check(lib.spmx_tiled_postprocess(self._h), "tiledPostprocess")
+
+    def tiledspmv(self, alpha, y):
+        check(lib.spmx_tiledspmv(self._h, float(alpha), _f32(y)), "tiledspmv")
+
+    def tiledspmspv(self, alpha, y):
+        check(lib.spmx_tiledspmspv(self._h, float(alpha), _f32(y)), "tiledspmspv")
+
     def set_spmv_type(self, code):
         check(lib.spmx_set_spmv_type(self._h, int(code)), "set_spmv_type")
 

@@ -159,3 +159,51 @@ def test_csr5_zipf_full_size(torch_cuda):
     y64, mag = orc.spmv_f64(A.rowptr, A.col, A.val, x)
     ok, _ = orc.within_tol(y.cpu().numpy(), y64, mag, RTOL)
     assert ok
+
+
+@pytest.mark.parametrize("name,A", CASES, ids=[c[0] for c in CASES])
+@pytest.mark.parametrize("rb,win", [(256, 512), (1024, 256), (16384, 16384)])
+def test_tiled_spmv(torch_cuda, name, A, rb, win):
+    torch = torch_cuda
+    h = make_handle(A, torch, csc=False, hola=False)
+    h.tiledPreprocess(rb, win, 300 if rb < 16384 else 0)
+    x = np.random.default_rng(17).uniform(-1, 1, A.n).astype(np.float32)
+    h.set_x(dev(x, torch))
+    y64, mag = orc.spmv_f64(A.rowptr, A.col, A.val, x, alpha=-1.5)
+    for rep in range(2):
+        y = torch.full((A.m,), 3.0, device="cuda")
+        h.tiledspmv(-1.5, y)
+        h.check_device_error()
+        ok, _ = orc.within_tol(y.cpu().numpy(), y64, mag, RTOL)
+        assert ok, orc.max_scaled_err(y.cpu().numpy(), y64, mag)
+    # bitmap-gated form through the dispatcher
+    h.set_spmv_type(2)
+    rng = np.random.default_rng(2)
+    k = max(1, A.n // 30)
+    key = np.sort(rng.choice(A.n, k, replace=False)).astype(np.int32)
+    val = rng.uniform(-1, 1, k).astype(np.float32)
+    kd, vd = dev(key, torch), dev(val, torch)
+    h.set_sparse_x(kd, vd, k)
+    h.sparse2bitarray()
+    y = torch.empty(A.m, device="cuda")
+    h.spmspv(1.0, y)
+    xd, bits = orc.sparse2dense_bits(A.n, key, val)
+    y64, mag = orc.spmv_f64(A.rowptr, A.col, A.val, xd, bits=bits.view(np.int32))
+    ok, _ = orc.within_tol(y.cpu().numpy(), y64, mag, RTOL)
+    assert ok
+
+
+def test_tiled_zipf_full_size(torch_cuda):
+    torch = torch_cuda
+    from spmx import gen
+    A = gen.zipf_1m()
+    h = make_handle(A, torch, csc=False, hola=False)
+    h.tiledPreprocess()
+    x = np.random.default_rng(2).uniform(-1, 1, A.n).astype(np.float32)
+    h.set_x(dev(x, torch))
+    y = torch.empty(A.m, device="cuda")
+    h.tiledspmv(1.0, y)
+    h.check_device_error()
+    y64, mag = orc.spmv_f64(A.rowptr, A.col, A.val, x)
+    ok, _ = orc.within_tol(y.cpu().numpy(), y64, mag, RTOL)
+    assert ok
