@@ -332,6 +332,7 @@ def run_ours(args, world, rank, local):
 
     # --- BFS on R-MAT scale 14 (plain), bit-exact check against the oracle ---
     bfs = run_bfs_plain(torch, dev, stream, args) if rank == 0 and not args.no_bfs else None
+    bfs64 = run_bfs_batched(torch, dev, stream, args) if rank == 0 and not args.no_bfs else None
 
     line = None
     if rank == 0:
@@ -357,6 +358,7 @@ def run_ours(args, world, rank, local):
             "sweep": sweep,
             "cpu_baseline": cpu,
             "bfs": bfs,
+            "batched_bfs": bfs64,
         }
         print(json.dumps(line), flush=True)
     h.Destroy()
@@ -395,6 +397,55 @@ def run_bfs_plain(torch, dev, stream, args):
             "bit_exact": bool(np.array_equal(got, ref)), "edges": edges}
 
 
+def run_bfs_batched(torch, dev, stream, args):
+    """R-MAT scale 22 (edge factor 16, seed 3), 64 sources drawn (seed 3) from
+    vertices of degree > 0: one batched launch vs 64 plain traversals."""
+    import spmx
+    from spmx import gen
+    g = gen.rmat(22, 16, seed=3)
+    rng = np.random.default_rng(3)
+    deg = np.diff(g.rowptr)
+    srcs = rng.choice(np.nonzero(deg > 0)[0], 64, replace=False).tolist()
+    rp = torch.from_numpy(g.rowptr).to(dev)
+    cl = torch.from_numpy(g.col).to(dev)
+    h = spmx.SpmspvHandle(g.m, g.n, g.nnz, stream=stream)
+    h.InputCSR(g.nnz, rp, cl, None)
+    n = g.n
+    lv_b = torch.empty(64 * n, dtype=torch.int32, device=dev)
+    lv_p = torch.empty(64 * n, dtype=torch.int32, device=dev)
+    s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    reps = 3
+    h.bfs_batched(srcs, lv_b, layout=1)
+    tb = []
+    for _ in range(reps):
+        s.record(stream)
+        h.bfs_batched(srcs, lv_b, layout=1, sync=False)
+        e.record(stream)
+        stream.synchronize()
+        tb.append(s.elapsed_time(e))
+    for i, src in enumerate(srcs[:2]):
+        h.bfs(src, lv_p[i * n:(i + 1) * n])
+    tp = []
+    for _ in range(reps):
+        s.record(stream)
+        for i, src in enumerate(srcs):
+            h.bfs(src, lv_p[i * n:(i + 1) * n], sync=False)
+        e.record(stream)
+        stream.synchronize()
+        tp.append(s.elapsed_time(e))
+    h.check_device_error()
+    exact = bool(torch.equal(lv_b, lv_p))
+    degd = torch.from_numpy(deg.astype(np.int64)).to(dev)
+    reached = (lv_p.view(64, n) >= 0).to(torch.int64)
+    edges = int((reached * degd).sum().item()) // 2
+    mb, mp = statistics.median(tb), statistics.median(tp)
+    h.Destroy()
+    return {"graph": "rmat scale 22, edge factor 16, seed 3, 64 sources (seed 3)",
+            "batched_ms": mb, "plain64_ms": mp, "edges": edges,
+            "batched_gteps": edges / (mb * 1e-3) / 1e9, "plain64_gteps": edges / (mp * 1e-3) / 1e9,
+            "speedup": mp / mb, "bit_exact_vs_plain": exact}
+
+
 def cpu_baseline(A, xs, binl):
     """The reference's serial CPU routines (restated), one core, one sweep."""
     import oracle.oracle as orc
@@ -422,8 +473,8 @@ def cpu_baseline(A, xs, binl):
             "ms": best * 1e3}
 
 
-ONLY = ("hola-spmv", "csr5-spmv", "naive-spmv", "hola-spmspv", "csc-lb-atomic", "csc-naive-atomic",
-        "csc-bucket", "csc-lb-sort", "bfs-rmat14")
+ONLY = ("hola-spmv", "csr5-spmv", "naive-spmv", "tiled-spmv", "hola-spmspv", "csc-lb-atomic",
+        "csc-naive-atomic", "csc-bucket", "csc-lb-sort", "bfs-rmat14", "bfs-batched")
 
 
 def run_only(args):
@@ -436,6 +487,9 @@ def run_only(args):
     if args.only == "bfs-rmat14":
         print(json.dumps(run_bfs_plain(torch, dev, stream, args)))
         return 0
+    if args.only == "bfs-batched":
+        print(json.dumps(run_bfs_batched(torch, dev, stream, args)))
+        return 0
     A, xs = make_inputs()
     d = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)  # noqa: E731
     rp, cl, vl = d(A.rowptr), d(A.col), d(A.val)
@@ -444,6 +498,7 @@ def run_only(args):
     h.ToCSC()
     h.holaPreprocess()
     h.CSR5Preprocess()
+    h.tiledPreprocess()
     h.allocPreBuffer()
     dens = 1.0 if args.only.endswith("spmv") else args.density
     k = [x for x in xs if abs(x[0] - dens) < 1e-12][0]
@@ -457,6 +512,7 @@ def run_only(args):
         "hola-spmv": lambda: h.holaspmv(1.0, y),
         "csr5-spmv": lambda: h.csr5spmv(1.0, y),
         "naive-spmv": lambda: h.naivespmv(1.0, y),
+        "tiled-spmv": lambda: h.tiledspmv(1.0, y),
         "hola-spmspv": lambda: h.holaspmspv(1.0, y),
         "csc-lb-atomic": lambda: h.spmspv_csc(1, 0, 1.0, y, sync=False),
         "csc-naive-atomic": lambda: h.spmspv_csc(0, 0, 1.0, y, sync=False),

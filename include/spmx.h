@@ -287,6 +287,10 @@ int spmx_features(spmx_handle_t h, double out[SPMX_NUM_FEATURES]);
  * TEST/new_test_app.cu:121-131 (stubs there); a decision tree here.
  * kernel_id receives one of SPMX_K_*. */
 int spmx_select(spmx_handle_t h, int* kernel_id);
+/* the feature vector spmx_select decides on: the 23-entry schema with the
+ * host-known values (bin_len estimated as x_nnz*nnz/n unless measured, the
+ * matrix's longest column in the "max" slot, 0 in the "min" slot) */
+int spmx_selector_inputs(spmx_handle_t h, double out[SPMX_NUM_FEATURES]);
 /* the selector on a caller-supplied feature vector (host only, no handle, no
  * GPU): predictSolution / predictWorkloadDistribution / predictWritingBack
  * combined (TEST/new_test_app.cu:121-131) */
@@ -295,6 +299,15 @@ int spmx_select_features(const double f[SPMX_NUM_FEATURES], int* kernel_id);
  * select, convert x as the chosen kernel needs (s2d / s2a), run it.
  * d_y (dense, m) always receives y; kernel_used (host, may be NULL). */
 int spmx_run_adaptive(spmx_handle_t h, float alpha, float* d_y, int* kernel_used);
+/* Per-matrix autotuner (no reference counterpart beyond the reference's
+ * Hola-vs-CSR5 timing, TEST/generate_model_data.cu:487-516): times the
+ * load-balanced SpMV back-ends (Hola 4/8/16 nonzeros per thread, CSR5, tiled
+ * geometries), the naive kernels' lanes per row / column, merge-path vs
+ * fixed-nonzero CSC blocks and the bucket count, and keeps the fastest.
+ * cache_path (may be NULL): a text file of tuned parameters keyed by a matrix
+ * fingerprint; a hit applies them without timing.  spmv_type_out (may be NULL)
+ * receives the chosen SpMV back-end. */
+int spmx_autotune(spmx_handle_t h, const char* cache_path, int* spmv_type_out);
 /* run one of the eight kernels by id (used by the exhaustive timing harness) */
 int spmx_run_kernel(spmx_handle_t h, int kernel_id, float alpha, float* d_y);
 

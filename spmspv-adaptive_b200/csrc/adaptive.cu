@@ -235,17 +235,24 @@ static int compute_col_max(spmx_handle_t h) {
   return launch_ok("column features");
 }
 
-extern "C" int spmx_select(spmx_handle_t h, int* kernel_id) {
+extern "C" int spmx_selector_inputs(spmx_handle_t h, double out[SPMX_NUM_FEATURES]) {
   SPMX_CHECK_HANDLE(h);
-  if (!kernel_id) return set_error(SPMX_ERR_INVALID_VALUE, "kernel_id is NULL");
+  if (!out) return set_error(SPMX_ERR_INVALID_VALUE, "out is NULL");
   SPMX_TRY(compute_mat_features(h));
   SPMX_TRY(compute_col_max(h));
-  double f[SPMX_NUM_FEATURES];
   const double est = h->bin_len >= 0 ? (double)h->bin_len
                                       : (h->n ? (double)h->x_nnz * h->nnz / h->n : 0.0);
   // x's own longest / shortest column need a device pass; the matrix's
   // longest column bounds the former, the latter is not used
-  fill_features(h, est, h->col_max, 0, f);
+  fill_features(h, est, h->col_max, 0, out);
+  return SPMX_SUCCESS;
+}
+
+extern "C" int spmx_select(spmx_handle_t h, int* kernel_id) {
+  SPMX_CHECK_HANDLE(h);
+  if (!kernel_id) return set_error(SPMX_ERR_INVALID_VALUE, "kernel_id is NULL");
+  double f[SPMX_NUM_FEATURES];
+  SPMX_TRY(spmx_selector_inputs(h, f));
   *kernel_id = spmx_select_kernel(f);
   return SPMX_SUCCESS;
 }

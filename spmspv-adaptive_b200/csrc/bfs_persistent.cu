@@ -280,18 +280,25 @@ __global__ void levels_transpose_kernel(int n, int ns, const int* __restrict__ v
 }
 
 // --------------------------------------------------------------------------
+// Co-resident grid for a cooperative launch, scaled to the work: every CTA
+// joins every grid barrier, so a small graph gets few CTAs (one per SM down
+// to 1024 vertices per CTA) and a large one the whole resident capacity.
 template <class K>
-static int max_coop_grid(K kernel, int num_sms) {
+static int coop_grid(K kernel, int num_sms, long long work_items) {
   int per = 0;
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, 256, 0) != cudaSuccess) {
     cudaGetLastError();
     return 0;
   }
-  return per * num_sms;
+  const long long cap = (long long)per * num_sms;
+  long long want = (work_items + 1023) / 1024;
+  if (want < num_sms) want = num_sms;
+  if (want > cap) want = cap;
+  return (int)want;
 }
 
 int launch_bfs_persistent(const BfsPersistentArgs& a, cudaStream_t st) {
-  const int grid = max_coop_grid(bfs_persistent_kernel, a.num_sms);
+  const int grid = coop_grid(bfs_persistent_kernel, a.num_sms, a.n);
   if (grid <= 0) return -1;
   cudaMemsetAsync(a.ctrl, 0, sizeof(BfsCtrl), st);
   note_launch(2);
@@ -316,7 +323,7 @@ int launch_bfs_persistent(const BfsPersistentArgs& a, cudaStream_t st) {
 }
 
 int launch_msbfs_persistent(const MsBfsArgs& a, cudaStream_t st) {
-  const int grid = max_coop_grid(msbfs_persistent_kernel, a.num_sms);
+  const int grid = coop_grid(msbfs_persistent_kernel, a.num_sms, a.n);
   if (grid <= 0) return -1;
   cudaMemsetAsync(a.ctrl, 0, sizeof(BfsCtrl), st);
   note_launch(2);

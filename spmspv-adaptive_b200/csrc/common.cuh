@@ -3,6 +3,7 @@
 #pragma once
 #include <cuda_runtime.h>
 #include <stdint.h>
+#include <utility>
 
 namespace spmx {
 
@@ -301,6 +302,38 @@ __device__ __forceinline__ bool grid_sync(const GridBarrier& b, int* err) {
   }
   __syncthreads();
   return s_ok != 0;
+}
+
+// ---------------------------------------------------------------------------
+// Launch with an L2 access-policy window: the window [base, base + bytes) is
+// marked persisting for this launch only (no stream state changes), so a
+// small gathered operand (the dense x, a frontier bitmap) stays in L2 while
+// the streamed matrix passes through it.  bytes == 0 launches plainly.
+// ---------------------------------------------------------------------------
+size_t l2_window_bytes(const void* base, size_t bytes);  // clamp; 0 = disabled
+
+template <class... KArgs, class... Args>
+cudaError_t launch_l2_window(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem,
+                             cudaStream_t st, const void* win_base, size_t win_bytes,
+                             Args&&... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  const size_t wb = win_base ? l2_window_bytes(win_base, win_bytes) : 0;
+  if (wb) {
+    attr[0].id = cudaLaunchAttributeAccessPolicyWindow;
+    attr[0].val.accessPolicyWindow.base_ptr = const_cast<void*>(win_base);
+    attr[0].val.accessPolicyWindow.num_bytes = wb;
+    attr[0].val.accessPolicyWindow.hitRatio = 1.0f;
+    attr[0].val.accessPolicyWindow.hitProp = cudaAccessPropertyPersisting;
+    attr[0].val.accessPolicyWindow.missProp = cudaAccessPropertyStreaming;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+  }
+  return cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
 }
 
 }  // namespace spmx

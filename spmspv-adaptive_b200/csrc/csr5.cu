@@ -124,11 +124,11 @@ csr5_spmv_kernel(int m, int n, int ntiles, const int* __restrict__ rowptr,
   bool seen = false;
 #pragma unroll
   for (int j = 0; j < SIGMA; ++j) {
-    const int c = __ldg(col5 + base + (size_t)j * 32);
+    const int c = __ldcs(col5 + base + (size_t)j * 32);
     double p = 0.0;
     if ((unsigned)c < (unsigned)n) {
       if (!GATED || ((__ldg((const unsigned*)xbits + (c >> 5)) >> (c & 31)) & 1u))
-        p = (double)__ldg(val5 + base + (size_t)j * 32) * (double)__ldg(x + c);
+        p = (double)__ldcs(val5 + base + (size_t)j * 32) * (double)__ldg(x + c);
     } else {
       flag_error(err, kDevErrOob);
     }
@@ -336,16 +336,21 @@ int csr5_spmv_impl(spmx_handle_t h, float alpha, float* y, bool gated) {
 #define SPMX_CSR5_CASE(S)                                                                 \
   case S:                                                                                \
     if (gated)                                                                           \
-      csr5_spmv_kernel<S, true><<<grid, 256, 0, st>>>(                                   \
-          h->m, h->n, t->ntiles, h->rowptr, t->col5, t->val5, t->bits, t->lane_rank,     \
-          t->nz_rows, t->m_nz, h->x_dense, xb, (double)alpha, y, t->carry, t->arrive,     \
+      e = launch_l2_window(csr5_spmv_kernel<S, true>, dim3(grid), dim3(256), 0, st,      \
+          h->x_dense, 4 * (size_t)h->n,                                                  \
+          h->m, h->n, t->ntiles, h->rowptr, (const int*)t->col5, (const float*)t->val5,  \
+          (const unsigned*)t->bits, (const int*)t->lane_rank, (const int*)t->nz_rows,    \
+          t->m_nz, (const float*)h->x_dense, xb, (double)alpha, y, t->carry, t->arrive,   \
           h->d_err);                                                                     \
     else                                                                                 \
-      csr5_spmv_kernel<S, false><<<grid, 256, 0, st>>>(                                  \
-          h->m, h->n, t->ntiles, h->rowptr, t->col5, t->val5, t->bits, t->lane_rank,     \
-          t->nz_rows, t->m_nz, h->x_dense, xb, (double)alpha, y, t->carry, t->arrive,     \
+      e = launch_l2_window(csr5_spmv_kernel<S, false>, dim3(grid), dim3(256), 0, st,     \
+          h->x_dense, 4 * (size_t)h->n,                                                  \
+          h->m, h->n, t->ntiles, h->rowptr, (const int*)t->col5, (const float*)t->val5,  \
+          (const unsigned*)t->bits, (const int*)t->lane_rank, (const int*)t->nz_rows,    \
+          t->m_nz, (const float*)h->x_dense, xb, (double)alpha, y, t->carry, t->arrive,   \
           h->d_err);                                                                     \
     break;
+  cudaError_t e = cudaSuccess;
   note_launch();
   switch (t->sigma) {
     SPMX_CSR5_CASE(4)
@@ -359,7 +364,7 @@ int csr5_spmv_impl(spmx_handle_t h, float alpha, float* y, bool gated) {
       return set_error(SPMX_ERR_INVALID_VALUE, "unsupported sigma");
   }
 #undef SPMX_CSR5_CASE
-  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) e = cudaGetLastError();
   if (e != cudaSuccess) return set_error(SPMX_ERR_CUDA, std::string("csr5 spmv: ") + cudaGetErrorString(e));
   return SPMX_SUCCESS;
 }

@@ -4,6 +4,8 @@
 // spmspv.h); line numbers are given per entry point in spmx.h.
 #include <algorithm>
 #include <atomic>
+#include <cstdlib>
+#include <mutex>
 #include <cmath>
 #include <cstring>
 #include <string>
@@ -42,6 +44,40 @@ void dfree(void* p) {
 }
 
 static std::atomic<unsigned long long> g_launches{0};
+
+// L2 persistence for gathered operands: on by default, SPMX_L2_WINDOW=0 turns
+// it off.  The first use on a device raises the CUDA context's persisting-L2
+// set-aside (a property of this process's context, released with it) to at
+// most 32 MiB.
+static std::mutex g_l2_mu;
+static int g_l2_state[64] = {0};       // 0 unknown, 1 ready, -1 unavailable
+static size_t g_l2_maxwin[64] = {0};
+
+size_t l2_window_bytes(const void* base, size_t bytes) {
+  static const bool enabled = [] {
+    const char* e = getenv("SPMX_L2_WINDOW");
+    return !(e && e[0] == '0');
+  }();
+  if (!enabled || !base || bytes == 0) return 0;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) { cudaGetLastError(); return 0; }
+  std::lock_guard<std::mutex> lock(g_l2_mu);
+  if (g_l2_state[dev] == 0) {
+    int maxwin = 0, maxpersist = 0;
+    cudaDeviceGetAttribute(&maxwin, cudaDevAttrMaxAccessPolicyWindowSize, dev);
+    cudaDeviceGetAttribute(&maxpersist, cudaDevAttrMaxPersistingL2CacheSize, dev);
+    size_t cur = 0;
+    cudaDeviceGetLimit(&cur, cudaLimitPersistingL2CacheSize);
+    const size_t want = std::min<size_t>((size_t)maxpersist, (size_t)32 << 20);
+    bool ok = maxwin > 0 && maxpersist > 0;
+    if (ok && cur < want) ok = cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, want) == cudaSuccess;
+    cudaGetLastError();
+    g_l2_maxwin[dev] = ok ? (size_t)maxwin : 0;
+    g_l2_state[dev] = ok ? 1 : -1;
+  }
+  if (g_l2_state[dev] != 1) return 0;
+  return std::min(bytes, g_l2_maxwin[dev]);
+}
 void note_launch(int k) { g_launches.fetch_add((unsigned long long)k, std::memory_order_relaxed); }
 
 int csc_lb_blocks_per_sm();

@@ -121,7 +121,7 @@ spmv_chunk_kernel(int m, int n, int nnz, const int* __restrict__ rowptr,
   if (vec_ok && s + K <= nnz && (VT % 4) == 0) {
 #pragma unroll
     for (int q = 0; q < VT / 4; ++q) {
-      const int4 c4 = __ldg(reinterpret_cast<const int4*>(col + base) + q);
+      const int4 c4 = __ldcs(reinterpret_cast<const int4*>(col + base) + q);
       const int cc[4] = {c4.x, c4.y, c4.z, c4.w};
       bool want[4];
       bool any = false;
@@ -133,7 +133,7 @@ spmv_chunk_kernel(int m, int n, int nnz, const int* __restrict__ rowptr,
         any |= want[t];
       }
       if (!GATED || any) {
-        const float4 v4 = __ldg(reinterpret_cast<const float4*>(val + base) + q);
+        const float4 v4 = __ldcs(reinterpret_cast<const float4*>(val + base) + q);
         const float vv[4] = {v4.x, v4.y, v4.z, v4.w};
 #pragma unroll
         for (int t = 0; t < 4; ++t)
@@ -259,14 +259,15 @@ int launch_spmv_hola(const SpmvArgs& a, const HolaTables& t, cudaStream_t st) {
 #define SPMX_HOLA_CASE(VT)                                                       \
   case VT:                                                                       \
     if (a.bits)                                                                  \
-      spmv_chunk_kernel<NT, VT, true><<<t.nchunks, NT, 0, st>>>(                 \
-          a.m, a.n, a.nnz, a.rowptr, a.col, a.val, a.x, a.bits, a.alpha, a.y,    \
-          t.chunk_row, t.carry, t.arrive, vec_ok, a.err);                        \
+      e = launch_l2_window(spmv_chunk_kernel<NT, VT, true>, dim3(t.nchunks), dim3(NT), 0, st, \
+          a.x, 4 * (size_t)a.n, a.m, a.n, a.nnz, a.rowptr, a.col, a.val, a.x, a.bits, \
+          a.alpha, a.y, (const int*)t.chunk_row, t.carry, t.arrive, vec_ok, a.err); \
     else                                                                         \
-      spmv_chunk_kernel<NT, VT, false><<<t.nchunks, NT, 0, st>>>(                \
-          a.m, a.n, a.nnz, a.rowptr, a.col, a.val, a.x, a.bits, a.alpha, a.y,    \
-          t.chunk_row, t.carry, t.arrive, vec_ok, a.err);                        \
+      e = launch_l2_window(spmv_chunk_kernel<NT, VT, false>, dim3(t.nchunks), dim3(NT), 0, st, \
+          a.x, 4 * (size_t)a.n, a.m, a.n, a.nnz, a.rowptr, a.col, a.val, a.x, a.bits, \
+          a.alpha, a.y, (const int*)t.chunk_row, t.carry, t.arrive, vec_ok, a.err); \
     break;
+  cudaError_t e = cudaSuccess;
   note_launch();
   switch (t.vt) {
     SPMX_HOLA_CASE(4)
@@ -274,6 +275,7 @@ int launch_spmv_hola(const SpmvArgs& a, const HolaTables& t, cudaStream_t st) {
     SPMX_HOLA_CASE(16)
     default: return -1;
   }
+  (void)e;
 #undef SPMX_HOLA_CASE
   return 0;
 }

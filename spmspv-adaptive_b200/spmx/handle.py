@@ -322,6 +322,11 @@ class SpmspvHandle:
         check(lib.spmx_features(self._h, out), "features")
         return dict(zip(_lib.FEATURE_NAMES, list(out)))
 
+    def selector_inputs(self):
+        out = (c_double * _lib.NUM_FEATURES)()
+        check(lib.spmx_selector_inputs(self._h, out), "selector_inputs")
+        return list(out)
+
     def select(self):
         k = c_int()
         check(lib.spmx_select(self._h, ctypes.byref(k)), "select")
@@ -331,6 +336,14 @@ class SpmspvHandle:
         k = c_int()
         check(lib.spmx_run_adaptive(self._h, float(alpha), _f32(y), ctypes.byref(k)), "run_adaptive")
         return k.value
+
+    def autotune(self, cache_path=None):
+        """Time the tunable choices on this matrix and keep the fastest;
+        returns the chosen SpMV back-end (0 Hola, 1 CSR5, 2 tiled)."""
+        t = c_int()
+        check(lib.spmx_autotune(self._h, cache_path.encode() if cache_path else None,
+                                ctypes.byref(t)), "autotune")
+        return t.value
 
     def run_kernel(self, kid, alpha, y):
         check(lib.spmx_run_kernel(self._h, int(kid), float(alpha), _f32(y)), "run_kernel")
@@ -346,19 +359,22 @@ class SpmspvHandle:
               "spmv_backward_sparse")
 
     # -- BFS ---------------------------------------------------------------------------
-    def bfs(self, source, levels):
+    def bfs(self, source, levels, sync=True):
+        """Levels of a BFS from `source` into `levels` (int32 [n]); returns the
+        number of levels (reads it back) unless sync=False."""
         d = c_int()
-        check(lib.spmx_bfs(self._h, int(source), _i32(levels), ctypes.byref(d)), "bfs")
-        return d.value
+        check(lib.spmx_bfs(self._h, int(source), _i32(levels), ctypes.byref(d) if sync else None),
+              "bfs")
+        return d.value if sync else None
 
     def set_bfs_mode(self, mode):
         check(lib.spmx_set_bfs_mode(self._h, int(mode)), "set_bfs_mode")
 
-    def bfs_batched(self, sources, levels, layout=1):
+    def bfs_batched(self, sources, levels, layout=1, sync=True):
         """Up to 64 sources in one launch; levels is [n*len(sources)] int32
         (layout 1: source-major [s][v]; layout 0: vertex-major [v][s])."""
         src = (c_int * len(sources))(*[int(s) for s in sources])
         d = c_int()
         check(lib.spmx_bfs_batched(self._h, src, len(sources), _i32(levels), int(layout),
-                                   ctypes.byref(d)), "bfs_batched")
-        return d.value
+                                   ctypes.byref(d) if sync else None), "bfs_batched")
+        return d.value if sync else None

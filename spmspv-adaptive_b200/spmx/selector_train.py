@@ -1,0 +1,180 @@
+"""Train the kernel selector on this hardware and export it as C++.
+
+Follows the reference's offline pipeline (model/1-generate_matrix_class.py:
+label = the fastest kernel; model/1-test_dtree.py: a DecisionTreeClassifier
+chosen by GridSearchCV over criterion and depth on a 70/30 split with
+random_state=4; get_code, :93-112, prints the tree as if/else), with three
+differences:
+  - one tree over the eight kernels instead of three chained trees;
+  - the inputs are exactly what spmx_select sees at run time without a device
+    round trip (spmx_selector_inputs: matrix features, x_nnz, bin_len
+    estimated as x_nnz*nnz/n, the matrix's longest column);
+  - the labels come from timing all eight kernels on the GPU here
+    (`collect`), the split and the fit run on the host (`fit`).
+
+usage:
+  python -m spmx.selector_train collect OUT.jsonl      (GPU)
+  python -m spmx.selector_train fit DATA.jsonl OUT.inc  (host, scikit-learn)
+"""
+import json
+import math
+import statistics
+import sys
+
+import numpy as np
+
+from ._lib import FEATURE_NAMES, KERNEL_NAMES, NUM_KERNELS
+
+DENSITIES = [1e-6, 3e-6, 1e-5, 3e-5, 1e-4, 3e-4, 1e-3, 3e-3, 1e-2, 2e-2, 5e-2, 0.1, 0.2, 0.35,
+             0.5, 0.75, 1.0]
+
+
+def matrices():
+    """(name, Csr) pairs: the benchmark's shapes and a spread around them."""
+    from . import gen
+    yield "zipf-1M", gen.zipf_rows(1 << 20, 1.5, 16, 10000, seed=2)
+    yield "zipf-256K", gen.zipf_rows(1 << 18, 1.5, 16, 10000, seed=12)
+    yield "zipf-1M-mean4", gen.zipf_rows(1 << 20, 1.5, 4, 10000, seed=13)
+    yield "zipf-512K-mean64", gen.zipf_rows(1 << 19, 1.5, 64, 10000, seed=14)
+    for sc in (16, 20):
+        g = gen.rmat(sc, 16, seed=sc)
+        g.val = np.random.default_rng(sc).uniform(-1, 1, g.nnz).astype(np.float32)
+        yield f"rmat-{sc}", g
+    yield "chunglu-1M", gen.chung_lu(1 << 20, 2.1, 32.0, seed=5)
+    yield "laplacian-1024", gen.laplacian(1024, 0.01, seed=4)
+    yield "laplacian-2048", gen.laplacian(2048, 0.01, seed=4)
+
+
+def collect(out_path, reps=7):
+    import torch
+    from .handle import SpmspvHandle
+    from . import gen
+    dev = torch.device("cuda", 0)
+    stream = torch.cuda.current_stream(dev)
+    flush = torch.empty(64 << 20, device=dev)
+    s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with open(out_path, "w") as out:
+        for name, A in matrices():
+            t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)  # noqa: E731
+            rp, cl, vl = t(A.rowptr), t(A.col), t(A.val)
+            h = SpmspvHandle(A.m, A.n, A.nnz, stream=stream)
+            h.InputCSR(A.nnz, rp, cl, vl)
+            h.ToCSC()
+            h.allocPreBuffer()
+            backend = h.autotune()
+            y = torch.empty(A.m, device=dev)
+            for d in DENSITIES:
+                k = gen.density_nnz(A.n, d)
+                if k == 0:
+                    continue
+                key, val = gen.sparse_vector(A.n, k, seed=77 + k)
+                kd, vd = t(key), t(val)
+                h.set_sparse_x(kd, vd, k)
+                inputs = h.selector_inputs()
+                exact = h.features()
+                times = []
+                for kid in range(NUM_KERNELS):
+                    ts = []
+                    for it in range(reps + 2):
+                        flush.fill_(float(it))
+                        s.record(stream)
+                        h.run_kernel(kid, 1.0, y)
+                        e.record(stream)
+                        stream.synchronize()
+                        if it >= 2:
+                            ts.append(s.elapsed_time(e) * 1e3)
+                    times.append(statistics.median(ts))
+                h.check_device_error()
+                rec = {"matrix": name, "density": d, "x_nnz": k, "spmv_backend": backend,
+                       "inputs": inputs,
+                       "features": [exact[n_] for n_ in FEATURE_NAMES], "us": times,
+                       "best": int(np.argmin(times))}
+                out.write(json.dumps(rec) + "\n")
+                out.flush()
+                print(name, d, KERNEL_NAMES[rec["best"]], [round(x, 1) for x in times], flush=True)
+            h.Destroy()
+
+
+# host-known inputs the tree may split on (indices into the 23-entry schema);
+# "min" (13) is not known without a device pass and is left out
+TREE_FEATURES = [0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 11, 12, 14, 15, 16, 17, 18, 19, 20, 21, 22]
+
+
+def _load(path):
+    recs = [json.loads(ln) for ln in open(path) if ln.strip()]
+    X = np.array([[r["inputs"][i] for i in TREE_FEATURES] for r in recs], np.float64)
+    T = np.array([r["us"] for r in recs], np.float64)
+    return recs, X, T
+
+
+def fit(data_path, out_inc, report=True):
+    from sklearn.model_selection import GridSearchCV, train_test_split
+    from sklearn.tree import DecisionTreeClassifier
+    recs, X, T = _load(data_path)
+    y = T.argmin(axis=1)
+    idx = np.arange(len(y))
+    tr, te = train_test_split(idx, test_size=0.3, random_state=4)
+    grid = GridSearchCV(DecisionTreeClassifier(random_state=4),
+                        {"criterion": ["gini", "entropy"], "max_depth": list(range(1, 11))},
+                        cv=min(5, max(2, len(tr) // 8)))
+    # sample weight: how much picking wrong costs, relative to the best time
+    w = (T[tr].max(axis=1) / T[tr].min(axis=1))
+    grid.fit(X[tr], y[tr], sample_weight=w)
+    tree = grid.best_estimator_
+    def regret(ix):
+        p = tree.predict(X[ix])
+        return float(np.mean(T[ix, p] / T[ix].min(axis=1)))
+    stats = {"train_regret": regret(tr), "test_regret": regret(te),
+             "test_accuracy": float(np.mean(tree.predict(X[te]) == y[te])),
+             "params": grid.best_params_, "n": int(len(y))}
+    with open(out_inc, "w") as f:
+        f.write(export_cpp(tree, stats))
+    if report:
+        print(json.dumps(stats))
+    return tree, stats
+
+
+def export_cpp(tree, stats):
+    """The fitted tree as nested if/else over the feature vector."""
+    t = tree.tree_
+    lines = [
+        "// Generated by spmx/selector_train.py (fit) from kernel timings measured on",
+        "// B200; do not edit by hand.  Regret (time of the pick / time of the best",
+        f"// kernel): train {stats['train_regret']:.3f}, held-out {stats['test_regret']:.3f};",
+        f"// held-out accuracy {stats['test_accuracy']:.3f}; {stats['n']} (matrix, density) cases;",
+        f"// {json.dumps(stats['params'])}.",
+        "#pragma once",
+        "namespace spmx {",
+        "SPMX_HD inline int select_by_tree(const double* f) {",
+    ]
+
+    def rec(node, depth):
+        pad = "  " * depth
+        if t.children_left[node] == -1:
+            lines.append(f"{pad}return {int(np.argmax(t.value[node][0]))};")
+            return
+        fi = TREE_FEATURES[t.feature[node]]
+        lines.append(f"{pad}if (f[{fi}] <= {repr(float(t.threshold[node]))}) {{  // {FEATURE_NAMES[fi]}")
+        rec(t.children_left[node], depth + 1)
+        lines.append(f"{pad}}} else {{")
+        rec(t.children_right[node], depth + 1)
+        lines.append(f"{pad}}}")
+
+    rec(0, 1)
+    lines += ["}", "}  // namespace spmx", ""]
+    return "\n".join(lines)
+
+
+def main(argv):
+    if len(argv) >= 2 and argv[0] == "collect":
+        collect(argv[1])
+    elif len(argv) >= 3 and argv[0] == "fit":
+        fit(argv[1], argv[2])
+    else:
+        print(__doc__)
+        return 2
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main(sys.argv[1:]))
