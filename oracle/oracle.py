@@ -36,6 +36,7 @@ _sigs = {
     "oracle_mat_features": (None, [_i, _i, _i, _P, _P]),
     "oracle_mat_features_faithful": (None, [_i, _i, _i, _P, _P]),
     "oracle_std_row_intmean": (_d, [_i, _i, _P]),
+    "oracle_std_row_intmean_faithful": (_f, [_i, _i, _P]),
     "oracle_vec_features": (None, [_P, _i, _P, _P]),
     "oracle_gm": (None, [_i, _i, _i, ctypes.c_longlong, _P]),
     "oracle_csr5_sigma": (_i, [_i, _i]),
@@ -139,6 +140,11 @@ def mat_features_faithful(n, rowptr):
 def std_row_intmean(rowptr):
     rowptr = _a(rowptr, np.int32)
     return _lib.oracle_std_row_intmean(len(rowptr) - 1, int(rowptr[-1]), _p(rowptr))
+
+
+def std_row_intmean_faithful(rowptr):
+    rowptr = _a(rowptr, np.int32)
+    return _lib.oracle_std_row_intmean_faithful(len(rowptr) - 1, int(rowptr[-1]), _p(rowptr))
 
 
 def vec_features(colptr, x_key):

@@ -242,6 +242,18 @@ EXPORT double oracle_std_row_intmean(int m, int nnz, const int* rowptr) {
   return sqrt(s / m);
 }
 
+/* extractMatFeature, faithful: int-truncated mean, int differences squared
+ * and added into a float, float square root (spmspv.h:423-447). */
+EXPORT float oracle_std_row_intmean_faithful(int m, int nnz, const int* rowptr) {
+  const int avg_nnz = (int)(nnz / (float)m);
+  float sum = 0.0f;
+  for (int i = 0; i < m; i++) {
+    const int num = rowptr[i + 1] - rowptr[i];
+    sum += (num - avg_nnz) * (num - avg_nnz);
+  }
+  return sqrtf(sum / m);
+}
+
 /* computeVecFeture_serial (spmspv.h:2338-2361): out = {bin_len, max, min} */
 EXPORT void oracle_vec_features(const int* colptr, int x_nnz, const int* x_key,
                                 long long* out) {
