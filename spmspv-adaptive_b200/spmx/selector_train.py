@@ -151,7 +151,8 @@ def export_cpp(tree, stats):
     def rec(node, depth):
         pad = "  " * depth
         if t.children_left[node] == -1:
-            lines.append(f"{pad}return {int(np.argmax(t.value[node][0]))};")
+            # leaf values are indexed like tree.classes_ (the labels seen in training)
+            lines.append(f"{pad}return {int(tree.classes_[int(np.argmax(t.value[node][0]))])};")
             return
         fi = TREE_FEATURES[t.feature[node]]
         lines.append(f"{pad}if (f[{fi}] <= {repr(float(t.threshold[node]))}) {{  // {FEATURE_NAMES[fi]}")
