@@ -529,8 +529,10 @@ def run_only(args):
         if it >= args.warmup:
             ts.append(s.elapsed_time(e))
     h.check_device_error()
-    print(json.dumps({"only": args.only, "density": dens, "ms": statistics.mean(ts),
-                      "min_ms": min(ts)}))
+    out = {"only": args.only, "density": dens, "ms": statistics.mean(ts), "min_ms": min(ts)}
+    if args.only.startswith("tiled"):
+        out["tiled"] = h.tiled_info()
+    print(json.dumps(out))
     return 0
 
 

@@ -177,12 +177,19 @@ int spmx_csr5_postprocess(spmx_handle_t h);
 /* the sigma in use (after CSR5Preprocess) or that the auto rule would pick */
 int spmx_csr5_sigma(spmx_handle_t h, int* sigma);
 /* Tiled SpMV format (no reference counterpart; a third back-end for
- * spmv / spmspv): nonzeros grouped into tiles of rb_rows rows x win columns
- * (powers of two, rb_rows <= 32768, win <= 65536) so that each CTA's x
- * accesses stay inside one window cached in L1 while y accumulates in shared
- * memory; chunk = nonzeros per work unit.  0 selects the defaults. */
-int spmx_tiled_preprocess(spmx_handle_t h, int rb_rows, int win, int chunk);
+ * spmv / spmspv): rows cut into blocks whose y fits in shared memory (at
+ * most rb_rows rows; 0 = as many as fit), columns into windows of win
+ * entries of x (a multiple of 128, <= 65536; 0 = 4096), tiles cut into
+ * stages of at most chunk nonzeros (0 = 2048); warps = row-owning warps per
+ * CTA (8 or 16; 0 = 16).  Each stage's x window and
+ * nonzeros are streamed into shared memory with bulk copies; a row block is
+ * shared by a cluster of CTAs whose partial y vectors are combined through
+ * distributed shared memory.  The result is deterministic. */
+int spmx_tiled_preprocess(spmx_handle_t h, int rb_rows, int win, int chunk, int warps);
 int spmx_tiled_postprocess(spmx_handle_t h);
+/* geometry chosen by spmx_tiled_preprocess: info[0..7] = row blocks, CTAs
+ * per cluster, stages, win, chunk, shared y rows, shared bytes, row warps */
+int spmx_tiled_info(spmx_handle_t h, int* info);
 int spmx_tiledspmv(spmx_handle_t h, float alpha, float* d_y);
 int spmx_tiledspmspv(spmx_handle_t h, float alpha, float* d_y);
 /* set_spmv_type — H:1767 (0 Hola, 1 CSR5, 2 tiled) */

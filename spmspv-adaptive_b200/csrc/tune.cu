@@ -4,7 +4,7 @@
 // of every tunable choice on the handle's matrix with CUDA events and keeps
 // the fastest:
 //   - the load-balanced SpMV back-end: Hola (4, 8 or 16 nonzeros per thread),
-//     CSR5 (sigma by the reference's rule) or tiled (row block x window);
+//     CSR5 (sigma by the reference's rule) or tiled (x window width);
 //   - the lanes per row of the naive CSR kernel and per column of the naive
 //     CSC kernel;
 //   - merge-path vs fixed-nonzero blocks for the load-balanced CSC kernel;
@@ -39,7 +39,7 @@ __global__ void stride_keys_kernel(int* key, float* val, int k, int n) {
 }
 
 struct Params {
-  int spmv_type = SPMX_SPMV_HOLA, hola_vt = 8, tiled_rb = 16384, tiled_win = 16384;
+  int spmv_type = SPMX_SPMV_HOLA, hola_vt = 8, tiled_rb = 0, tiled_win = 4096;
   int row_group = 0, col_group = 0, lb_variant = SPMX_CSC_LB_MERGE, buckets = 256;
 };
 
@@ -110,7 +110,7 @@ static int apply_params(spmx_handle_t h, const Params& p) {
   } else if (p.spmv_type == SPMX_SPMV_CSR5) {
     if (!h->csr5) rc = spmx_csr5_preprocess(h);
   } else if (p.spmv_type == SPMX_SPMV_TILED) {
-    rc = spmx_tiled_preprocess(h, p.tiled_rb, p.tiled_win, 0);
+    rc = spmx_tiled_preprocess(h, p.tiled_rb, p.tiled_win, 0, 0);
   }
   return rc;
 }
@@ -179,10 +179,9 @@ extern "C" int spmx_autotune(spmx_handle_t h, const char* cache_path, int* spmv_
       if (t < best_t) { best_t = t; best.spmv_type = SPMX_SPMV_CSR5; }
       spmx_csr5_postprocess(h);
     }
-    for (int rbw : {0, 1, 2, 3}) {
-      const int rb = rbw < 2 ? 16384 : 32768;
-      const int win = (rbw & 1) ? 8192 : 16384;
-      if (spmx_tiled_preprocess(h, rb, win, 0) != SPMX_SUCCESS) continue;
+    for (int win : {2048, 4096, 8192}) {
+      const int rb = 0;  // rows per block: as many as shared memory holds
+      if (spmx_tiled_preprocess(h, rb, win, 0, 0) != SPMX_SUCCESS) continue;
       const float t = time_us([&] { return spmx_tiledspmv(h, 1.0f, y); });
       if (t < best_t) {
         best_t = t;

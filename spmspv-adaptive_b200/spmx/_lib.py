@@ -86,8 +86,9 @@ _SIGS = {
     "spmx_csr5_postprocess": (c_int, [P]),
     "spmx_csr5_sigma": (c_int, [P, PI]),
     "spmx_set_spmv_type": (c_int, [P, c_int]),
-    "spmx_tiled_preprocess": (c_int, [P, c_int, c_int, c_int]),
+    "spmx_tiled_preprocess": (c_int, [P, c_int, c_int, c_int, c_int]),
     "spmx_tiled_postprocess": (c_int, [P]),
+    "spmx_tiled_info": (c_int, [P, P]),
     "spmx_tiledspmv": (c_int, [P, c_float, P]),
     "spmx_tiledspmspv": (c_int, [P, c_float, P]),
     "spmx_naivespmv": (c_int, [P, c_float, P]),

@@ -182,11 +182,20 @@ class SpmspvHandle:
     def CSR5Postprocess(self):
         check(lib.spmx_csr5_postprocess(self._h), "CSR5Postprocess")
 
-    def tiledPreprocess(self, rb_rows=0, win=0, chunk=0):
-        check(lib.spmx_tiled_preprocess(self._h, int(rb_rows), int(win), int(chunk)), "tiledPreprocess")
+    def tiledPreprocess(self, rb_rows=0, win=0, chunk=0, warps=0):
+        check(lib.spmx_tiled_preprocess(self._h, int(rb_rows), int(win), int(chunk), int(warps)),
+              "tiledPreprocess")
 
     def tiledPostprocess(self):
         check(lib.spmx_tiled_postprocess(self._h), "tiledPostprocess")
+
+    def tiled_info(self):
+        """Geometry of the tiled format: row blocks, CTAs per cluster, stages,
+        window, chunk, shared y rows, shared bytes, row warps."""
+        info = (ctypes.c_int * 8)()
+        check(lib.spmx_tiled_info(self._h, info), "tiled_info")
+        names = ("row_blocks", "cluster", "stages", "win", "chunk", "rmax", "smem", "warps")
+        return dict(zip(names, list(info)))
 
     def tiledspmv(self, alpha, y):
         check(lib.spmx_tiledspmv(self._h, float(alpha), _f32(y)), "tiledspmv")

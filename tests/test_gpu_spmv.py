@@ -162,11 +162,12 @@ def test_csr5_zipf_full_size(torch_cuda):
 
 
 @pytest.mark.parametrize("name,A", CASES, ids=[c[0] for c in CASES])
-@pytest.mark.parametrize("rb,win", [(256, 512), (1024, 256), (16384, 16384)])
-def test_tiled_spmv(torch_cuda, name, A, rb, win):
+@pytest.mark.parametrize("rb,win,chunk,warps", [(256, 512, 300, 8), (1024, 256, 64, 16), (0, 0, 0, 0),
+                                               (0, 8192, 4096, 8)])
+def test_tiled_spmv(torch_cuda, name, A, rb, win, chunk, warps):
     torch = torch_cuda
     h = make_handle(A, torch, csc=False, hola=False)
-    h.tiledPreprocess(rb, win, 300 if rb < 16384 else 0)
+    h.tiledPreprocess(rb, win, chunk, warps)
     x = np.random.default_rng(17).uniform(-1, 1, A.n).astype(np.float32)
     h.set_x(dev(x, torch))
     y64, mag = orc.spmv_f64(A.rowptr, A.col, A.val, x, alpha=-1.5)
