@@ -179,9 +179,9 @@ int spmx_csr5_sigma(spmx_handle_t h, int* sigma);
 /* Tiled SpMV format (no reference counterpart; a third back-end for
  * spmv / spmspv): rows cut into blocks whose y fits in shared memory (at
  * most rb_rows rows; 0 = as many as fit), columns into windows of win
- * entries of x (a multiple of 128, <= 65536; 0 = 4096), tiles cut into
+ * entries of x (a multiple of 128, <= 65536; 0 = 8192), tiles cut into
  * stages of at most chunk nonzeros (0 = 2048); warps = row-owning warps per
- * CTA (8 or 16; 0 = 16).  Each stage's x window and
+ * CTA (4, 8 or 16; 0 = 8).  Each stage's x window and
  * nonzeros are streamed into shared memory with bulk copies; a row block is
  * shared by a cluster of CTAs whose partial y vectors are combined through
  * distributed shared memory.  The result is deterministic. */

@@ -8,8 +8,9 @@
 // third of HBM bandwidth.  Reading x from shared memory instead costs a few
 // bank wavefronts per warp, so this back-end stages x in shared memory:
 //
-//   - rows are cut into row blocks whose y fits in shared memory (about 33K
-//     rows), columns into windows of `win` entries of x (4096 by default);
+//   - rows are cut into row blocks whose y fits in shared memory (up to about
+//     20K rows with the default window), columns into windows of `win`
+//     entries of x (8192 by default);
 //     a tile is the set of nonzeros of one row block inside one window, in
 //     CSR order (sorted by row), cut into stages of at most `chunk` entries;
 //   - a row block is processed by a cluster of `cs` CTAs (cs chosen so that
@@ -135,12 +136,12 @@ struct TileSmem {
 // ranges of equal length (the first len % 32 lanes get one more).  The
 // preprocessing stores the slice lane-interleaved: entry j of lane l's range
 // sits at lo + 32 * j + l, so every load below is one conflict-free
-// wavefront.  A lane walks its range in groups of 8 entries (all loads
+// wavefront.  A lane walks its range in groups of G entries (all loads
 // first), keeps the running sum of the current row in a register and adds
 // every run that starts and ends inside its range to ys with a plain
 // read-modify-write.  Only a run that continues into a neighbouring lane is
 // added with shared atomics, piece by piece.  No other warp owns these rows.
-template <bool GATED>
+template <int G, bool GATED>
 __device__ __forceinline__ void tile_warp_slice(int lo, int hi, const unsigned* __restrict__ P,
                                                 const float* __restrict__ V, const float* __restrict__ X,
                                                 const unsigned* __restrict__ B, float* __restrict__ ys) {
@@ -154,14 +155,14 @@ __device__ __forceinline__ void tile_warp_slice(int lo, int hi, const unsigned* 
   int hk = -1, cur = -1;  // head run row, current run row
   float hs = 0.f, acc = 0.f;
   bool head_open = true;  // still inside the first run of the range
-  for (int j0 = 0; j0 < cnt; j0 += 8) {
-    const int ng = min(8, cnt - j0);
-    unsigned w[8];
-    float pr[8];
+  for (int j0 = 0; j0 < cnt; j0 += G) {
+    const int ng = min(G, cnt - j0);
+    unsigned w[G];
+    float pr[G];
 #pragma unroll
-    for (int j = 0; j < 8; ++j) w[j] = j < ng ? Pl[32 * (j0 + j)] : 0u;
+    for (int j = 0; j < G; ++j) w[j] = j < ng ? Pl[32 * (j0 + j)] : 0u;
 #pragma unroll
-    for (int j = 0; j < 8; ++j) {
+    for (int j = 0; j < G; ++j) {
       const int c = (int)(w[j] & 0xffffu);
       float v = 0.f;
       if (j < ng) {
@@ -170,10 +171,10 @@ __device__ __forceinline__ void tile_warp_slice(int lo, int hi, const unsigned* 
       }
       pr[j] = v;
     }
-    int fr[8];
-    float fs[8];
+    int fr[G];
+    float fs[G];
 #pragma unroll
-    for (int j = 0; j < 8; ++j) {
+    for (int j = 0; j < G; ++j) {
       fr[j] = -1;
       fs[j] = 0.f;
       if (j < ng) {
@@ -197,11 +198,11 @@ __device__ __forceinline__ void tile_warp_slice(int lo, int hi, const unsigned* 
         }
       }
     }
-    float old[8];
+    float old[G];
 #pragma unroll
-    for (int j = 0; j < 8; ++j) old[j] = fr[j] >= 0 ? ys[fr[j]] : 0.f;
+    for (int j = 0; j < G; ++j) old[j] = fr[j] >= 0 ? ys[fr[j]] : 0.f;
 #pragma unroll
-    for (int j = 0; j < 8; ++j)
+    for (int j = 0; j < G; ++j)
       if (fr[j] >= 0) ys[fr[j]] = old[j] + fs[j];
   }
   // lane summary: head run (hk, hs) and tail run (cur, acc); one run if the
@@ -375,7 +376,7 @@ tiled_spmv_kernel(int n, TileGeom g, int cs, const int* __restrict__ rb_row,
         break;
       }
       const int lo = offs[b * (NW + 1) + warp], hi = offs[b * (NW + 1) + warp + 1];
-      tile_warp_slice<GATED>(lo, hi, pk_of(b), vv_of(b), xs_of(b), bits_of(b), ys);
+      tile_warp_slice<(NW <= 4 ? 16 : 8), GATED>(lo, hi, pk_of(b), vv_of(b), xs_of(b), bits_of(b), ys);
       if (lane == 0) bar_arrive(empty + b);
     }
   }
@@ -515,7 +516,7 @@ __global__ void tile_interleave_kernel(int nw, const TileStage* __restrict__ sta
 using namespace spmx;
 
 struct TiledTables {
-  TileGeom g{4096, 2048, 4};
+  TileGeom g{8192, 2048, 4};
   int nw = 8, cs = 1, nrb = 0, grid = 0, nstages = 0;
   size_t smem = 0;
   unsigned* packed = nullptr;
@@ -579,35 +580,55 @@ static int tiled_max_clusters(int cs, size_t smem) {
   return nc;
 }
 
+// static shared memory of the kernel (barriers' abort flag and friends)
+static long long tiled_static_smem(int nw) {
+  cudaFuncAttributes a = {};
+  cudaError_t e;
+  if (nw == 16) e = cudaFuncGetAttributes(&a, tiled_spmv_kernel<16, true>);
+  else if (nw == 4) e = cudaFuncGetAttributes(&a, tiled_spmv_kernel<4, true>);
+  else e = cudaFuncGetAttributes(&a, tiled_spmv_kernel<8, true>);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return 1024;
+  }
+  return (long long)a.sharedSizeBytes + 16;
+}
+
 static size_t tiled_smem_total(int nw, const TileGeom& g) {
-  return nw == 16 ? (size_t)TileSmem<16>::total(g) : (size_t)TileSmem<8>::total(g);
+  if (nw == 16) return (size_t)TileSmem<16>::total(g);
+  if (nw == 4) return (size_t)TileSmem<4>::total(g);
+  return (size_t)TileSmem<8>::total(g);
 }
 
 static void tiled_set_smem_nw(int nw, size_t smem) {
   if (nw == 16) tiled_set_smem<16>(smem);
+  else if (nw == 4) tiled_set_smem<4>(smem);
   else tiled_set_smem<8>(smem);
 }
 
 static int tiled_max_clusters_nw(int nw, int cs, size_t smem) {
-  return nw == 16 ? tiled_max_clusters<16>(cs, smem) : tiled_max_clusters<8>(cs, smem);
+  if (nw == 16) return tiled_max_clusters<16>(cs, smem);
+  if (nw == 4) return tiled_max_clusters<4>(cs, smem);
+  return tiled_max_clusters<8>(cs, smem);
 }
 
 extern "C" int spmx_tiled_preprocess(spmx_handle_t h, int rb_rows, int win, int chunk, int warps) {
   if (!h) return set_error(SPMX_ERR_INVALID_VALUE, "NULL handle");
   if (!h->has_csr || (!h->val && h->nnz > 0))
     return set_error(SPMX_ERR_NOT_READY, "tiled SpMV needs the CSR input with values");
-  if (win <= 0) win = 4096;
+  if (win <= 0) win = 8192;
   if (chunk <= 0) chunk = 2048;
   chunk = (chunk + 3) & ~3;
-  if (warps <= 0) warps = 16;
-  if (rb_rows < 0 || win % 128 || win > 65536 || chunk < 4 || chunk > (1 << 16) || (warps != 8 && warps != 16))
+  if (warps <= 0) warps = 8;
+  if (rb_rows < 0 || win % 128 || win > 65536 || chunk < 4 || chunk > (1 << 16) ||
+      (warps != 4 && warps != 8 && warps != 16))
     return set_error(SPMX_ERR_INVALID_VALUE,
-                     "tiled SpMV: win must be a multiple of 128 (<= 65536), chunk in [4, 65536], warps 8 or 16");
+                     "tiled SpMV: win must be a multiple of 128 (<= 65536), chunk in [4, 65536], warps 4, 8 or 16");
   const int NW = warps;
   int optin = 0;
   cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, h->device);
   TileGeom g{win, chunk, 4};
-  const long long fixed = (long long)tiled_smem_total(NW, g) - 4 * g.rmax + 16;  // + static shared memory
+  const long long fixed = (long long)tiled_smem_total(NW, g) - 4 * g.rmax + tiled_static_smem(NW);
   long long rcap = ((long long)optin - fixed) / 4;
   rcap = std::min<long long>(rcap & ~3LL, 65532);
   if (rb_rows > 0) rcap = std::min<long long>(rcap, std::max(4, (rb_rows + 3) & ~3));
@@ -626,25 +647,25 @@ extern "C" int spmx_tiled_preprocess(spmx_handle_t h, int rb_rows, int win, int 
     return set_error(SPMX_ERR_CUDA, "tiled SpMV: row pointer copy");
   }
   cudaStreamSynchronize(st);
-  // cluster size and row block count: the largest cluster (<= 8) whose grid of
-  // one CTA per SM still covers the rows and fits in one wave; fewer row
-  // blocks mean fewer passes over x
+  // cluster size and row block count: the largest cluster (4, 3 or 2 CTAs)
+  // whose grid of one CTA per SM covers the rows in one wave (every cluster
+  // resident at once); fewer row blocks mean fewer passes over x.  Otherwise
+  // single CTAs over as many row blocks as needed.
   const int sms = h->num_sms;
   const long long need = std::max<long long>(1, (m + rcap - 1) / rcap);
-  int cs = 1, nrb = (int)need;
-  g.rmax = (int)rcap;
-  t->smem = tiled_smem_total(NW, g);
-  tiled_set_smem_nw(NW, t->smem);
-  for (int c = 8; c >= 2; --c) {
-    // one wave: no more row blocks than clusters that fit at once
-    const int nb = std::min(sms / c, tiled_max_clusters_nw(NW, c, t->smem));
-    if (nb < need) continue;
+  int cs = 1, nrb = (int)std::max<long long>(need, std::min(sms, std::max(1, m / 4)));
+  for (int c = 4; c >= 2; --c) {
+    const int nb = sms / c;
+    if (nb < need || nb > std::max(1, m / 4)) continue;
+    TileGeom gc = g;
+    gc.rmax = (int)std::min<long long>(rcap, ((((long long)m + nb - 1) / nb) + 64 + 3) & ~3LL);
+    const size_t sm_c = tiled_smem_total(NW, gc);
+    tiled_set_smem_nw(NW, sm_c);
+    if (tiled_max_clusters_nw(NW, c, sm_c) < nb) continue;
     cs = c;
     nrb = nb;
     break;
   }
-  if (cs == 1) nrb = (int)std::max<long long>(need, std::min(sms, std::max(1, m / 4)));
-  nrb = (int)std::max<long long>(nrb, need);
   nrb = std::max(1, std::min(nrb, (m + 3) / 4));
   // row blocks: about equal nonzero counts, boundaries on multiples of 4, at
   // most rcap rows each
@@ -870,6 +891,9 @@ int tiled_spmv_impl(spmx_handle_t h, float alpha, float* y, bool gated) {
   if (t->nw == 16)
     e = gated ? tiled_launch<16, true>(h, t, alpha, y, bits, aligned)
               : tiled_launch<16, false>(h, t, alpha, y, bits, aligned);
+  else if (t->nw == 4)
+    e = gated ? tiled_launch<4, true>(h, t, alpha, y, bits, aligned)
+              : tiled_launch<4, false>(h, t, alpha, y, bits, aligned);
   else
     e = gated ? tiled_launch<8, true>(h, t, alpha, y, bits, aligned)
               : tiled_launch<8, false>(h, t, alpha, y, bits, aligned);

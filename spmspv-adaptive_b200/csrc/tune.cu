@@ -39,7 +39,7 @@ __global__ void stride_keys_kernel(int* key, float* val, int k, int n) {
 }
 
 struct Params {
-  int spmv_type = SPMX_SPMV_HOLA, hola_vt = 8, tiled_rb = 0, tiled_win = 4096;
+  int spmv_type = SPMX_SPMV_HOLA, hola_vt = 8, tiled_rb = 0, tiled_win = 8192;
   int row_group = 0, col_group = 0, lb_variant = SPMX_CSC_LB_MERGE, buckets = 256;
 };
 
@@ -179,7 +179,7 @@ extern "C" int spmx_autotune(spmx_handle_t h, const char* cache_path, int* spmv_
       if (t < best_t) { best_t = t; best.spmv_type = SPMX_SPMV_CSR5; }
       spmx_csr5_postprocess(h);
     }
-    for (int win : {2048, 4096, 8192}) {
+    for (int win : {4096, 8192}) {
       const int rb = 0;  // rows per block: as many as shared memory holds
       if (spmx_tiled_preprocess(h, rb, win, 0, 0) != SPMX_SUCCESS) continue;
       const float t = time_us([&] { return spmx_tiledspmv(h, 1.0f, y); });

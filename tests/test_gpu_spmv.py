@@ -163,7 +163,7 @@ def test_csr5_zipf_full_size(torch_cuda):
 
 @pytest.mark.parametrize("name,A", CASES, ids=[c[0] for c in CASES])
 @pytest.mark.parametrize("rb,win,chunk,warps", [(256, 512, 300, 8), (1024, 256, 64, 16), (0, 0, 0, 0),
-                                               (0, 8192, 4096, 8)])
+                                               (0, 8192, 4096, 4)])
 def test_tiled_spmv(torch_cuda, name, A, rb, win, chunk, warps):
     torch = torch_cuda
     h = make_handle(A, torch, csc=False, hola=False)
