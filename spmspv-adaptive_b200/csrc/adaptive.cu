@@ -391,6 +391,39 @@ static int ensure_msbfs(spmx_handle_t h) {
   return SPMX_SUCCESS;
 }
 
+// vertices of degree above this are pulled in chunks of this many edges
+constexpr int kHubDegree = 1024;
+
+// hub chunk list of the multi-source pull, built once per matrix
+static int ensure_hubs(spmx_handle_t h) {
+  if (h->ms_hub_rowptr == h->rowptr && h->ms_hub_nnz == h->nnz && h->ms_hcounters) return SPMX_SUCCESS;
+  cudaStream_t st = h->stream;
+  SPMX_CUDA(cudaStreamSynchronize(st));
+  dfree(h->ms_hchunk); dfree(h->ms_hcnt); dfree(h->ms_hacc); dfree(h->ms_hleft); dfree(h->ms_hcounters);
+  h->ms_hchunk = nullptr; h->ms_hcnt = nullptr; h->ms_hacc = nullptr; h->ms_hleft = nullptr;
+  h->ms_hcounters = nullptr;
+  const long long nnz = std::max(h->nnz, 0);
+  const int max_hubs = (int)(nnz / (kHubDegree + 1) + 1);
+  const long long max_chunks = nnz / kHubDegree + max_hubs + 1;
+  SPMX_TRY(dalloc((void**)&h->ms_hchunk, sizeof(int4) * (size_t)max_chunks, "msbfs hub chunks"));
+  SPMX_TRY(dalloc((void**)&h->ms_hcnt, 4 * (size_t)max_hubs, "msbfs hub chunk counts"));
+  SPMX_TRY(dalloc((void**)&h->ms_hacc, 8 * (size_t)max_hubs, "msbfs hub accumulators"));
+  SPMX_TRY(dalloc((void**)&h->ms_hleft, 4 * (size_t)max_hubs, "msbfs hub counters"));
+  SPMX_TRY(dalloc((void**)&h->ms_hcounters, 8, "msbfs hub totals"));
+  SPMX_CUDA(cudaMemsetAsync(h->ms_hcounters, 0, 8, st));
+  launch_hub_chunks(h->n, h->rowptr, kHubDegree, h->ms_hchunk, h->ms_hcnt, h->ms_hcounters, max_hubs,
+                    (int)max_chunks, st);
+  int cnt[2] = {0, 0};
+  SPMX_CUDA(cudaMemcpyAsync(cnt, h->ms_hcounters, 8, cudaMemcpyDeviceToHost, st));
+  SPMX_CUDA(cudaStreamSynchronize(st));
+  if (cnt[0] > max_hubs || cnt[1] > max_chunks) return set_error(SPMX_ERR_OOB, "hub chunk capacity");
+  h->ms_nhubs = cnt[0];
+  h->ms_nhchunks = cnt[1];
+  h->ms_hub_rowptr = h->rowptr;
+  h->ms_hub_nnz = h->nnz;
+  return SPMX_SUCCESS;
+}
+
 extern "C" int spmx_bfs_batched(spmx_handle_t h, const int* srcs, int nsrc, int* levels,
                                 int layout, int* depth) {
   SPMX_CHECK_HANDLE(h);
@@ -401,6 +434,7 @@ extern "C" int spmx_bfs_batched(spmx_handle_t h, const int* srcs, int nsrc, int*
   for (int s = 0; s < nsrc; ++s)
     if (srcs[s] < 0 || srcs[s] >= h->n) return set_error(SPMX_ERR_INVALID_VALUE, "source out of range");
   SPMX_TRY(ensure_msbfs(h));
+  SPMX_TRY(ensure_hubs(h));
   cudaStream_t st = h->stream;
   const size_t n = (size_t)h->n;
   const size_t total = n * (size_t)nsrc;
@@ -422,9 +456,14 @@ extern "C" int spmx_bfs_batched(spmx_handle_t h, const int* srcs, int nsrc, int*
   SPMX_CUDA(cudaMemsetAsync(h->ms_front0, 0, 8 * n, st));
   SPMX_CUDA(cudaMemsetAsync(h->ms_front1, 0, 8 * n, st));
   SPMX_CUDA(cudaMemsetAsync(h->ms_next, 0, 8 * n, st));
+  if (h->ms_nhubs > 0) {
+    SPMX_CUDA(cudaMemsetAsync(h->ms_hacc, 0, 8 * (size_t)h->ms_nhubs, st));
+    SPMX_CUDA(cudaMemcpyAsync(h->ms_hleft, h->ms_hcnt, 4 * (size_t)h->ms_nhubs, cudaMemcpyDeviceToDevice, st));
+  }
+  HubChunks hub{h->ms_hchunk, h->ms_nhchunks, h->ms_hcnt, h->ms_hacc, h->ms_hleft, h->ms_nhubs, kHubDegree};
   MsBfsArgs a{h->n, nsrc, h->num_sms, (long long)h->nnz, h->msbfs_alpha, h->ms_srcs, h->rowptr,
               h->col, vmajor, h->ms_visit, h->ms_front0, h->ms_front1, h->ms_next, h->ms_q0,
-              h->ms_q1, (BfsCtrl*)h->ms_ctrl, h->d_err};
+              h->ms_q1, (BfsCtrl*)h->ms_ctrl, hub, h->d_err};
   if (launch_msbfs_persistent(a, st))
     return set_error(SPMX_ERR_CUDA, std::string("cooperative multi-source BFS launch: ") +
                                         cudaGetErrorString(cudaGetLastError()));

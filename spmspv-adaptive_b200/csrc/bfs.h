@@ -31,6 +31,20 @@ struct BfsPersistentArgs {
   int* err;
 };
 
+// Hubs for the multi-source pull: every vertex of degree > deg is cut into
+// chunks of deg edges that all warps share; acc / left are per-hub OR
+// accumulators and outstanding-chunk counters, reset to 0 / nchunk_of each
+// level.
+struct HubChunks {
+  const int4* chunk;     // {vertex, first edge, end edge, hub index}
+  long long nchunks;
+  const int* nchunk_of;  // chunks per hub
+  unsigned long long* acc;
+  int* left;
+  int nhubs;
+  int deg;
+};
+
 struct MsBfsArgs {
   int n, ns, num_sms;
   long long total_edges;
@@ -46,9 +60,12 @@ struct MsBfsArgs {
   int* q0;
   int* q1;
   BfsCtrl* ctrl;
+  HubChunks hub;
   int* err;
 };
 
+int launch_hub_chunks(int n, const int* rowptr, int deg_cut, int4* chunk, int* nchunk_of,
+                      int* counters, int max_hubs, int max_chunks, cudaStream_t st);
 int launch_bfs_persistent(const BfsPersistentArgs& a, cudaStream_t st);
 int launch_msbfs_persistent(const MsBfsArgs& a, cudaStream_t st);
 int launch_levels_transpose(int n, int ns, const int* vmajor, int* smajor, cudaStream_t st);

@@ -12,6 +12,8 @@
 //   unvisited vertex pulls the OR of its neighbours' frontier words and stops
 //   once every source has reached it.  Levels are written vertex-major,
 //   levels[v * ns + s], so each finished vertex is one contiguous store.
+#include <algorithm>
+
 #include "bfs.h"
 #include "common.cuh"
 #include "kernels.h"
@@ -20,6 +22,12 @@ namespace spmx {
 
 __device__ __forceinline__ bool tbit(const unsigned* bits, int v) {
   return (bits[v >> 5] >> (v & 31)) & 1u;
+}
+
+__device__ __forceinline__ unsigned long long warp_or64(unsigned long long v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v |= __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
 }
 
 __device__ __forceinline__ void warp_append2(bool want, int v, int deg, int* q, int* q_count,
@@ -64,27 +72,58 @@ bfs_persistent_kernel(int n, long long total_edges, const int* __restrict__ rowp
       for (long long vb = gwarp * 32; vb < n; vb += nwarps * 32) {
         const int v = (int)(vb + lane);
         bool found = false;
-        int deg = 0;
-        if (v < n && !tbit(visited, v)) {
-          const int a = __ldg(rowptr + v), b = __ldg(rowptr + v + 1);
+        int deg = 0, a = 0, b = 0;
+        const bool open = v < n && !tbit(visited, v);
+        if (open) {
+          a = __ldg(rowptr + v);
+          b = __ldg(rowptr + v + 1);
           deg = b - a;
+        }
+        const bool heavy = open && deg > 32;
+        if (open && !heavy) {
           for (int k = a; k < b; ++k) {
             const int u = __ldg(col + k);
             if ((unsigned)u >= (unsigned)n) { flag_error(err, kDevErrOob); continue; }
             if (tbit(fbc, u)) { found = true; break; }
           }
-          if (found) {
-            levels[v] = L + 1;
-            atomicOr(visited + (v >> 5), 1u << (v & 31));
-            atomicOr(fbn + (v >> 5), 1u << (v & 31));
+        }
+        // vertices of degree > 32: the whole warp looks for a frontier neighbour
+        unsigned hm = __ballot_sync(0xffffffffu, heavy);
+        while (hm) {
+          const int sl = __ffs(hm) - 1;
+          hm &= hm - 1;
+          const int ha = __shfl_sync(0xffffffffu, a, sl), hb = __shfl_sync(0xffffffffu, b, sl);
+          bool any = false;
+          for (int kb = ha; kb < hb && !any; kb += 32) {
+            const int k = kb + lane;
+            bool hit = false;
+            if (k < hb) {
+              const int u = __ldg(col + k);
+              if ((unsigned)u >= (unsigned)n) flag_error(err, kDevErrOob);
+              else hit = tbit(fbc, u);
+            }
+            any = __any_sync(0xffffffffu, hit);
           }
+          if (lane == sl) found = any;
+        }
+        if (found) {
+          levels[v] = L + 1;
+          atomicOr(visited + (v >> 5), 1u << (v & 31));
+          atomicOr(fbn + (v >> 5), 1u << (v & 31));
         }
         warp_append2(found, v, deg, qn, &ctrl->cnt[slot], &ctrl->edges[slot]);
       }
     } else {
-      for (long long f = gwarp; f < nf; f += nwarps) {
+      // a small frontier gets several warps per vertex (equal slices of its
+      // adjacency), so a hub vertex does not serialise on one warp
+      const long long g = nf < nwarps ? nwarps / nf : 1;
+      for (long long wi = gwarp; wi < nf * g; wi += nwarps) {
+        const long long f = wi / g;
+        const long long part = wi - f * g;
         const int u = qc[f];
-        const int a = __ldg(rowptr + u), b = __ldg(rowptr + u + 1);
+        const int a0 = __ldg(rowptr + u), b0 = __ldg(rowptr + u + 1);
+        const int a = a0 + (int)(((long long)(b0 - a0) * part) / g);
+        const int b = a0 + (int)(((long long)(b0 - a0) * (part + 1)) / g);
         for (int kb = a; kb < b; kb += 32) {
           const int k = kb + lane;
           bool win = false;
@@ -145,7 +184,7 @@ msbfs_persistent_kernel(int n, int ns, long long total_edges, double alpha_ms,
                         int* __restrict__ levels, unsigned long long* visit,
                         unsigned long long* front0, unsigned long long* front1,
                         unsigned long long* next, int* q0, int* q1, BfsCtrl* ctrl,
-                        int* err) {
+                        HubChunks hub, int* err) {
   const GridBarrier bar{&ctrl->bar_count, &ctrl->bar_gen, &ctrl->abort_flag};
   const unsigned long long FULL = ns >= 64 ? ~0ull : ((1ull << ns) - 1ull);
   const int lane = threadIdx.x & 31;
@@ -168,30 +207,100 @@ msbfs_persistent_kernel(int n, int ns, long long total_edges, double alpha_ms,
       for (long long vb = gwarp * 32; vb < n; vb += nwarps * 32) {
         const int v = (int)(vb + lane);
         bool add = false;
-        int deg = 0;
+        int deg = 0, a = 0, b = 0;
+        unsigned long long vis = FULL;
         if (v < n) {
-          const unsigned long long vis = visit[v];
-          if (vis != FULL) {
-            const int a = __ldg(rowptr + v), b = __ldg(rowptr + v + 1);
-            deg = b - a;
-            unsigned long long acc = 0ull;
-            for (int k = a; k < b; ++k) {
-              const int u = __ldg(col + k);
-              if ((unsigned)u >= (unsigned)n) { flag_error(err, kDevErrOob); continue; }
-              acc |= fc[u];
-              if ((acc | vis) == FULL) break;
-            }
-            const unsigned long long nv = acc & ~vis;
-            if (nv) { next[v] = nv; add = true; }
+          vis = visit[v];
+          a = __ldg(rowptr + v);
+          b = __ldg(rowptr + v + 1);
+          deg = b - a;
+        }
+        // hubs (degree > hub.deg) are pulled chunk by chunk below
+        const bool open = v < n && vis != FULL && deg <= hub.deg;
+        const bool heavy = open && deg > 32;
+        unsigned long long nv = 0ull;
+        if (open && !heavy) {
+          unsigned long long acc = 0ull;
+          for (int k = a; k < b; ++k) {
+            const int u = __ldg(col + k);
+            if ((unsigned)u >= (unsigned)n) { flag_error(err, kDevErrOob); continue; }
+            acc |= fc[u];
+            if ((acc | vis) == FULL) break;
           }
+          nv = acc & ~vis;
+        }
+        // vertices of degree > 32: the whole warp pulls, one vertex at a time,
+        // and stops once every source has reached the vertex
+        unsigned hm = __ballot_sync(0xffffffffu, heavy);
+        while (hm) {
+          const int sl = __ffs(hm) - 1;
+          hm &= hm - 1;
+          const int ha = __shfl_sync(0xffffffffu, a, sl), hb = __shfl_sync(0xffffffffu, b, sl);
+          const unsigned long long hvis = __shfl_sync(0xffffffffu, vis, sl);
+          unsigned long long acc = 0ull;
+          for (int kb = ha; kb < hb; kb += 32) {
+            const int k = kb + lane;
+            if (k < hb) {
+              const int u = __ldg(col + k);
+              if ((unsigned)u >= (unsigned)n) flag_error(err, kDevErrOob);
+              else acc |= fc[u];
+            }
+            acc = warp_or64(acc);
+            if ((acc | hvis) == FULL) break;
+          }
+          if (lane == sl) nv = acc & ~vis;
+        }
+        if (nv) {
+          next[v] = nv;
+          add = true;
         }
         warp_append2(add, v, deg, qn, &ctrl->cnt[slot], &ctrl->edges[slot]);
       }
+      // hub chunks, spread over all warps: each ORs its slice of a hub's
+      // neighbours into the hub's accumulator; the warp that retires the
+      // hub's last chunk (a counter, no waiting) finishes the hub
+      for (long long c = gwarp; c < hub.nchunks; c += nwarps) {
+        const int4 ch = hub.chunk[c];  // {vertex, first edge, end edge, hub index}
+        const unsigned long long hvis = visit[ch.x];
+        unsigned long long acc = 0ull;
+        if (hvis != FULL) {
+          for (int kb = ch.y; kb < ch.z; kb += 32) {
+            const int k = kb + lane;
+            if (k < ch.z) {
+              const int u = __ldg(col + k);
+              if ((unsigned)u >= (unsigned)n) flag_error(err, kDevErrOob);
+              else acc |= fc[u];
+            }
+          }
+          acc = warp_or64(acc);
+        }
+        bool add = false;
+        int deg = 0;
+        if (lane == 0) {
+          if (acc) atomicOr(hub.acc + ch.w, acc);
+          __threadfence();
+          if (atomicSub(hub.left + ch.w, 1) == 1) {
+            __threadfence();
+            const unsigned long long nv = atomicOr(hub.acc + ch.w, 0ull) & ~hvis;
+            if (nv) {
+              next[ch.x] = nv;
+              add = true;
+              deg = __ldg(rowptr + ch.x + 1) - __ldg(rowptr + ch.x);
+            }
+          }
+        }
+        warp_append2(add, ch.x, deg, qn, &ctrl->cnt[slot], &ctrl->edges[slot]);
+      }
     } else {
-      for (long long f = gwarp; f < nq; f += nwarps) {
+      const long long g = nq < nwarps ? nwarps / nq : 1;  // warps per frontier vertex
+      for (long long wi = gwarp; wi < nq * g; wi += nwarps) {
+        const long long f = wi / g;
+        const long long part = wi - f * g;
         const int u = qc[f];
         const unsigned long long fu = fc[u];
-        const int a = __ldg(rowptr + u), b = __ldg(rowptr + u + 1);
+        const int a0 = __ldg(rowptr + u), b0 = __ldg(rowptr + u + 1);
+        const int a = a0 + (int)(((long long)(b0 - a0) * part) / g);
+        const int b = a0 + (int)(((long long)(b0 - a0) * (part + 1)) / g);
         for (int kb = a; kb < b; kb += 32) {
           const int k = kb + lane;
           bool add = false;
@@ -233,6 +342,11 @@ msbfs_persistent_kernel(int n, int ns, long long total_edges, double alpha_ms,
       nv = __shfl_sync(0xffffffffu, nv, 0);
       for (int s = lane; s < ns; s += 32)
         if ((nv >> s) & 1ull) levels[(long long)v * ns + s] = L + 1;
+    }
+    // hub accumulators for the next level
+    for (long long i = gtid; i < hub.nhubs; i += nthreads) {
+      hub.acc[i] = 0ull;
+      hub.left[i] = hub.nchunk_of[i];
     }
     if (gtid == 0) {
       ctrl->cnt[(L + 2) % 3] = 0;
@@ -322,6 +436,31 @@ int launch_bfs_persistent(const BfsPersistentArgs& a, cudaStream_t st) {
   return e == cudaSuccess ? 0 : -2;
 }
 
+// chunks of hub.deg edges of every vertex of degree > hub.deg
+__global__ void hub_chunks_kernel(int n, const int* __restrict__ rowptr, int deg_cut, int4* chunk,
+                                  int* nchunk_of, int* counters, int max_hubs, int max_chunks) {
+  for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
+    const int a = __ldg(rowptr + v), b = __ldg(rowptr + v + 1);
+    if (b - a <= deg_cut) continue;
+    const int nch = (b - a + deg_cut - 1) / deg_cut;
+    const int hi = atomicAdd(counters, 1);
+    const int base = atomicAdd(counters + 1, nch);
+    if (hi >= max_hubs || base + nch > max_chunks) continue;  // cannot happen by the bounds
+    nchunk_of[hi] = nch;
+    for (int j = 0; j < nch; ++j)
+      chunk[base + j] = make_int4(v, a + j * deg_cut, min(b, a + (j + 1) * deg_cut), hi);
+  }
+}
+
+int launch_hub_chunks(int n, const int* rowptr, int deg_cut, int4* chunk, int* nchunk_of,
+                      int* counters, int max_hubs, int max_chunks, cudaStream_t st) {
+  if (n <= 0) return 0;
+  note_launch();
+  hub_chunks_kernel<<<std::min((n + 255) / 256, 148 * 8), 256, 0, st>>>(n, rowptr, deg_cut, chunk, nchunk_of,
+                                                                       counters, max_hubs, max_chunks);
+  return 0;
+}
+
 int launch_msbfs_persistent(const MsBfsArgs& a, cudaStream_t st) {
   const int grid = coop_grid(msbfs_persistent_kernel, a.num_sms, a.n);
   if (grid <= 0) return -1;
@@ -342,8 +481,9 @@ int launch_msbfs_persistent(const MsBfsArgs& a, cudaStream_t st) {
   int* q0 = a.q0;
   int* q1 = a.q1;
   BfsCtrl* ctrl = a.ctrl;
+  HubChunks hub = a.hub;
   int* err = a.err;
-  void* args[] = {&n, &ns, &te, &al, &rp, &cl, &lv, &vis, &f0, &f1, &nx, &q0, &q1, &ctrl, &err};
+  void* args[] = {&n, &ns, &te, &al, &rp, &cl, &lv, &vis, &f0, &f1, &nx, &q0, &q1, &ctrl, &hub, &err};
   cudaError_t e = cudaLaunchCooperativeKernel((void*)msbfs_persistent_kernel, grid, 256, args, 0, st);
   return e == cudaSuccess ? 0 : -2;
 }

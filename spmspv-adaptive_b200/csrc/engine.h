@@ -114,6 +114,16 @@ struct spmx_handle_s {
   size_t ms_tmp_len = 0;
   void* ms_ctrl = nullptr;
   int ms_n = 0;
+  // hub chunks of the multi-source pull (built once per matrix)
+  int4* ms_hchunk = nullptr;
+  int* ms_hcnt = nullptr;
+  unsigned long long* ms_hacc = nullptr;
+  int* ms_hleft = nullptr;
+  int* ms_hcounters = nullptr;
+  long long ms_nhchunks = 0;
+  int ms_nhubs = 0;
+  const int* ms_hub_rowptr = nullptr;
+  int ms_hub_nnz = -1;
   double bfs_alpha = 14.0, bfs_beta = 24.0, msbfs_alpha = 12.0;
   unsigned* bfs_visited = nullptr;
   unsigned* bfs_front = nullptr;
