@@ -348,6 +348,28 @@ int spmx_spmv_backward_sparse(spmx_handle_t h, const float* d_x,
                               const int* d_dy_key, const float* d_dy_val,
                               int dy_nnz, float* d_dx, float* d_dvals);
 
+/* ======================= batched SpMSpV (FP32) ============================= */
+/* No reference counterpart (the reference runs one vector per call).  nvec
+ * sparse vectors in one concatenated list: vector v owns entries
+ * [xptr[v], xptr[v+1]) of (xkey, xval); xptr has nvec + 1 entries, all
+ * pointers are device pointers (xkey and xval may be NULL when the batch has
+ * no entries; with entries the device error word records SPMX_ERR_OOB).  Forward: Y[v * m + i] = alpha * (A x_v)[i]
+ * (Y dense, nvec x m, zero-filled by the call).  One persistent kernel with a
+ * device work queue of 256-entry chunks; needs the CSC with values.  No host
+ * synchronisation: after one call outside stream capture (which allocates the
+ * handle's 4-byte work counter) both entry points can be captured in a CUDA
+ * graph.  Concurrent batched calls on one handle race on the counter. */
+int spmx_spmspv_batched(spmx_handle_t h, int nvec, const int* d_xptr, const int* d_xkey,
+                        const float* d_xval, float alpha, float* d_Y);
+/* Adjoint of the batch for an upstream gradient dY (nvec x m):
+ *   dxval[e] = alpha * sum over column xkey[e] of A[k] * dY[v * m + row_k]
+ *   dvals[k] = alpha * sum over the batch of xval[e] * dY[v * m + row_k]
+ * (dvals in CSR order, overwritten; the first call with dvals builds a
+ * CSC-to-CSR permutation and synchronises).  Either output may be NULL. */
+int spmx_spmspv_batched_backward(spmx_handle_t h, int nvec, const int* d_xptr, const int* d_xkey,
+                                 const float* d_xval, float alpha, const float* d_dY,
+                                 float* d_dxval, float* d_dvals);
+
 /* ======================= device counters ================================== */
 /* device pointers to the handle's counters: [0] y_nnz of the last SpMSpV,
  * [1] bin_len of the last scan, [2] x_nnz after dense2sparse */

@@ -23,30 +23,6 @@
 
 using namespace spmx;
 
-#define SPMX_CUDA(call)                                                        \
-  do {                                                                         \
-    cudaError_t e_ = (call);                                                   \
-    if (e_ != cudaSuccess) {                                                   \
-      return set_error(SPMX_ERR_CUDA,                                          \
-                       std::string(#call) + ": " + cudaGetErrorString(e_));    \
-    }                                                                          \
-  } while (0)
-#define SPMX_TRY(expr)                                                         \
-  do {                                                                         \
-    int r_ = (expr);                                                           \
-    if (r_ != SPMX_SUCCESS) return r_;                                         \
-  } while (0)
-#define SPMX_CHECK_HANDLE(h)                                                   \
-  do {                                                                         \
-    if (!(h)) return set_error(SPMX_ERR_INVALID_VALUE, "NULL handle");         \
-  } while (0)
-
-static int launch_ok(const char* what) {
-  cudaError_t e = cudaGetLastError();
-  if (e != cudaSuccess)
-    return set_error(SPMX_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
-  return SPMX_SUCCESS;
-}
 
 // ---------------------------------------------------------------------------
 // matrix features

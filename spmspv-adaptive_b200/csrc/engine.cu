@@ -86,32 +86,6 @@ int csc_lb_blocks_per_sm();
 
 using namespace spmx;
 
-#define SPMX_CUDA(call)                                                        \
-  do {                                                                         \
-    cudaError_t e_ = (call);                                                   \
-    if (e_ != cudaSuccess) {                                                   \
-      return set_error(SPMX_ERR_CUDA,                                          \
-                       std::string(#call) + ": " + cudaGetErrorString(e_));    \
-    }                                                                          \
-  } while (0)
-
-#define SPMX_TRY(expr)                                                         \
-  do {                                                                         \
-    int r_ = (expr);                                                           \
-    if (r_ != SPMX_SUCCESS) return r_;                                         \
-  } while (0)
-
-#define SPMX_CHECK_HANDLE(h)                                                   \
-  do {                                                                         \
-    if (!(h)) return set_error(SPMX_ERR_INVALID_VALUE, "NULL handle");         \
-  } while (0)
-
-static int launch_ok(const char* what) {
-  cudaError_t e = cudaGetLastError();
-  if (e != cudaSuccess)
-    return set_error(SPMX_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
-  return SPMX_SUCCESS;
-}
 
 static int pow2_group(double mean) {
   int g = 1;
@@ -224,6 +198,7 @@ extern "C" int spmx_destroy(spmx_handle_t h) {
   dfree(h->ms_visit); dfree(h->ms_front0); dfree(h->ms_front1); dfree(h->ms_next);
   dfree(h->ms_q0); dfree(h->ms_q1); dfree(h->ms_srcs); dfree(h->ms_tmp); dfree(h->ms_ctrl);
   dfree(h->ms_hchunk); dfree(h->ms_hcnt); dfree(h->ms_hacc); dfree(h->ms_hleft); dfree(h->ms_hcounters);
+  dfree(h->batch_work); dfree(h->csc_perm);
   delete h;
   return SPMX_SUCCESS;
 }

@@ -114,6 +114,11 @@ struct spmx_handle_s {
   size_t ms_tmp_len = 0;
   void* ms_ctrl = nullptr;
   int ms_n = 0;
+  // batched SpMSpV: work-queue counter; CSC position -> CSR index (dvals)
+  unsigned* batch_work = nullptr;
+  int* csc_perm = nullptr;
+  int csc_perm_nnz = -1;
+  const int* csc_perm_col = nullptr;
   // hub chunks of the multi-source pull (built once per matrix)
   int4* ms_hchunk = nullptr;
   int* ms_hcnt = nullptr;
@@ -138,3 +143,32 @@ int set_error(int code, const std::string& msg);
 int dalloc(void** p, size_t bytes, const char* what);
 void dfree(void* p);
 }  // namespace spmx
+
+// Status plumbing shared by the entry points: return the first failure.
+#define SPMX_CUDA(call)                                                        \
+  do {                                                                         \
+    cudaError_t e_ = (call);                                                   \
+    if (e_ != cudaSuccess) {                                                   \
+      return set_error(SPMX_ERR_CUDA,                                          \
+                       std::string(#call) + ": " + cudaGetErrorString(e_));    \
+    }                                                                          \
+  } while (0)
+
+#define SPMX_TRY(expr)                                                         \
+  do {                                                                         \
+    int r_ = (expr);                                                           \
+    if (r_ != SPMX_SUCCESS) return r_;                                         \
+  } while (0)
+
+#define SPMX_CHECK_HANDLE(h)                                                   \
+  do {                                                                         \
+    if (!(h)) return set_error(SPMX_ERR_INVALID_VALUE, "NULL handle");         \
+  } while (0)
+
+// status of the last kernel launch on this thread
+inline int launch_ok(const char* what) {
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess)
+    return spmx::set_error(SPMX_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+  return SPMX_SUCCESS;
+}

@@ -368,6 +368,21 @@ class SpmspvHandle:
               "spmv_backward_sparse")
 
     # -- BFS ---------------------------------------------------------------------------
+    # -- batched SpMSpV (no reference counterpart) ------------------------------
+    def spmspv_batched(self, xptr, xkey, xval, alpha, Y):
+        """Y[v, :] = alpha * A @ x_v for the nvec = len(xptr) - 1 sparse vectors
+        of the concatenated (xkey, xval); Y is (nvec, m) float32 on the device."""
+        nvec = int(xptr.numel()) - 1
+        check(lib.spmx_spmspv_batched(self._h, nvec, _i32(xptr), _i32(xkey), _f32(xval), float(alpha),
+                                      _f32(Y)), "spmspv_batched")
+
+    def spmspv_batched_backward(self, xptr, xkey, xval, alpha, dY, dxval=None, dvals=None):
+        """dxval (layout of xval) and dvals (CSR order) for an upstream dY."""
+        nvec = int(xptr.numel()) - 1
+        check(lib.spmx_spmspv_batched_backward(self._h, nvec, _i32(xptr), _i32(xkey), _f32(xval),
+                                               float(alpha), _f32(dY), _f32(dxval), _f32(dvals)),
+              "spmspv_batched_backward")
+
     def bfs(self, source, levels, sync=True):
         """Levels of a BFS from `source` into `levels` (int32 [n]); returns the
         number of levels (reads it back) unless sync=False."""
