@@ -338,6 +338,7 @@ def run_ours(args, world, rank, local):
     bfs = run_bfs_plain(torch, dev, stream, args) if rank == 0 and not args.no_bfs else None
     bfs64 = run_bfs_batched(torch, dev, stream, args) if rank == 0 and not args.no_bfs else None
     batched = run_batched_spmspv(torch, dev, stream, args) if rank == 0 and not args.no_batched else None
+    adjoint = run_adjoint(torch, dev, stream, args) if rank == 0 and not args.no_batched else None
 
     line = None
     if rank == 0:
@@ -366,6 +367,7 @@ def run_ours(args, world, rank, local):
             "bfs": bfs,
             "batched_bfs": bfs64,
             "batched_spmspv": batched,
+            "adjoint": adjoint,
         }
         print(json.dumps(line), flush=True)
     h.Destroy()
@@ -555,6 +557,59 @@ def run_batched_spmspv(torch, dev, stream, args):
                     "gradient from single calls needs extra sums); the graph computes dvals too"}
 
 
+def run_adjoint(torch, dev, stream, args):
+    """Differentiable SpMV: the 5-point Laplacian on a 2048 x 2048 grid
+    (4,194,304 rows, off-diagonals -1 + N(0, 0.01^2), seed 4), x and dy
+    N(0,1).  Forward = the autotuned load-balanced SpMV; backward = dx = A^T dy
+    and dvals on the pattern in one pass (dense dy), and the same for dy masked
+    to 1 % of the rows (sparse dy).  L2 flushed before every timed call."""
+    import spmx
+    from spmx import gen
+    A = gen.laplacian(2048, 0.01, seed=4)
+    m, n = A.m, A.n
+    t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)  # noqa: E731
+    h = spmx.SpmspvHandle(m, n, A.nnz, stream=stream)
+    h.InputCSR(A.nnz, t(A.rowptr), t(A.col), t(A.val))
+    h.holaPreprocess()
+    backend = SPMV_BACKENDS.get(h.autotune(), "?")
+    rng = np.random.default_rng(4)
+    x = t(rng.standard_normal(n).astype(np.float32))
+    dy = t(rng.standard_normal(m).astype(np.float32))
+    k = m // 100
+    key = np.sort(rng.choice(m, k, replace=False)).astype(np.int32)
+    dk, dv = t(key), t(rng.standard_normal(k).astype(np.float32))
+    h.set_x(x)
+    y = torch.empty(m, device=dev)
+    dx = torch.empty(n, device=dev)
+    dvals = torch.empty(A.nnz, device=dev)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+    def timed(fn):
+        ts = []
+        for it in range(3 + max(args.steps, 5)):
+            flush.fill_(float(it))
+            e0.record(stream)
+            fn()
+            e1.record(stream)
+            stream.synchronize()
+            if it >= 3:
+                ts.append(e0.elapsed_time(e1))
+        return statistics.median(ts)
+
+    f_ms = timed(lambda: h.spmv(1.0, y))
+    b_ms = timed(lambda: h.spmv_backward(x, dy, dx, dvals))
+    s_ms = timed(lambda: h.spmv_backward_sparse(x, dk, dv, k, dx, dvals))
+    h.check_device_error()
+    h.Destroy()
+    fb = spmv_bytes(m, n, A.nnz)
+    bb = 4 * (m + 1) + 8 * A.nnz + 4 * m + 4 * n + 4 * A.nnz + 4 * n  # CSR, dy, x, dvals, dx
+    return {"matrix": "5-point Laplacian 2048^2, nnz %d, off-diagonals -1 + N(0, 0.01^2)" % A.nnz,
+            "forward_backend": backend, "forward_ms": f_ms, "backward_dense_dy_ms": b_ms,
+            "backward_sparse_dy_1pct_ms": s_ms, "backward_over_forward": b_ms / f_ms,
+            "forward_gbs": fb / (f_ms * 1e-3) / 1e9, "backward_gbs": bb / (b_ms * 1e-3) / 1e9}
+
+
 def cpu_baseline(A, xs, binl):
     """The reference's serial CPU routines (restated), one core, one sweep."""
     import oracle.oracle as orc
@@ -582,7 +637,7 @@ def cpu_baseline(A, xs, binl):
             "ms": best * 1e3}
 
 
-ONLY = ("batched-spmspv", "hola-spmv", "csr5-spmv", "naive-spmv", "tiled-spmv", "hola-spmspv", "csc-lb-atomic",
+ONLY = ("batched-spmspv", "adjoint", "hola-spmv", "csr5-spmv", "naive-spmv", "tiled-spmv", "hola-spmspv", "csc-lb-atomic",
         "csc-naive-atomic", "csc-bucket", "csc-lb-sort", "bfs-rmat14", "bfs-batched")
 
 
@@ -601,6 +656,9 @@ def run_only(args):
         return 0
     if args.only == "batched-spmspv":
         print(json.dumps(run_batched_spmspv(torch, dev, stream, args)))
+        return 0
+    if args.only == "adjoint":
+        print(json.dumps(run_adjoint(torch, dev, stream, args)))
         return 0
     A, xs = make_inputs()
     d = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)  # noqa: E731

@@ -367,7 +367,6 @@ class SpmspvHandle:
                                             int(dy_nnz), _f32(dx), _f32(dvals)),
               "spmv_backward_sparse")
 
-    # -- BFS ---------------------------------------------------------------------------
     # -- batched SpMSpV (no reference counterpart) ------------------------------
     def spmspv_batched(self, xptr, xkey, xval, alpha, Y):
         """Y[v, :] = alpha * A @ x_v for the nvec = len(xptr) - 1 sparse vectors
@@ -383,6 +382,7 @@ class SpmspvHandle:
                                                float(alpha), _f32(dY), _f32(dxval), _f32(dvals)),
               "spmspv_batched_backward")
 
+    # -- BFS ---------------------------------------------------------------------------
     def bfs(self, source, levels, sync=True):
         """Levels of a BFS from `source` into `levels` (int32 [n]); returns the
         number of levels (reads it back) unless sync=False."""
