@@ -206,21 +206,36 @@ __device__ __forceinline__ void tile_warp_slice(int lo, int hi, const unsigned* 
       if (fr[j] >= 0) ys[fr[j]] = old[j] + fs[j];
   }
   // lane summary: head run (hk, hs) and tail run (cur, acc); one run if the
-  // head never closed.  A run that crosses a lane boundary is added with
-  // shared atomics by every lane holding a piece of it (tails first, then
-  // heads); all other runs were or are added with plain stores.
+  // head never closed.  Every run that crosses a lane boundary is added once,
+  // with a plain store, by the lane where it ends.
   const bool single = head_open;
   if (single) hs = acc;
   const int ptail = __shfl_up_sync(0xffffffffu, cur, 1);  // row ending the previous lane's range
   const bool cont = lane > 0 && cnt > 0 && ptail == hk;
   const bool ncont = __shfl_down_sync(0xffffffffu, cont, 1) && lane < 31;
-  if (cur >= 0 && !(single && cont)) {
-    if (ncont) atomicAdd(ys + cur, acc);
-    else ys[cur] += acc;
+  const float pacc = __shfl_up_sync(0xffffffffu, acc, 1);  // the previous lane's tail sum
+  if (!__any_sync(0xffffffffu, single && cont && ncont)) {
+    // common case: a crossing run spans two lanes; the second adds the first's part
+    if (cont) ys[single ? cur : hk] += (single ? acc : hs) + pacc;
+    else if (!single && hk >= 0) ys[hk] += hs;
+    if (cur >= 0 && !ncont && !(single && cont)) ys[cur] += acc;
+  } else {
+    // a lane inside a longer run: chain the tail sums with a segmented scan
+    float S = acc;
+    bool F = !(single && cont);
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+      const float oS = __shfl_up_sync(0xffffffffu, S, d);
+      const bool oF = __shfl_up_sync(0xffffffffu, F, d);
+      if (lane >= d && !F) {
+        S += oS;
+        F = oF;
+      }
+    }
+    const float PS = __shfl_up_sync(0xffffffffu, S, 1);  // chain sum ending at lane - 1
+    if (!single && hk >= 0) ys[hk] += hs + (cont ? PS : 0.f);
+    if ((lane == 31 || !ncont) && cur >= 0) ys[cur] += S;
   }
-  __syncwarp();
-  if (hk >= 0 && cont) atomicAdd(ys + hk, single ? acc : hs);
-  else if (hk >= 0 && !single) ys[hk] += hs;
   __syncwarp();
 }
 
