@@ -289,11 +289,12 @@ static int bfs_stepped(spmx_handle_t h, int source, int* levels, int* depth);
 static int ensure_bfs(spmx_handle_t h) {
   if (h->bfs_n == h->n && h->bfs_visited) return SPMX_SUCCESS;
   dfree(h->bfs_visited); dfree(h->bfs_front); dfree(h->bfs_q[0]); dfree(h->bfs_q[1]);
-  dfree(h->bfs_cnt); dfree(h->bfs_edges); dfree(h->bfs_fb1); dfree(h->bfs_ctrl);
+  dfree(h->bfs_cnt); dfree(h->bfs_edges); dfree(h->bfs_fb1); dfree(h->bfs_fb2); dfree(h->bfs_ctrl);
   const size_t words = (size_t)std::max((h->n + 31) / 32, 1);
   SPMX_TRY(dalloc((void**)&h->bfs_visited, 4 * words, "bfs visited"));
   SPMX_TRY(dalloc((void**)&h->bfs_front, 4 * words, "bfs front"));
   SPMX_TRY(dalloc((void**)&h->bfs_fb1, 4 * words, "bfs front 1"));
+  SPMX_TRY(dalloc((void**)&h->bfs_fb2, 4 * words, "bfs front 2"));
   SPMX_TRY(dalloc((void**)&h->bfs_q[0], 4 * (size_t)std::max(h->n, 1), "bfs queue 0"));
   SPMX_TRY(dalloc((void**)&h->bfs_q[1], 4 * (size_t)std::max(h->n, 1), "bfs queue 1"));
   SPMX_TRY(dalloc((void**)&h->bfs_cnt, 4 * 4, "bfs counts"));
@@ -319,23 +320,18 @@ extern "C" int spmx_set_bfs_mode(spmx_handle_t h, int mode) {
 static int bfs_persistent(spmx_handle_t h, int source, int* levels, int* depth) {
   cudaStream_t st = h->stream;
   const int n = h->n;
-  const size_t words = (size_t)((n + 31) / 32);
-  SPMX_CUDA(cudaMemsetAsync(levels, 0xff, 4 * (size_t)n, st));
-  SPMX_CUDA(cudaMemsetAsync(h->bfs_visited, 0, 4 * words, st));
-  SPMX_CUDA(cudaMemsetAsync(h->bfs_front, 0, 4 * words, st));
-  SPMX_CUDA(cudaMemsetAsync(h->bfs_fb1, 0, 4 * words, st));
+  // the kernel initialises levels, the visited set and the frontier bitmaps
   BfsPersistentArgs a{n, source, h->num_sms, (long long)h->nnz, h->rowptr, h->col, levels,
-                      h->bfs_visited, h->bfs_front, h->bfs_fb1, h->bfs_q[0], h->bfs_q[1],
+                      h->bfs_visited, h->bfs_front, h->bfs_fb1, h->bfs_fb2, h->bfs_q[0], h->bfs_q[1],
                       (BfsCtrl*)h->bfs_ctrl, h->bfs_alpha, h->bfs_beta, h->d_err};
   const int rc = launch_bfs_persistent(a, st);
   if (rc) return set_error(SPMX_ERR_CUDA, std::string("cooperative BFS launch: ") +
                                               cudaGetErrorString(cudaGetLastError()));
-  if (depth) {
-    int d = 0;
-    SPMX_CUDA(cudaMemcpyAsync(&d, &((BfsCtrl*)h->bfs_ctrl)->depth, sizeof(int),
+  if (depth) {  // through the handle's pinned word: a pageable copy costs ~15 us
+    SPMX_CUDA(cudaMemcpyAsync(h->h_pinned + 1, &((BfsCtrl*)h->bfs_ctrl)->depth, sizeof(int),
                               cudaMemcpyDeviceToHost, st));
     SPMX_CUDA(cudaStreamSynchronize(st));
-    *depth = d;
+    *depth = h->h_pinned[1];
   }
   return SPMX_SUCCESS;
 }
@@ -446,11 +442,10 @@ extern "C" int spmx_bfs_batched(spmx_handle_t h, const int* srcs, int nsrc, int*
   if (layout == 1) launch_levels_transpose(h->n, nsrc, vmajor, levels, st);
   SPMX_TRY(launch_ok("batched bfs"));
   if (depth) {
-    int d = 0;
-    SPMX_CUDA(cudaMemcpyAsync(&d, &((BfsCtrl*)h->ms_ctrl)->depth, sizeof(int),
+    SPMX_CUDA(cudaMemcpyAsync(h->h_pinned + 1, &((BfsCtrl*)h->ms_ctrl)->depth, sizeof(int),
                               cudaMemcpyDeviceToHost, st));
     SPMX_CUDA(cudaStreamSynchronize(st));
-    *depth = d;
+    *depth = h->h_pinned[1];
   }
   return SPMX_SUCCESS;
 }

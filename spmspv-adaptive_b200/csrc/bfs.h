@@ -23,6 +23,7 @@ struct BfsPersistentArgs {
   unsigned* visited;
   unsigned* fb0;
   unsigned* fb1;
+  unsigned* fb2;
   int* q0;
   int* q1;
   BfsCtrl* ctrl;

@@ -48,17 +48,36 @@ __device__ __forceinline__ void warp_append2(bool want, int v, int deg, int* q, 
 __global__ void __launch_bounds__(256)
 bfs_persistent_kernel(int n, long long total_edges, const int* __restrict__ rowptr,
                       const int* __restrict__ col, int* __restrict__ levels,
-                      unsigned* visited, unsigned* fb0, unsigned* fb1, int* q0, int* q1,
+                      unsigned* visited, unsigned* fb0, unsigned* fb1, unsigned* fb2, int* q0, int* q1,
                       BfsCtrl* ctrl, double alpha_b, double beta_b, int src, int* err) {
   const GridBarrier bar{&ctrl->bar_count, &ctrl->bar_gen, &ctrl->abort_flag};
   const int lane = threadIdx.x & 31;
   const long long gtid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   const long long nthreads = (long long)gridDim.x * blockDim.x;
   const long long gwarp = gtid >> 5, nwarps = nthreads >> 5;
+  const long long words = (n + 31) >> 5;
+  // initial state: every write goes to a distinct place, so one barrier suffices
+  for (long long i = gtid; i < n; i += nthreads) levels[i] = i == src ? 0 : -1;
+  for (long long w = gtid; w < words; w += nthreads) {
+    const unsigned sb = w == (src >> 5) ? 1u << (src & 31) : 0u;
+    visited[w] = sb;
+    fb0[w] = sb;
+    fb1[w] = 0u;
+    fb2[w] = 0u;
+  }
+  if (gtid == 0) {
+    q0[0] = src;
+    for (int k = 0; k < 3; ++k) {
+      ctrl->cnt[k] = 0;
+      ctrl->edges[k] = 0ull;
+    }
+  }
+  if (!grid_sync(bar, err)) return;
   const int src_deg = __ldg(rowptr + src + 1) - __ldg(rowptr + src);
   long long nf = 1, mf = src_deg, mu = total_edges - src_deg;
   bool pull = false;
   int L = 0, cur = 0;
+  unsigned* fbs[3] = {fb0, fb1, fb2};
   while (true) {
     if (!pull && (double)mf > (double)mu / alpha_b) pull = true;
     else if (pull && (double)nf < (double)n / beta_b) pull = false;
@@ -66,8 +85,19 @@ bfs_persistent_kernel(int n, long long total_edges, const int* __restrict__ rowp
     const int slot = (L + 1) % 3;
     int* qn = nxt ? q1 : q0;
     const int* qc = cur ? q1 : q0;
-    unsigned* fbn = nxt ? fb1 : fb0;
-    unsigned* fbc = cur ? fb1 : fb0;
+    // frontier bitmaps rotate over three buffers: this level reads fbs[L % 3],
+    // writes fbs[(L + 1) % 3], and clears fbs[(L + 2) % 3] (the frontier of
+    // the previous level, read by nobody now) for the next level; the counter
+    // slot of the next level is cleared the same way.  One barrier per level.
+    const unsigned* fbc = fbs[L % 3];
+    unsigned* fbn = fbs[(L + 1) % 3];
+    unsigned* fbr = fbs[(L + 2) % 3];
+    if (L > 0)
+      for (long long w = gtid; w < words; w += nthreads) fbr[w] = 0u;
+    if (gtid == 0) {
+      ctrl->cnt[(L + 2) % 3] = 0;
+      ctrl->edges[(L + 2) % 3] = 0ull;
+    }
     if (pull) {
       for (long long vb = gwarp * 32; vb < n; vb += nwarps * 32) {
         const int v = (int)(vb + lane);
@@ -148,16 +178,8 @@ bfs_persistent_kernel(int n, long long total_edges, const int* __restrict__ rowp
       }
     }
     if (!grid_sync(bar, err)) return;
-    const long long nn = *(volatile int*)&ctrl->cnt[slot];
+    nf = *(volatile int*)&ctrl->cnt[slot];
     const long long me = (long long)*(volatile unsigned long long*)&ctrl->edges[slot];
-    // clear the current frontier's bitmap for reuse two levels on
-    for (long long f = gtid; f < nf; f += nthreads) fbc[qc[f] >> 5] = 0u;
-    if (gtid == 0) {
-      ctrl->cnt[(L + 2) % 3] = 0;
-      ctrl->edges[(L + 2) % 3] = 0ull;
-    }
-    if (!grid_sync(bar, err)) return;
-    nf = nn;
     mf = me;
     mu -= me;
     if (nf == 0) break;
@@ -167,13 +189,6 @@ bfs_persistent_kernel(int n, long long total_edges, const int* __restrict__ rowp
   if (gtid == 0) ctrl->depth = L + 1;
 }
 
-__global__ void bfs_persistent_init_kernel(int src, int* levels, unsigned* visited,
-                                           unsigned* fb0, int* q0) {
-  levels[src] = 0;
-  visited[src >> 5] |= 1u << (src & 31);
-  fb0[src >> 5] |= 1u << (src & 31);
-  q0[0] = src;
-}
 
 // ---------------------------------------------------------------------------
 // multi-source BFS, up to 64 sources
@@ -398,25 +413,25 @@ __global__ void levels_transpose_kernel(int n, int ns, const int* __restrict__ v
 // joins every grid barrier, so a small graph gets few CTAs (one per SM down
 // to 1024 vertices per CTA) and a large one the whole resident capacity.
 template <class K>
-static int coop_grid(K kernel, int num_sms, long long work_items) {
+static int coop_grid(K kernel, int num_sms, int min_ctas, long long work_items) {
   int per = 0;
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, 256, 0) != cudaSuccess) {
     cudaGetLastError();
     return 0;
   }
   const long long cap = (long long)per * num_sms;
-  long long want = (work_items + 1023) / 1024;
-  if (want < num_sms) want = num_sms;
+  long long want = (work_items + 255) / 256;
+  if (want < min_ctas) want = min_ctas;
   if (want > cap) want = cap;
   return (int)want;
 }
 
 int launch_bfs_persistent(const BfsPersistentArgs& a, cudaStream_t st) {
-  const int grid = coop_grid(bfs_persistent_kernel, a.num_sms, a.n);
+  // small graphs get few CTAs: the level barriers then cost less
+  const int grid = coop_grid(bfs_persistent_kernel, a.num_sms, 16, a.n);
   if (grid <= 0) return -1;
   cudaMemsetAsync(a.ctrl, 0, sizeof(BfsCtrl), st);
-  note_launch(2);
-  bfs_persistent_init_kernel<<<1, 1, 0, st>>>(a.src, a.levels, a.visited, a.fb0, a.q0);
+  note_launch();
   int n = a.n;
   long long te = a.total_edges;
   const int* rp = a.rowptr;
@@ -425,13 +440,14 @@ int launch_bfs_persistent(const BfsPersistentArgs& a, cudaStream_t st) {
   unsigned* vis = a.visited;
   unsigned* f0 = a.fb0;
   unsigned* f1 = a.fb1;
+  unsigned* f2 = a.fb2;
   int* q0 = a.q0;
   int* q1 = a.q1;
   BfsCtrl* ctrl = a.ctrl;
   double al = a.alpha, be = a.beta;
   int src = a.src;
   int* err = a.err;
-  void* args[] = {&n, &te, &rp, &cl, &lv, &vis, &f0, &f1, &q0, &q1, &ctrl, &al, &be, &src, &err};
+  void* args[] = {&n, &te, &rp, &cl, &lv, &vis, &f0, &f1, &f2, &q0, &q1, &ctrl, &al, &be, &src, &err};
   cudaError_t e = cudaLaunchCooperativeKernel((void*)bfs_persistent_kernel, grid, 256, args, 0, st);
   return e == cudaSuccess ? 0 : -2;
 }
@@ -462,7 +478,7 @@ int launch_hub_chunks(int n, const int* rowptr, int deg_cut, int4* chunk, int* n
 }
 
 int launch_msbfs_persistent(const MsBfsArgs& a, cudaStream_t st) {
-  const int grid = coop_grid(msbfs_persistent_kernel, a.num_sms, a.n);
+  const int grid = coop_grid(msbfs_persistent_kernel, a.num_sms, a.num_sms, a.n);
   if (grid <= 0) return -1;
   cudaMemsetAsync(a.ctrl, 0, sizeof(BfsCtrl), st);
   note_launch(2);

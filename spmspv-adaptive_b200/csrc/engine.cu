@@ -194,7 +194,7 @@ extern "C" int spmx_destroy(spmx_handle_t h) {
   spmx_csr5_postprocess(h);
   spmx_tiled_postprocess(h);
   dfree(h->bfs_visited); dfree(h->bfs_front); dfree(h->bfs_q[0]); dfree(h->bfs_q[1]);
-  dfree(h->bfs_cnt); dfree(h->bfs_edges); dfree(h->bfs_fb1); dfree(h->bfs_ctrl);
+  dfree(h->bfs_cnt); dfree(h->bfs_edges); dfree(h->bfs_fb1); dfree(h->bfs_fb2); dfree(h->bfs_ctrl);
   dfree(h->ms_visit); dfree(h->ms_front0); dfree(h->ms_front1); dfree(h->ms_next);
   dfree(h->ms_q0); dfree(h->ms_q1); dfree(h->ms_srcs); dfree(h->ms_tmp); dfree(h->ms_ctrl);
   dfree(h->ms_hchunk); dfree(h->ms_hcnt); dfree(h->ms_hacc); dfree(h->ms_hleft); dfree(h->ms_hcounters);

@@ -132,6 +132,7 @@ struct spmx_handle_s {
   double bfs_alpha = 14.0, bfs_beta = 24.0, msbfs_alpha = 12.0;
   unsigned* bfs_visited = nullptr;
   unsigned* bfs_front = nullptr;
+  unsigned* bfs_fb2 = nullptr;
   int* bfs_q[2] = {nullptr, nullptr};
   int* bfs_cnt = nullptr;                  // [0..1] queue counts
   unsigned long long* bfs_edges = nullptr; // [0..1]
