@@ -1,3 +1,4 @@
+#include <algorithm>
 // CSC SpMSpV kernels: y = alpha * A * x with x sparse (x_key, x_val).
 //
 // Stage 1, csc_scan_kernel: gathers the length of every selected column
@@ -118,19 +119,43 @@ csc_lb_kernel(CscArgs a, CscScratch s, int variant, float* __restrict__ y,
   }
 }
 
+// y is zero-filled by the grid launched before this one (zero_fill_kernel).
+// With programmatic dependent launch this grid starts early: it reads x, the
+// column bounds and the first row / value while y is being cleared, and waits
+// (griddepcontrol.wait, a no-op without the launch attribute) only before its
+// first atomic.
 template <int G>
 __global__ void __launch_bounds__(256)
 csc_naive_kernel(CscArgs a, float* __restrict__ y) {
   const long long gid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   const int i = (int)(gid / G);
   const int g = (int)(gid % G);
-  if (i >= a.x_nnz) return;
-  const int key = __ldg(a.x_key + i);
-  if ((unsigned)key >= (unsigned)a.n) { if (g == 0) flag_error(a.err, kDevErrOob); return; }
-  const int cs = __ldg(a.colptr + key), ce = __ldg(a.colptr + key + 1);
-  const float xv = (float)(a.alpha * (double)__ldg(a.x_val + i));
+  int cs = 0, ce = 0, r0 = -1;
+  float xv = 0.f, v0 = 0.f;
+  bool ok = i < a.x_nnz;
+  if (ok) {
+    const int key = __ldg(a.x_key + i);
+    if ((unsigned)key >= (unsigned)a.n) {
+      if (g == 0) flag_error(a.err, kDevErrOob);
+      ok = false;
+    } else {
+      cs = __ldg(a.colptr + key);
+      ce = __ldg(a.colptr + key + 1);
+      xv = (float)(a.alpha * (double)__ldg(a.x_val + i));
+      if (cs + g < ce) {
+        r0 = __ldg(a.row + cs + g);
+        v0 = __ldg(a.val + cs + g);
+      }
+    }
+  }
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  if (!ok) return;
+  if (cs + g < ce) {
+    if ((unsigned)r0 < (unsigned)a.m) atomicAdd(y + r0, v0 * xv);
+    else flag_error(a.err, kDevErrOob);
+  }
 #pragma unroll 4
-  for (int k = cs + g; k < ce; k += G) {
+  for (int k = cs + g + G; k < ce; k += G) {
     const int r = __ldg(a.row + k);
     if ((unsigned)r < (unsigned)a.m) atomicAdd(y + r, __ldg(a.val + k) * xv);
     else flag_error(a.err, kDevErrOob);
@@ -190,6 +215,45 @@ int launch_csc_lb(const CscArgs& a, const CscScratch& s, int variant, float* y,
     case 32: { constexpr int G = 32; BODY; break; }                             \
     default: return -1;                                                         \
   }
+
+// y[0..m) = 0; lets the next grid on the stream launch right away
+__global__ void zero_fill_kernel(float* __restrict__ y, long long m) {
+  asm volatile("griddepcontrol.launch_dependents;");
+  const long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long nt = (long long)gridDim.x * blockDim.x;
+  if ((((uintptr_t)y) & 15u) == 0) {
+    float4* y4 = reinterpret_cast<float4*>(y);
+    const long long m4 = m >> 2;
+    for (long long i = tid; i < m4; i += nt) y4[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+    for (long long i = (m4 << 2) + tid; i < m; i += nt) y[i] = 0.f;
+  } else {
+    for (long long i = tid; i < m; i += nt) y[i] = 0.f;
+  }
+}
+
+// zero y, then the naive CSC SpMSpV as a programmatic dependent launch
+int launch_csc_naive_zeroed(const CscArgs& a, int group, float* y, int num_sms, cudaStream_t st) {
+  if (a.m > 0) {
+    const long long blocks = std::min<long long>(((long long)a.m + 1023) / 1024, (long long)num_sms * 4);
+    note_launch();
+    zero_fill_kernel<<<(unsigned)std::max(1LL, blocks), 256, 0, st>>>(y, a.m);
+  }
+  if (a.x_nnz <= 0) return 0;
+  const long long threads = (long long)a.x_nnz * group;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)((threads + 255) / 256));
+  cfg.blockDim = dim3(256);
+  cfg.stream = st;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  note_launch();
+  cudaError_t e = cudaSuccess;
+  SPMX_GROUP_SWITCH(group, (e = cudaLaunchKernelEx(&cfg, csc_naive_kernel<G>, a, y)));
+  return e == cudaSuccess ? 0 : -2;
+}
 
 int launch_csc_naive(const CscArgs& a, int group, float* y, cudaStream_t st) {
   if (a.x_nnz <= 0) return 0;

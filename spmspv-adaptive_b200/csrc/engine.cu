@@ -737,10 +737,12 @@ static int csc_atomic(spmx_handle_t h, int variant, float alpha, float* y, int* 
                       float* yval, int* ynnz) {
   cudaStream_t st = h->stream;
   const CscArgs a = csc_args(h, alpha);
-  SPMX_CUDA(cudaMemsetAsync(y, 0, 4 * (size_t)h->m, st));
   if (variant == SPMX_CSC_NAIVE) {
-    if (launch_csc_naive(a, col_group(h), y, st)) return set_error(SPMX_ERR_INVALID_VALUE, "bad column group");
+    // zero-fill and SpMSpV overlap through a programmatic dependent launch
+    if (launch_csc_naive_zeroed(a, col_group(h), y, h->num_sms, st))
+      return set_error(SPMX_ERR_INVALID_VALUE, "bad column group");
   } else {
+    SPMX_CUDA(cudaMemsetAsync(y, 0, 4 * (size_t)h->m, st));
     SPMX_TRY(ensure_csc_scratch(h));
     if (launch_csc_scan(a, h->cs, h->ls, kCscLbNT * kCscLbVT, st))
       return set_error(SPMX_ERR_INVALID_VALUE, "scan capacity");

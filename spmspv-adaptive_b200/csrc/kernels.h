@@ -100,6 +100,8 @@ int launch_csc_scan(const CscArgs& a, const CscScratch& s, ScanScratch& ls,
 int launch_csc_lb(const CscArgs& a, const CscScratch& s, int variant, float* y,
                   int* pairs_row, float* pairs_val, int grid, cudaStream_t st);
 int launch_csc_naive(const CscArgs& a, int group, float* y, cudaStream_t st);
+// y = 0 then the naive CSC SpMSpV, as a programmatic dependent launch pair
+int launch_csc_naive_zeroed(const CscArgs& a, int group, float* y, int num_sms, cudaStream_t st);
 int launch_csc_naive_pairs(const CscArgs& a, const CscScratch& s, int group,
                            int* pairs_row, float* pairs_val, cudaStream_t st);
 
