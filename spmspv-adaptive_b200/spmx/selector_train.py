@@ -113,7 +113,7 @@ class _RegressionPick:
 
     def __init__(self, reg):
         self.reg = reg
-        self.tree_ = reg.tree_
+        self.tree_ = getattr(reg, "tree_", None)  # set again after fitting
         self.classes_ = np.arange(NUM_KERNELS)
 
     def predict(self, X):
@@ -123,46 +123,74 @@ class _RegressionPick:
         return int(np.argmin(self.tree_.value[node][:, 0]))
 
 
+def _cv_pick(make, grid, X, T, fit_kw, folds=5, seed=4):
+    """The hyper-parameters with the lowest mean cross-validated regret."""
+    from sklearn.model_selection import KFold
+    best, best_r = None, None
+    kf = KFold(n_splits=min(folds, len(X)), shuffle=True, random_state=seed)
+    for params in grid:
+        rs = []
+        for a, b in kf.split(X):
+            m = make(params)
+            fit_kw(m, X[a], T[a])
+            p = m.predict(X[b])
+            rs.append(float(np.mean(T[b, p] / T[b].min(axis=1))))
+        r = float(np.mean(rs))
+        if best_r is None or r < best_r - 1e-12:
+            best, best_r = params, r
+    return best, best_r
+
+
 def fit(data_path, out_inc, report=True):
     """Fit a classification tree (the reference's model) and a multi-output
-    regression tree on log kernel times; keep the one with the lower held-out
-    regret."""
-    from sklearn.model_selection import GridSearchCV, train_test_split
+    regression tree on log kernel times, each with the hyper-parameters of the
+    lowest cross-validated regret on a 70/30 split (random_state=4, as the
+    reference's model/1-test_dtree.py); keep the one with the lower held-out
+    regret, then refit it on every case for export."""
+    from sklearn.model_selection import train_test_split
     from sklearn.tree import DecisionTreeClassifier, DecisionTreeRegressor
     recs, X, T = _load(data_path)
     y = T.argmin(axis=1)
     idx = np.arange(len(y))
     tr, te = train_test_split(idx, test_size=0.3, random_state=4)
-    cv = min(5, max(2, len(tr) // 8))
-    # classification tree: sample weight = what a wrong pick can cost
-    w = (T[tr].max(axis=1) / T[tr].min(axis=1))
-    clf = GridSearchCV(DecisionTreeClassifier(random_state=4),
-                       {"criterion": ["gini", "entropy"], "max_depth": list(range(1, 11))},
-                       cv=cv)
-    clf.fit(X[tr], y[tr], sample_weight=w)
-    reg = GridSearchCV(DecisionTreeRegressor(random_state=4),
-                       {"max_depth": list(range(2, 13)), "min_samples_leaf": [1, 2, 4]}, cv=cv)
-    reg.fit(X[tr], np.log(T[tr]))
-    cands = {"classifier": clf.best_estimator_, "regressor": _RegressionPick(reg.best_estimator_)}
+
+    def make_clf(p):
+        return DecisionTreeClassifier(random_state=4, **p)
+
+    def fit_clf(m, Xa, Ta):
+        # sample weight: what a wrong pick can cost
+        m.fit(Xa, Ta.argmin(axis=1), sample_weight=Ta.max(axis=1) / Ta.min(axis=1))
+
+    def make_reg(p):
+        return _RegressionPick(DecisionTreeRegressor(random_state=4, **p))
+
+    def fit_reg(m, Xa, Ta):
+        m.reg.fit(Xa, np.log(Ta))
+        m.tree_ = m.reg.tree_
+
+    clf_grid = [{"criterion": c, "max_depth": d} for c in ("gini", "entropy") for d in range(1, 11)]
+    reg_grid = [{"max_depth": d, "min_samples_leaf": l} for d in range(2, 13) for l in (1, 2, 4)]
+    cp, _ = _cv_pick(make_clf, clf_grid, X[tr], T[tr], fit_clf)
+    rp, _ = _cv_pick(make_reg, reg_grid, X[tr], T[tr], fit_reg)
+    clf = make_clf(cp)
+    fit_clf(clf, X[tr], T[tr])
+    reg = make_reg(rp)
+    fit_reg(reg, X[tr], T[tr])
+    cands = {"classifier": (clf, cp, make_clf, fit_clf), "regressor": (reg, rp, make_reg, fit_reg)}
 
     def regret(model, ix):
         p = model.predict(X[ix])
         return float(np.mean(T[ix, p] / T[ix].min(axis=1)))
 
-    kind = min(cands, key=lambda k: (regret(cands[k], te), regret(cands[k], tr)))
-    held = cands[kind]
+    kind = min(cands, key=lambda k: (regret(cands[k][0], te), regret(cands[k][0], tr)))
+    held, params, make, fitter = cands[kind]
     stats = {"model": kind, "train_regret": regret(held, tr), "test_regret": regret(held, te),
              "test_accuracy": float(np.mean(held.predict(X[te]) == y[te])),
-             "params": (clf if kind == "classifier" else reg).best_params_, "n": int(len(y))}
+             "params": params, "n": int(len(y))}
     # the exported selector: the chosen model and hyper-parameters refitted
     # on every case (the held-out figures above describe the 70 % fit)
-    if kind == "classifier":
-        tree = DecisionTreeClassifier(random_state=4, **clf.best_params_)
-        tree.fit(X, y, sample_weight=T.max(axis=1) / T.min(axis=1))
-    else:
-        r = DecisionTreeRegressor(random_state=4, **reg.best_params_)
-        r.fit(X, np.log(T))
-        tree = _RegressionPick(r)
+    tree = make(params)
+    fitter(tree, X, T)
     stats["all_regret"] = regret(tree, idx)
     with open(out_inc, "w") as f:
         f.write(export_cpp(tree, stats))
