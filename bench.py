@@ -301,30 +301,6 @@ def run_ours(args, world, rank, local):
         with open(tp) as f:
             traffic = json.load(f).get(f"{kname}_spmv_zipf1m")
 
-    # --- the selector against exhaustive timing of all eight kernels ---
-    exhaustive = []
-    if rank == 0:
-        from spmx import KERNEL_NAMES
-        for i, (dd, kd, vd, k) in enumerate(dx):
-            h.set_sparse_x(kd, vd, k)
-            times = []
-            for kid in range(len(KERNEL_NAMES)):
-                ts = []
-                for it in range(7):
-                    flush.fill_(float(it))
-                    rs.record(stream)
-                    h.run_kernel(kid, 1.0, y)
-                    re_.record(stream)
-                    stream.synchronize()
-                    if it >= 2:
-                        ts.append(rs.elapsed_time(re_))
-                times.append(statistics.median(ts))
-            best = int(np.argmin(times))
-            exhaustive.append({"density": dd, "chosen": KERNEL_NAMES[chosen[i]], "best": KERNEL_NAMES[best],
-                               "regret": times[chosen[i]] / times[best],
-                               "ms": {KERNEL_NAMES[j]: round(t, 4) for j, t in enumerate(times)}})
-        h.check_device_error()
-
     # --- e2e through the public API with host buffers ---
     pin_k = [torch.from_numpy(np.ascontiguousarray(k)).pin_memory() for _, k, _ in xs]
     pin_v = [torch.from_numpy(np.ascontiguousarray(v)).pin_memory() for _, _, v in xs]
@@ -357,6 +333,31 @@ def run_ours(args, world, rank, local):
     e2e_ms = statistics.mean([e2e_step() for _ in range(args.steps)])
     e2e_ms = allmax(e2e_ms, world)
     e2e_val = world * total_bytes / (e2e_ms * 1e-3) / 1e9
+
+    # --- the selector against exhaustive timing of all eight kernels (rank 0,
+    # after the last collective) ---
+    exhaustive = []
+    if rank == 0:
+        from spmx import KERNEL_NAMES
+        for i, (dd, kd, vd, k) in enumerate(dx):
+            h.set_sparse_x(kd, vd, k)
+            times = []
+            for kid in range(len(KERNEL_NAMES)):
+                ts = []
+                for it in range(7):
+                    flush.fill_(float(it))
+                    rs.record(stream)
+                    h.run_kernel(kid, 1.0, y)
+                    re_.record(stream)
+                    stream.synchronize()
+                    if it >= 2:
+                        ts.append(rs.elapsed_time(re_))
+                times.append(statistics.median(ts))
+            best = int(np.argmin(times))
+            exhaustive.append({"density": dd, "chosen": KERNEL_NAMES[chosen[i]], "best": KERNEL_NAMES[best],
+                               "regret": times[chosen[i]] / times[best],
+                               "ms": {KERNEL_NAMES[j]: round(t, 4) for j, t in enumerate(times)}})
+        h.check_device_error()
 
     # --- BFS on R-MAT scale 14 (plain), bit-exact check against the oracle ---
     bfs = run_bfs_plain(torch, dev, stream, args) if rank == 0 and not args.no_bfs else None
