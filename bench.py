@@ -485,10 +485,10 @@ def run_batched_spmspv(torch, dev, stream, args):
     """Batched forward + adjoint SpMSpV: Chung-Lu power-law matrix (n 4,194,304,
     degree exponent 2.1, average degree 32, values N(0,1), seed 5) and 256
     sparse x with nnz log-uniform in [10, 100,000] (N(0,1) values, distinct
-    uniform positions).  One CUDA graph holds the forward Y = A X and the
-    backward (dxval, dvals) for a fixed upstream dY; it is timed against 256
-    sequential single-vector calls of the same entry points (those without
-    dvals, i.e. less work than the batch)."""
+    uniform positions).  One CUDA graph holds the forward Y = A X (m x 256)
+    and the backward (dxval, dvals) for a fixed upstream dY; it is timed
+    against 256 sequential single-vector calls (adaptive SpMSpV forward into a
+    dense y, one-vector backward without dvals: less work than the batch)."""
     import spmx
     from spmx import gen
     import oracle.oracle as orc
@@ -514,20 +514,21 @@ def run_batched_spmspv(torch, dev, stream, args):
     xp, xk, xv = t(xptr), t(xkey), t(xval)
     gen_t = torch.Generator(device=dev)
     gen_t.manual_seed(5)
-    dY = torch.randn((nvec, m), device=dev, generator=gen_t)
-    Y = torch.empty((nvec, m), device=dev)
+    dY = torch.randn((m, nvec), device=dev, generator=gen_t)
+    Y = torch.empty((m, nvec), device=dev)
+    tot = int(xptr[-1])
     dxval = torch.empty(len(xkey), device=dev)
     dvals = torch.empty(A.nnz, device=dev)
     s = torch.cuda.Stream(device=dev)
     h.set_stream(s)
     with torch.cuda.stream(s):
-        h.spmspv_batched(xp, xk, xv, 1.0, Y)
-        h.spmspv_batched_backward(xp, xk, xv, 1.0, dY, dxval, dvals)
+        h.spmspv_batched(xp, xk, xv, 1.0, Y, x_total=tot)
+        h.spmspv_batched_backward(xp, xk, xv, 1.0, dY, dxval, dvals, x_total=tot)
     s.synchronize()
     g = torch.cuda.CUDAGraph()
     with torch.cuda.graph(g, stream=s):
-        h.spmspv_batched(xp, xk, xv, 1.0, Y)
-        h.spmspv_batched_backward(xp, xk, xv, 1.0, dY, dxval, dvals)
+        h.spmspv_batched(xp, xk, xv, 1.0, Y, x_total=tot)
+        h.spmspv_batched_backward(xp, xk, xv, 1.0, dY, dxval, dvals, x_total=tot)
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     reps = max(args.steps, 5)
     with torch.cuda.stream(s):
@@ -548,17 +549,25 @@ def run_batched_spmspv(torch, dev, stream, args):
     for v in (0, nvec // 2, int(np.argmax(sizes))):
         a, b = xptr[v], xptr[v + 1]
         y64, mag, _ = orc.spmspv_csc_f64(m, colptr_h, row_h, cval_h, xkey[a:b], xval[a:b])
-        Yh = Y[v].cpu().numpy()
+        Yh = Y[:, v].cpu().numpy()
         ok = ok and orc.within_tol(Yh, y64, mag, 1e-5)[0]
     bins = int(np.sum(colptr_h[xkey + 1] - colptr_h[xkey]))
-    # 256 sequential single-vector calls (forward + backward), same entry points
-    per = [(t(np.array([0, xptr[v + 1] - xptr[v]], np.int32)), xk[xptr[v]:xptr[v + 1]],
-            xv[xptr[v]:xptr[v + 1]]) for v in range(nvec)]
+    # 256 sequential single-vector calls: the forward through the adaptive
+    # single-vector engine (selector + CSC SpMSpV into a dense y), the backward
+    # through the batched entry point with one vector and without dvals (its
+    # dxval pass walks only the vector's columns)
+    h.allocPreBuffer()
+    per = [(xk[xptr[v]:xptr[v + 1]], xv[xptr[v]:xptr[v + 1]], int(xptr[v + 1] - xptr[v]),
+            t(np.array([0, xptr[v + 1] - xptr[v]], np.int32)), dY[:, v].contiguous())
+           for v in range(nvec)]
+    y1 = torch.empty(m, device=dev)
     with torch.cuda.stream(s):
         def plain():
-            for v, (p1, k1, v1) in enumerate(per):
-                h.spmspv_batched(p1, k1, v1, 1.0, Y[v:v + 1])
-                h.spmspv_batched_backward(p1, k1, v1, 1.0, dY[v:v + 1], dxval[xptr[v]:xptr[v + 1]], None)
+            for v, (k1, v1, n1, p1, dy1) in enumerate(per):
+                h.set_sparse_x(k1, v1, n1)
+                h.run_adaptive(1.0, y1)
+                h.spmspv_batched_backward(p1, k1, v1, 1.0, dy1, dxval[xptr[v]:xptr[v + 1]], None,
+                                          x_total=n1)
         plain()
         tp = []
         for _ in range(max(2, reps // 3)):
@@ -572,15 +581,16 @@ def run_batched_spmspv(torch, dev, stream, args):
     h.set_stream(stream)
     mb, mp = statistics.median(tb), statistics.median(tp)
     xn = int(xptr[-1])
-    fwd_b = 16 * xn + 8 * bins + 4 * nvec * m
-    bwd_b = 16 * xn + 16 * bins + 4 * A.nnz + 4 * xn
+    # compulsory bytes: the batch, A once per pass, the dense Y / dY once
+    fwd_b = 12 * xn + 4 * (m + 1) + 8 * A.nnz + 4 * nvec * m
+    bwd_b = 12 * xn + 2 * (4 * (m + 1) + 8 * A.nnz) + 4 * nvec * m + 4 * A.nnz + 4 * xn
     h.Destroy()
     return {"matrix": "chung-lu n 4,194,304, exponent 2.1, average degree 32, seed 5",
             "nnz": int(A.nnz), "nvec": nvec, "x_nnz_total": xn, "products": bins,
             "graph_fwd_bwd_ms": mb, "plain256_fwd_bwd_ms": mp, "speedup": mp / mb,
             "eff_gbs": (fwd_b + bwd_b) / (mb * 1e-3) / 1e9, "forward_within_1e-5": bool(ok),
-            "note": "the 256 single calls skip dvals (a single call overwrites it, so a batch "
-                    "gradient from single calls needs extra sums); the graph computes dvals too"}
+            "note": "single calls: adaptive single-vector SpMSpV forward + one-vector backward "
+                    "without dvals (less work than the batch, which also computes dvals)"}
 
 
 def run_adjoint(torch, dev, stream, args):

@@ -350,25 +350,26 @@ int spmx_spmv_backward_sparse(spmx_handle_t h, const float* d_x,
 
 /* ======================= batched SpMSpV (FP32) ============================= */
 /* No reference counterpart (the reference runs one vector per call).  nvec
- * sparse vectors in one concatenated list: vector v owns entries
- * [xptr[v], xptr[v+1]) of (xkey, xval); xptr has nvec + 1 entries, all
- * pointers are device pointers (xkey and xval may be NULL when the batch has
- * no entries; with entries the device error word records SPMX_ERR_OOB).  Forward: Y[v * m + i] = alpha * (A x_v)[i]
- * (Y dense, nvec x m, zero-filled by the call).  One persistent kernel with a
- * device work queue of 256-entry chunks; needs the CSC with values.  No host
- * synchronisation: after one call outside stream capture (which allocates the
- * handle's 4-byte work counter) both entry points can be captured in a CUDA
- * graph.  Concurrent batched calls on one handle race on the counter. */
-int spmx_spmspv_batched(spmx_handle_t h, int nvec, const int* d_xptr, const int* d_xkey,
-                        const float* d_xval, float alpha, float* d_Y);
-/* Adjoint of the batch for an upstream gradient dY (nvec x m):
- *   dxval[e] = alpha * sum over column xkey[e] of A[k] * dY[v * m + row_k]
- *   dvals[k] = alpha * sum over the batch of xval[e] * dY[v * m + row_k]
- * (dvals in CSR order, overwritten; the first call with dvals builds a
- * CSC-to-CSR permutation and synchronises).  Either output may be NULL. */
-int spmx_spmspv_batched_backward(spmx_handle_t h, int nvec, const int* d_xptr, const int* d_xkey,
-                                 const float* d_xval, float alpha, const float* d_dY,
-                                 float* d_dxval, float* d_dvals);
+ * (<= 1024) sparse vectors in one concatenated list: vector v owns entries
+ * [xptr[v], xptr[v+1]) of (xkey, xval); xptr has nvec + 1 entries and
+ * x_total = xptr[nvec] is also passed on the host (it sizes the scratch).  All
+ * arrays are device pointers.  Together the vectors are a sparse n x nvec
+ * matrix X and the call computes Y = alpha * A X, Y dense m x nvec row-major
+ * (Y[i * nvec + v]), every entry written.  The batch is inverted by column,
+ * then one warp per row of A accumulates the row of Y in shared memory.
+ * Needs the CSR with values.  No host synchronisation once the scratch for
+ * x_total exists: after one call outside stream capture with the largest
+ * x_total, both entry points can be captured in a CUDA graph. */
+int spmx_spmspv_batched(spmx_handle_t h, int nvec, int x_total, const int* d_xptr,
+                        const int* d_xkey, const float* d_xval, float alpha, float* d_Y);
+/* Adjoint of the batch for an upstream gradient dY (m x nvec, row-major):
+ *   dxval[e] = alpha * sum_i A[i][xkey[e]] * dY[i * nvec + v(e)]   (needs the CSC)
+ *   dvals[k] = alpha * sum over the batch's entries e in column col_k of
+ *              xval[e] * dY[row_k * nvec + v(e)]                    (CSR order)
+ * Both are written in full, deterministically.  Either output may be NULL. */
+int spmx_spmspv_batched_backward(spmx_handle_t h, int nvec, int x_total, const int* d_xptr,
+                                 const int* d_xkey, const float* d_xval, float alpha,
+                                 const float* d_dY, float* d_dxval, float* d_dvals);
 
 /* ======================= device counters ================================== */
 /* device pointers to the handle's counters: [0] y_nnz of the last SpMSpV,

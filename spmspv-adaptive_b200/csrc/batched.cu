@@ -2,26 +2,31 @@
 // runs one sparse vector per call).
 //
 // A batch is nvec sparse vectors in one concatenated list: vector v owns the
-// entries [xptr[v], xptr[v+1]) of (xkey, xval).  Forward: Y[v][:] = alpha *
-// A * x_v for every v (Y dense, nvec x m, row-major).  Backward, for an
-// upstream gradient dY (nvec x m):
-//   dxval[e] = alpha * sum_k A[k] * dY[v][row_k]     over column xkey[e]
-//              (the gradient of the stored values of x_v, same layout as xval)
-//   dvals[k] = alpha * sum_v sum_{e in v, xkey[e] = col_k} xval[e] * dY[v][row_k]
+// entries [xptr[v], xptr[v+1]) of (xkey, xval), x_total entries in all; seen
+// together they are a sparse n x nvec matrix X.  Forward: Y = alpha * A X,
+// Y dense m x nvec, row-major (Y[i * nvec + v] = alpha * (A x_v)[i]).
+// Backward, for an upstream gradient dY (m x nvec, row-major):
+//   dxval[e] = alpha * sum_i A[i][xkey[e]] * dY[i][v(e)]
+//              (the gradient of the stored values of x, same layout as xval)
+//   dvals[k] = alpha * sum_{e : xkey[e] = col_k} xval[e] * dY[row_k][v(e)]
 //              (the gradient of A's values, summed over the batch, CSR order)
 //
-// One persistent kernel serves the whole batch from a device work queue: a
-// CTA takes the next chunk of kBatchChunk consecutive entries of the
-// concatenated list (chunks cross vector boundaries, so uneven vectors
-// balance by themselves), scans the entries' column lengths in shared memory
-// and walks the chunk's products in tiles of equal size, each thread a run
-// of consecutive products found by one binary search.  The forward adds
-// into Y with FP32 atomics; the backward reads dY at the same positions,
-// reduces each entry's products in shared memory and adds dvals with
-// atomics.  The intermediates of the forward expansion are recomputed, never
-// stored.  Nothing is read back to the host (the entry count comes from
-// xptr[nvec] on the device), so both calls can be captured in a CUDA graph
-// once the handle's scratch exists (first call outside capture).
+// Design: the batch is inverted once per call (a stable radix sort of the
+// entries by column gives, per column, the (vector, entry) pairs that use
+// it), then
+//   forward  - one warp per row of A (CSR): lanes take the row's nonzeros,
+//              look up their columns' pairs and add a[k] * x into a shared
+//              row of nvec accumulators; the warp then stores the row of Y
+//              once, coalesced.  No zero-fill, no global atomics.
+//   dvals    - the same row walk against a shared copy of dY's row; every
+//              nonzero's gradient is a sum over its column's pairs in sorted
+//              order, stored once (deterministic).
+//   dxval    - one warp per entry: a dot product of the entry's column of A
+//              (CSC) with its vector's column of dY (deterministic).
+// The forward's shared accumulators take atomic adds only when two entries of
+// one vector meet in the same row.  Nothing is read back to the host, so after
+// one call outside stream capture (which sizes the scratch for x_total) both
+// entry points can be captured in a CUDA graph.
 #include <algorithm>
 #include <string>
 
@@ -32,216 +37,262 @@
 
 namespace spmx {
 
-constexpr int kBatchNT = 256;
-constexpr int kBatchChunk = 256;  // entries per work item
-constexpr int kBatchPT = 8;       // products per thread per tile
+constexpr int kBatchWarps = 8;      // warps per CTA in the row kernels
+constexpr int kBatchMaxVec = 1024;  // nvec limit (shared row accumulators)
 
-template <bool FWD>
-__global__ void __launch_bounds__(kBatchNT)
-spmspv_batched_kernel(int m, int n, int nvec, const int* __restrict__ xptr, const int* __restrict__ xkey,
-                      const float* __restrict__ xval, const int* __restrict__ colptr,
-                      const int* __restrict__ row, const float* __restrict__ aval,
-                      const int* __restrict__ perm, float alpha, float* __restrict__ Y,
-                      const float* __restrict__ dY, float* __restrict__ dxval, float* __restrict__ dvals,
-                      unsigned* work, int* err) {
-  __shared__ int s_off[kBatchChunk + 1];  // exclusive scan of column lengths
-  __shared__ int s_col0[kBatchChunk];     // first CSC position of each entry's column
-  __shared__ long long s_ybase[kBatchChunk];  // v * m of each entry
-  __shared__ float s_xv[kBatchChunk];
-  __shared__ float s_dx[kBatchChunk];
-  __shared__ int s_wtmp[kBatchNT / 32 + 1];
-  __shared__ int s_item;
-  const int tid = threadIdx.x;
-  const int total = __ldg(xptr + nvec);
-  if (total > 0 && (!xkey || !xval)) {  // entries but no arrays: nothing to read
-    if (tid == 0 && blockIdx.x == 0) flag_error(err, kDevErrOob);
-    return;
-  }
-  while (true) {
-    if (tid == 0) s_item = (int)atomicAdd(work, 1u);
-    __syncthreads();
-    const long long e0 = (long long)s_item * kBatchChunk;
-    if (e0 >= total) break;
-    const int ne = (int)min((long long)kBatchChunk, (long long)total - e0);
-    int len = 0;
-    if (tid < ne) {
-      const int e = (int)e0 + tid;
-      const int j = __ldg(xkey + e);
-      int v = 0;  // vector of entry e: last v with xptr[v] <= e
-      int lo = 0, hi = nvec;
-      while (hi - lo > 1) {
-        const int mid = (lo + hi) >> 1;
-        if (__ldg(xptr + mid) <= e) lo = mid;
-        else hi = mid;
-      }
-      v = lo;
-      if ((unsigned)j < (unsigned)n) {
-        const int a = __ldg(colptr + j);
-        len = __ldg(colptr + j + 1) - a;
-        s_col0[tid] = a;
-      } else {
-        flag_error(err, kDevErrOob);
-        s_col0[tid] = 0;
-      }
-      s_ybase[tid] = (long long)v * m;
-      s_xv[tid] = __ldg(xval + e);
-      s_dx[tid] = 0.f;
+// sort keys (column) and payloads (entry, vector) of every batch entry
+__global__ void batch_keys_kernel(int n, int nvec, int total, const int* __restrict__ xptr,
+                                  const int* __restrict__ xkey, unsigned* __restrict__ key,
+                                  unsigned* __restrict__ ent, unsigned* __restrict__ vec, int* err) {
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < total; e += gridDim.x * blockDim.x) {
+    int lo = 0, hi = nvec;  // vector of entry e: last v with xptr[v] <= e
+    while (hi - lo > 1) {
+      const int mid = (lo + hi) >> 1;
+      if (__ldg(xptr + mid) <= e) lo = mid;
+      else hi = mid;
     }
-    int tot = 0;
-    const int ex = block_exclusive_sum<kBatchNT, int>(len, s_wtmp, &tot);
-    if (tid < kBatchChunk) s_off[tid] = ex;
-    if (tid == 0) s_off[kBatchChunk] = tot;
-    __syncthreads();
-    // products of the chunk in tiles of kBatchNT * kBatchPT
-    for (int t0 = 0; t0 < tot; t0 += kBatchNT * kBatchPT) {
-      const int p0 = t0 + tid * kBatchPT;
-      if (p0 < tot) {
-        int lo = 0, hi = ne;  // entry holding product p0: last i with s_off[i] <= p0
-        while (hi - lo > 1) {
-          const int mid = (lo + hi) >> 1;
-          if (s_off[mid] <= p0) lo = mid;
-          else hi = mid;
-        }
-        int i = lo;
-        float dx_acc = 0.f;
-#pragma unroll
-        for (int q = 0; q < kBatchPT; ++q) {
-          const int p = p0 + q;
-          if (p >= tot) break;
-          while (s_off[i + 1] <= p) {
-            if (!FWD && dx_acc != 0.f) atomicAdd(&s_dx[i], dx_acc);
-            dx_acc = 0.f;
-            ++i;
-          }
-          const int k = s_col0[i] + (p - s_off[i]);
-          const int r = __ldg(row + k);
-          if ((unsigned)r >= (unsigned)m) {
-            flag_error(err, kDevErrOob);
-            continue;
-          }
-          const float a = __ldg(aval + k);
-          if (FWD) {
-            atomicAdd(Y + s_ybase[i] + r, alpha * s_xv[i] * a);
-          } else {
-            const float g = __ldg(dY + s_ybase[i] + r);
-            dx_acc += a * g;
-            if (dvals) atomicAdd(dvals + __ldg(perm + k), alpha * s_xv[i] * g);
-          }
-        }
-        if (!FWD && dx_acc != 0.f) atomicAdd(&s_dx[i], dx_acc);
-      }
-    }
-    __syncthreads();
-    if (!FWD && dxval && tid < ne) dxval[e0 + tid] = alpha * s_dx[tid];
-    __syncthreads();  // s_item, s_off, s_dx are reused by the next chunk
+    const int j = __ldg(xkey + e);
+    if ((unsigned)j >= (unsigned)n) flag_error(err, kDevErrOob);
+    key[e] = (unsigned)j < (unsigned)n ? (unsigned)j : (unsigned)n;  // invalid keys sort last
+    ent[e] = (unsigned)e;
+    vec[e] = (unsigned)lo;
   }
 }
 
-__global__ void iota_kernel(int n, unsigned* out) {
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) out[i] = (unsigned)i;
+// invptr[j] = first sorted position of column j, j in [0, n]
+__global__ void batch_bounds_kernel(int total, const unsigned* __restrict__ skey, int n,
+                                    int* __restrict__ invptr) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j > n) return;
+  int lo = 0, hi = total;
+  while (lo < hi) {
+    const int mid = (lo + hi) >> 1;
+    if ((int)__ldg(skey + mid) < j) lo = mid + 1;
+    else hi = mid;
+  }
+  invptr[j] = lo;
+}
+
+// Y[i][:] = alpha * sum_k A[i][k] * X[col_k][:], one warp per row
+__global__ void __launch_bounds__(kBatchWarps * 32)
+batch_forward_kernel(int m, int n, int nvec, const int* __restrict__ rowptr, const int* __restrict__ col,
+                     const float* __restrict__ val, const int* __restrict__ invptr,
+                     const unsigned* __restrict__ inv_ent, const unsigned* __restrict__ inv_vec,
+                     const float* __restrict__ xval, float alpha, float* __restrict__ Y, int* err) {
+  extern __shared__ float s_acc[];  // kBatchWarps rows of nvec
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  float* acc = s_acc + warp * nvec;
+  for (int v = lane; v < nvec; v += 32) acc[v] = 0.f;
+  __syncwarp();
+  const int nw = gridDim.x * kBatchWarps;
+  for (int i = blockIdx.x * kBatchWarps + warp; i < m; i += nw) {
+    const int a0 = __ldg(rowptr + i), a1 = __ldg(rowptr + i + 1);
+    for (int k = a0 + lane; k < a1; k += 32) {
+      const int j = __ldg(col + k);
+      if ((unsigned)j >= (unsigned)n) {
+        flag_error(err, kDevErrOob);
+        continue;
+      }
+      const float a = __ldg(val + k);
+      const int p1 = __ldg(invptr + j + 1);
+      for (int p = __ldg(invptr + j); p < p1; ++p)
+        atomicAdd(acc + __ldg(inv_vec + p), a * __ldg(xval + __ldg(inv_ent + p)));
+    }
+    __syncwarp();
+    float* yr = Y + (long long)i * nvec;
+    for (int v = lane; v < nvec; v += 32) {
+      yr[v] = alpha * acc[v];
+      acc[v] = 0.f;
+    }
+    __syncwarp();
+  }
+}
+
+// dvals[k] = alpha * sum over column col_k's pairs of xval[e] * dY[i][v(e)],
+// one warp per row with dY's row in shared memory
+__global__ void __launch_bounds__(kBatchWarps * 32)
+batch_dvals_kernel(int m, int n, int nvec, const int* __restrict__ rowptr, const int* __restrict__ col,
+                   const int* __restrict__ invptr, const unsigned* __restrict__ inv_ent,
+                   const unsigned* __restrict__ inv_vec, const float* __restrict__ xval, float alpha,
+                   const float* __restrict__ dY, float* __restrict__ dvals, int* err) {
+  extern __shared__ float s_dy[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  float* g = s_dy + warp * nvec;
+  const int nw = gridDim.x * kBatchWarps;
+  for (int i = blockIdx.x * kBatchWarps + warp; i < m; i += nw) {
+    const int a0 = __ldg(rowptr + i), a1 = __ldg(rowptr + i + 1);
+    if (a0 == a1) continue;  // warp-uniform
+    const float* dyr = dY + (long long)i * nvec;
+    for (int v = lane; v < nvec; v += 32) g[v] = __ldg(dyr + v);
+    __syncwarp();
+    for (int k = a0 + lane; k < a1; k += 32) {
+      const int j = __ldg(col + k);
+      float s = 0.f;
+      if ((unsigned)j < (unsigned)n) {
+        const int p1 = __ldg(invptr + j + 1);
+        for (int p = __ldg(invptr + j); p < p1; ++p)
+          s += __ldg(xval + __ldg(inv_ent + p)) * g[__ldg(inv_vec + p)];
+      } else {
+        flag_error(err, kDevErrOob);
+      }
+      dvals[k] = alpha * s;
+    }
+    __syncwarp();
+  }
+}
+
+// dxval[e] = alpha * sum_i A[i][xkey[e]] * dY[i][v(e)], one warp per entry
+__global__ void __launch_bounds__(256)
+batch_dxval_kernel(int m, int n, int nvec, int total, const int* __restrict__ xptr,
+                   const int* __restrict__ xkey, const int* __restrict__ colptr,
+                   const int* __restrict__ row, const float* __restrict__ cval, float alpha,
+                   const float* __restrict__ dY, float* __restrict__ dxval, int* err) {
+  const int lane = threadIdx.x & 31;
+  const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
+  for (long long e = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; e < total; e += nw) {
+    int lo = 0, hi = nvec;
+    while (hi - lo > 1) {
+      const int mid = (lo + hi) >> 1;
+      if (__ldg(xptr + mid) <= (int)e) lo = mid;
+      else hi = mid;
+    }
+    const int v = lo;
+    const int j = __ldg(xkey + e);
+    float s = 0.f;
+    if ((unsigned)j < (unsigned)n) {
+      const int c1 = __ldg(colptr + j + 1);
+      for (int q = __ldg(colptr + j) + lane; q < c1; q += 32) {
+        const int i = __ldg(row + q);
+        if ((unsigned)i < (unsigned)m) s += __ldg(cval + q) * __ldg(dY + (long long)i * nvec + v);
+        else flag_error(err, kDevErrOob);
+      }
+    }
+    s = warp_sum(s);
+    if (lane == 0) dxval[e] = alpha * s;
+  }
 }
 
 }  // namespace spmx
 
 using namespace spmx;
 
-static int batched_grid(spmx_handle_t h) {
+// scratch for the inverted batch of x_total entries (grown, never shrunk)
+static int ensure_batch_scratch(spmx_handle_t h, int total) {
+  if (h->batch_cap >= total && h->batch_invptr_n == h->n && h->batch_invptr) return SPMX_SUCCESS;
+  cudaStreamSynchronize(h->stream);
+  const int cap = std::max(total, 1);
+  for (auto& p : h->batch_buf) {
+    dfree(p);
+    p = nullptr;
+  }
+  dfree(h->batch_hist);
+  dfree(h->batch_hoff);
+  dfree(h->batch_invptr);
+  h->batch_hist = h->batch_hoff = h->batch_invptr = nullptr;
+  h->batch_cap = 0;
+  const char* what[6] = {"batch keys", "batch keys alt", "batch entries", "batch entries alt",
+                         "batch vectors", "batch vectors alt"};
+  for (int b = 0; b < 6; ++b) SPMX_TRY(dalloc(&h->batch_buf[b], 4 * (size_t)cap, what[b]));
+  const size_t hn = radix_hist_ints(cap);
+  SPMX_TRY(dalloc((void**)&h->batch_hist, 4 * hn, "batch hist"));
+  SPMX_TRY(dalloc((void**)&h->batch_hoff, 4 * hn, "batch hist off"));
+  SPMX_TRY(dalloc((void**)&h->batch_invptr, 4 * ((size_t)h->n + 1), "batch inverse pointers"));
+  h->batch_cap = cap;
+  h->batch_invptr_n = h->n;
+  return SPMX_SUCCESS;
+}
+
+// invert the batch: per column, the (entry, vector) pairs in entry order
+static int batch_invert(spmx_handle_t h, int nvec, int total, const int* xptr, const int* xkey,
+                        const unsigned** inv_ent, const unsigned** inv_vec) {
+  SPMX_TRY(ensure_batch_scratch(h, total));
+  cudaStream_t st = h->stream;
+  unsigned** b = reinterpret_cast<unsigned**>(h->batch_buf);
+  if (total > 0) {
+    note_launch();
+    batch_keys_kernel<<<std::min((total + 255) / 256, h->num_sms * 8), 256, 0, st>>>(
+        h->n, nvec, total, xptr, xkey, b[0], b[2], b[4], h->d_err);
+  }
+  RadixBuffers rb{b[0], b[1], b[2], b[3], b[4], b[5], h->batch_hist, h->batch_hoff, false};
+  int bits = 1;
+  while ((1LL << bits) <= (long long)h->n) ++bits;  // keys in [0, n]
+  if (radix_sort_pairs(rb, total, bits, h->ls, h->d_err, st))
+    return set_error(SPMX_ERR_INVALID_VALUE, "batch sort capacity");
+  const unsigned* skey = rb.result_in_alt ? b[1] : b[0];
+  *inv_ent = rb.result_in_alt ? b[3] : b[2];
+  *inv_vec = rb.result_in_alt ? b[5] : b[4];
+  note_launch();
+  batch_bounds_kernel<<<(h->n + 1 + 255) / 256, 256, 0, st>>>(total, skey, h->n, h->batch_invptr);
+  return SPMX_SUCCESS;
+}
+
+static int batched_common(spmx_handle_t h, int nvec, int total, const int* xptr) {
+  if (nvec < 1 || nvec > kBatchMaxVec)
+    return set_error(SPMX_ERR_INVALID_VALUE, "nvec must be in [1, 1024]");
+  if (total < 0) return set_error(SPMX_ERR_INVALID_VALUE, "x_total must be >= 0");
+  if (!xptr) return set_error(SPMX_ERR_INVALID_VALUE, "xptr is NULL");
+  if (!h->has_csr || (!h->val && h->nnz > 0))
+    return set_error(SPMX_ERR_NOT_READY, "batched SpMSpV needs the CSR input with values");
+  return SPMX_SUCCESS;
+}
+
+static int batch_rows_grid(spmx_handle_t h, const void* kernel, size_t smem) {
   int per = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, spmspv_batched_kernel<true>, kBatchNT, 0) !=
-          cudaSuccess ||
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, kBatchWarps * 32, smem) != cudaSuccess ||
       per < 1) {
     cudaGetLastError();
-    per = 4;
+    per = 2;
   }
-  return per * h->num_sms;
+  const long long want = ((long long)h->m + kBatchWarps - 1) / kBatchWarps;
+  return (int)std::max(1LL, std::min<long long>(want, (long long)per * h->num_sms));
 }
 
-// CSR index of every CSC position (stable sort of the CSR column keys with
-// the CSR index as payload), built once per matrix
-static int ensure_csc_perm(spmx_handle_t h) {
-  if (h->csc_perm && h->csc_perm_nnz == h->nnz && h->csc_perm_col == h->col) return SPMX_SUCCESS;
-  if (!h->has_csr) return set_error(SPMX_ERR_NOT_READY, "dvals needs the CSR input (spmx_input_csr)");
-  cudaStream_t st = h->stream;
-  const int nnz = h->nnz, n = h->n;
-  dfree(h->csc_perm);
-  h->csc_perm = nullptr;
-  SPMX_TRY(dalloc((void**)&h->csc_perm, 4 * (size_t)std::max(nnz, 1), "csc to csr permutation"));
-  if (nnz > 0) {
-    unsigned *k0 = nullptr, *k1 = nullptr, *p0 = nullptr, *p1 = nullptr;
-    int *hist = nullptr, *hoff = nullptr;
-    const size_t b = 4 * (size_t)nnz;
-    const size_t hn = radix_hist_ints(nnz);
-    int rc = SPMX_SUCCESS;
-    rc = rc ? rc : dalloc((void**)&k0, b, "perm keys");
-    rc = rc ? rc : dalloc((void**)&k1, b, "perm keys alt");
-    rc = rc ? rc : dalloc((void**)&p0, b, "perm payload");
-    rc = rc ? rc : dalloc((void**)&p1, b, "perm payload alt");
-    rc = rc ? rc : dalloc((void**)&hist, 4 * hn, "perm hist");
-    rc = rc ? rc : dalloc((void**)&hoff, 4 * hn, "perm hist off");
-    if (!rc) {
-      cudaMemcpyAsync(k0, h->col, b, cudaMemcpyDeviceToDevice, st);
-      note_launch();
-      iota_kernel<<<std::min((nnz + 255) / 256, h->num_sms * 16), 256, 0, st>>>(nnz, p0);
-      int bits = 1;
-      while ((1LL << bits) < (long long)std::max(n, 2)) ++bits;
-      RadixBuffers rb{k0, k1, p0, p1, nullptr, nullptr, hist, hoff, false};
-      if (radix_sort_pairs(rb, nnz, bits, h->ls, h->d_err, st))
-        rc = set_error(SPMX_ERR_INVALID_VALUE, "permutation sort capacity");
-      else
-        cudaMemcpyAsync(h->csc_perm, rb.result_in_alt ? p1 : p0, b, cudaMemcpyDeviceToDevice, st);
-    }
-    const cudaError_t se = cudaStreamSynchronize(st);
-    dfree(k0); dfree(k1); dfree(p0); dfree(p1); dfree(hist); dfree(hoff);
-    if (!rc && se != cudaSuccess) rc = set_error(SPMX_ERR_CUDA, cudaGetErrorString(se));
-    if (rc) {
-      dfree(h->csc_perm);
-      h->csc_perm = nullptr;
-      return rc;
-    }
-  }
-  h->csc_perm_nnz = h->nnz;
-  h->csc_perm_col = h->col;
-  return SPMX_SUCCESS;
-}
-
-static int batched_common(spmx_handle_t h, int nvec, const int* xptr, const int* xkey, const float* xval) {
-  if (nvec < 1) return set_error(SPMX_ERR_INVALID_VALUE, "nvec must be >= 1");
-  // xkey / xval may be NULL for a batch without entries (the kernel checks
-  // xptr[nvec] on the device and records an error if entries exist)
-  if (!xptr) return set_error(SPMX_ERR_INVALID_VALUE, "xptr is NULL");
-  if (!h->has_csc || !h->csc_val) return set_error(SPMX_ERR_NOT_READY, "batched SpMSpV needs the CSC with values");
-  if (!h->batch_work) SPMX_TRY(dalloc((void**)&h->batch_work, 4, "batch work counter"));
-  return SPMX_SUCCESS;
-}
-
-extern "C" int spmx_spmspv_batched(spmx_handle_t h, int nvec, const int* d_xptr, const int* d_xkey,
-                                   const float* d_xval, float alpha, float* d_Y) {
+extern "C" int spmx_spmspv_batched(spmx_handle_t h, int nvec, int x_total, const int* d_xptr,
+                                   const int* d_xkey, const float* d_xval, float alpha, float* d_Y) {
   SPMX_CHECK_HANDLE(h);
-  SPMX_TRY(batched_common(h, nvec, d_xptr, d_xkey, d_xval));
-  if (!d_Y) return set_error(SPMX_ERR_INVALID_VALUE, "Y is NULL");
-  cudaStream_t st = h->stream;
-  SPMX_CUDA(cudaMemsetAsync(d_Y, 0, 4 * (size_t)nvec * (size_t)h->m, st));
-  SPMX_CUDA(cudaMemsetAsync(h->batch_work, 0, 4, st));
+  SPMX_TRY(batched_common(h, nvec, x_total, d_xptr));
+  if (!d_Y && h->m > 0) return set_error(SPMX_ERR_INVALID_VALUE, "Y is NULL");
+  if (x_total > 0 && (!d_xkey || !d_xval)) return set_error(SPMX_ERR_INVALID_VALUE, "NULL batch arrays");
+  const unsigned *ie = nullptr, *iv = nullptr;
+  SPMX_TRY(batch_invert(h, nvec, x_total, d_xptr, d_xkey, &ie, &iv));
+  if (h->m == 0) return SPMX_SUCCESS;
+  const size_t smem = 4 * (size_t)kBatchWarps * nvec;
+  if (smem > 48 * 1024)
+    cudaFuncSetAttribute(batch_forward_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   note_launch();
-  spmspv_batched_kernel<true><<<batched_grid(h), kBatchNT, 0, st>>>(
-      h->m, h->n, nvec, d_xptr, d_xkey, d_xval, h->csc_colptr, h->csc_row, h->csc_val, nullptr, alpha, d_Y,
-      nullptr, nullptr, nullptr, h->batch_work, h->d_err);
+  batch_forward_kernel<<<batch_rows_grid(h, (const void*)batch_forward_kernel, smem), kBatchWarps * 32, smem,
+                         h->stream>>>(h->m, h->n, nvec, h->rowptr, h->col, h->val, h->batch_invptr, ie, iv,
+                                      d_xval, alpha, d_Y, h->d_err);
   return launch_ok("batched spmspv");
 }
 
-extern "C" int spmx_spmspv_batched_backward(spmx_handle_t h, int nvec, const int* d_xptr, const int* d_xkey,
-                                            const float* d_xval, float alpha, const float* d_dY,
-                                            float* d_dxval, float* d_dvals) {
+extern "C" int spmx_spmspv_batched_backward(spmx_handle_t h, int nvec, int x_total, const int* d_xptr,
+                                            const int* d_xkey, const float* d_xval, float alpha,
+                                            const float* d_dY, float* d_dxval, float* d_dvals) {
   SPMX_CHECK_HANDLE(h);
-  SPMX_TRY(batched_common(h, nvec, d_xptr, d_xkey, d_xval));
-  if (!d_dY) return set_error(SPMX_ERR_INVALID_VALUE, "dY is NULL");
-  if (d_dvals) SPMX_TRY(ensure_csc_perm(h));
+  SPMX_TRY(batched_common(h, nvec, x_total, d_xptr));
+  if (!d_dY && h->m > 0) return set_error(SPMX_ERR_INVALID_VALUE, "dY is NULL");
+  if (x_total > 0 && (!d_xkey || !d_xval)) return set_error(SPMX_ERR_INVALID_VALUE, "NULL batch arrays");
   cudaStream_t st = h->stream;
-  if (d_dvals) SPMX_CUDA(cudaMemsetAsync(d_dvals, 0, 4 * (size_t)std::max(h->nnz, 0), st));
-  SPMX_CUDA(cudaMemsetAsync(h->batch_work, 0, 4, st));
-  note_launch();
-  spmspv_batched_kernel<false><<<batched_grid(h), kBatchNT, 0, st>>>(
-      h->m, h->n, nvec, d_xptr, d_xkey, d_xval, h->csc_colptr, h->csc_row, h->csc_val, h->csc_perm, alpha,
-      nullptr, d_dY, d_dxval, d_dvals, h->batch_work, h->d_err);
+  if (d_dvals && h->nnz > 0) {
+    const unsigned *ie = nullptr, *iv = nullptr;
+    SPMX_TRY(batch_invert(h, nvec, x_total, d_xptr, d_xkey, &ie, &iv));
+    const size_t smem = 4 * (size_t)kBatchWarps * nvec;
+    if (smem > 48 * 1024)
+      cudaFuncSetAttribute(batch_dvals_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    note_launch();
+    batch_dvals_kernel<<<batch_rows_grid(h, (const void*)batch_dvals_kernel, smem), kBatchWarps * 32, smem,
+                         st>>>(h->m, h->n, nvec, h->rowptr, h->col, h->batch_invptr, ie, iv, d_xval, alpha,
+                               d_dY, d_dvals, h->d_err);
+  }
+  if (d_dxval && x_total > 0) {
+    if (!h->has_csc || !h->csc_val)
+      return set_error(SPMX_ERR_NOT_READY, "dxval needs the CSC with values (spmx_to_csc)");
+    const long long warps = x_total;
+    const int grid = (int)std::min<long long>((warps * 32 + 255) / 256, (long long)h->num_sms * 16);
+    note_launch();
+    batch_dxval_kernel<<<grid, 256, 0, st>>>(h->m, h->n, nvec, x_total, d_xptr, d_xkey, h->csc_colptr,
+                                             h->csc_row, h->csc_val, alpha, d_dY, d_dxval, h->d_err);
+  }
   return launch_ok("batched spmspv backward");
 }

@@ -114,11 +114,14 @@ struct spmx_handle_s {
   size_t ms_tmp_len = 0;
   void* ms_ctrl = nullptr;
   int ms_n = 0;
-  // batched SpMSpV: work-queue counter; CSC position -> CSR index (dvals)
-  unsigned* batch_work = nullptr;
-  int* csc_perm = nullptr;
-  int csc_perm_nnz = -1;
-  const int* csc_perm_col = nullptr;
+  // batched SpMSpV: the batch inverted by column (radix sort buffers for
+  // keys / entries / vectors and their alternates, column pointers)
+  void* batch_buf[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+  int* batch_hist = nullptr;
+  int* batch_hoff = nullptr;
+  int* batch_invptr = nullptr;
+  int batch_cap = 0;
+  int batch_invptr_n = -1;
   // hub chunks of the multi-source pull (built once per matrix)
   int4* ms_hchunk = nullptr;
   int* ms_hcnt = nullptr;

@@ -454,6 +454,20 @@ __global__ void tile_keys_kernel(int m, int n, const int* __restrict__ rowptr, c
   }
 }
 
+// tptr[t] = first position of key t in the sorted keys, t in [0, nkeys]
+__global__ void tile_bounds_kernel(int nnz, const unsigned* __restrict__ skey, long long nkeys,
+                                   int* __restrict__ tptr) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t > nkeys) return;
+  int lo = 0, hi = nnz;
+  while (lo < hi) {
+    const int mid = (int)(((long long)lo + hi) >> 1);
+    if ((long long)__ldg(skey + mid) < t) lo = mid + 1;
+    else hi = mid;
+  }
+  tptr[t] = lo;
+}
+
 // move sorted entries to their padded slots (tile t starts at pad_start[t]);
 // entries of the dump key (invalid columns) are dropped
 __global__ void tile_scatter_kernel(int nvalid, const unsigned* __restrict__ skey,
@@ -732,7 +746,7 @@ extern "C" int spmx_tiled_preprocess(spmx_handle_t h, int rb_rows, int win, int 
   }
   const size_t b = 4 * (size_t)std::max(nnz, 1);
   unsigned *k0 = nullptr, *k1 = nullptr, *p0 = nullptr, *p1 = nullptr, *v0 = nullptr, *v1 = nullptr;
-  int *hist = nullptr, *hoff = nullptr, *cnt = nullptr, *tptr = nullptr, *d_wsp = nullptr;
+  int *hist = nullptr, *hoff = nullptr, *tptr = nullptr, *d_wsp = nullptr;
   long long* d_pad = nullptr;
   const size_t hn = radix_hist_ints(std::max(nnz, 1));
   int rc = SPMX_SUCCESS;
@@ -744,7 +758,6 @@ extern "C" int spmx_tiled_preprocess(spmx_handle_t h, int rb_rows, int win, int 
   rc = rc ? rc : dalloc((void**)&v1, b, "tiled vals alt");
   rc = rc ? rc : dalloc((void**)&hist, 4 * hn, "tiled hist");
   rc = rc ? rc : dalloc((void**)&hoff, 4 * hn, "tiled hist off");
-  rc = rc ? rc : dalloc((void**)&cnt, 4 * (size_t)(ntiles + 1), "tiled counts");
   rc = rc ? rc : dalloc((void**)&tptr, 4 * (size_t)(ntiles + 2), "tiled pointers");
   rc = rc ? rc : dalloc((void**)&t->rb_row, 4 * (size_t)(nrb + 1), "tiled row blocks");
   rc = rc ? rc : dalloc((void**)&d_wsp, 4 * wsp.size(), "tiled warp splits");
@@ -769,10 +782,10 @@ extern "C" int spmx_tiled_preprocess(spmx_handle_t h, int rb_rows, int win, int 
       skey = rbuf.result_in_alt ? k1 : k0;
       spk = rbuf.result_in_alt ? p1 : p0;
       sval = (float*)(rbuf.result_in_alt ? v1 : v0);
-      cudaMemsetAsync(cnt, 0, 4 * (size_t)(ntiles + 1), st);
-      launch_count_keys(nnz, (int)ntiles + 1, (const int*)skey, cnt, h->d_err, st);
-      if (launch_scan_exclusive(cnt, tptr, (int)ntiles + 1, tptr + ntiles + 1, h->ls, h->d_err, st))
-        rc = set_error(SPMX_ERR_INVALID_VALUE, "tiled SpMV: scan capacity");
+      // tile pointers by binary search in the sorted keys (the dump key of
+      // invalid entries is ntiles, so tptr[ntiles] ends the valid entries)
+      note_launch();
+      tile_bounds_kernel<<<(unsigned)((ntiles + 1 + 256) / 256), 256, 0, st>>>(nnz, skey, ntiles + 1, tptr);
       if (!rc && cudaMemcpyAsync(htp.data(), tptr, 4 * (size_t)(ntiles + 2), cudaMemcpyDeviceToHost, st) !=
                      cudaSuccess)
         rc = set_error(SPMX_ERR_CUDA, "tiled SpMV: tile pointers");
@@ -863,7 +876,7 @@ extern "C" int spmx_tiled_preprocess(spmx_handle_t h, int rb_rows, int win, int 
   se = cudaStreamSynchronize(st);
   if (!rc && se != cudaSuccess) rc = set_error(SPMX_ERR_CUDA, cudaGetErrorString(se));
   dfree(k0); dfree(k1); dfree(p0); dfree(p1); dfree(v0); dfree(v1);
-  dfree(hist); dfree(hoff); dfree(cnt); dfree(tptr); dfree(d_wsp); dfree(d_pad);
+  dfree(hist); dfree(hoff); dfree(tptr); dfree(d_wsp); dfree(d_pad);
   if (rc) {
     spmx_tiled_postprocess(h);
     return rc;

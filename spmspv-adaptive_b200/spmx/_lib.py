@@ -89,8 +89,8 @@ _SIGS = {
     "spmx_tiled_preprocess": (c_int, [P, c_int, c_int, c_int, c_int]),
     "spmx_tiled_postprocess": (c_int, [P]),
     "spmx_tiled_info": (c_int, [P, P]),
-    "spmx_spmspv_batched": (c_int, [P, c_int, P, P, P, c_float, P]),
-    "spmx_spmspv_batched_backward": (c_int, [P, c_int, P, P, P, c_float, P, P, P]),
+    "spmx_spmspv_batched": (c_int, [P, c_int, c_int, P, P, P, c_float, P]),
+    "spmx_spmspv_batched_backward": (c_int, [P, c_int, c_int, P, P, P, c_float, P, P, P]),
     "spmx_tiledspmv": (c_int, [P, c_float, P]),
     "spmx_tiledspmspv": (c_int, [P, c_float, P]),
     "spmx_naivespmv": (c_int, [P, c_float, P]),

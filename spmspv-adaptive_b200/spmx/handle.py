@@ -368,19 +368,24 @@ class SpmspvHandle:
               "spmv_backward_sparse")
 
     # -- batched SpMSpV (no reference counterpart) ------------------------------
-    def spmspv_batched(self, xptr, xkey, xval, alpha, Y):
-        """Y[v, :] = alpha * A @ x_v for the nvec = len(xptr) - 1 sparse vectors
-        of the concatenated (xkey, xval); Y is (nvec, m) float32 on the device."""
+    def spmspv_batched(self, xptr, xkey, xval, alpha, Y, x_total=None):
+        """Y = alpha * A @ X for the nvec = len(xptr) - 1 sparse vectors of the
+        concatenated (xkey, xval); Y is (m, nvec) float32 on the device.
+        x_total (= xptr[-1]) is read back from xptr when not given."""
         nvec = int(xptr.numel()) - 1
-        check(lib.spmx_spmspv_batched(self._h, nvec, _i32(xptr), _i32(xkey), _f32(xval), float(alpha),
-                                      _f32(Y)), "spmspv_batched")
+        if x_total is None:
+            x_total = int(xptr[-1].item())
+        check(lib.spmx_spmspv_batched(self._h, nvec, int(x_total), _i32(xptr), _i32(xkey), _f32(xval),
+                                      float(alpha), _f32(Y)), "spmspv_batched")
 
-    def spmspv_batched_backward(self, xptr, xkey, xval, alpha, dY, dxval=None, dvals=None):
-        """dxval (layout of xval) and dvals (CSR order) for an upstream dY."""
+    def spmspv_batched_backward(self, xptr, xkey, xval, alpha, dY, dxval=None, dvals=None, x_total=None):
+        """dxval (layout of xval) and dvals (CSR order) for an upstream dY (m, nvec)."""
         nvec = int(xptr.numel()) - 1
-        check(lib.spmx_spmspv_batched_backward(self._h, nvec, _i32(xptr), _i32(xkey), _f32(xval),
-                                               float(alpha), _f32(dY), _f32(dxval), _f32(dvals)),
-              "spmspv_batched_backward")
+        if x_total is None:
+            x_total = int(xptr[-1].item())
+        check(lib.spmx_spmspv_batched_backward(self._h, nvec, int(x_total), _i32(xptr), _i32(xkey),
+                                               _f32(xval), float(alpha), _f32(dY), _f32(dxval),
+                                               _f32(dvals)), "spmspv_batched_backward")
 
     # -- BFS ---------------------------------------------------------------------------
     def bfs(self, source, levels, sync=True):

@@ -1,5 +1,7 @@
 """Batched SpMSpV forward and adjoint on the GPU against FP64 references.
 
+Y and dY are m x nvec, row-major (Y[i, v] = (A x_v)[i]).
+
 Forward: every vector of the batch against the oracle's SpmSpvCSCHost
 restatement, |y32 - y64| <= 1e-5 * max(|y64|, sum |a_ij x_j|).  Backward:
 dxval and dvals against FP64 sums of the same products, with the bound
@@ -46,7 +48,7 @@ def _refs(A, xptr, xkey, xval, dY, alpha):
         for e in range(xptr[v], xptr[v + 1]):
             j = xkey[e]
             ks = np.arange(colptr[j], colptr[j + 1])
-            g = dY[v, row[ks]].astype(np.float64)
+            g = dY[row[ks], v].astype(np.float64)
             a = cval[ks].astype(np.float64)
             dx[e] = alpha * np.sum(a * g)
             dxm[e] = abs(alpha) * np.sum(np.abs(a * g))
@@ -69,8 +71,8 @@ def _check_forward(A, xptr, xkey, xval, Y, alpha):
     for v in range(len(xptr) - 1):
         k, x = xkey[xptr[v]:xptr[v + 1]], xval[xptr[v]:xptr[v + 1]]
         y64, mag, _ = orc.spmspv_csc_f64(A.m, colptr, row, cval, k, x, alpha=alpha)
-        ok, _ = orc.within_tol(Y[v], y64, mag, RTOL)
-        assert ok, (v, orc.max_scaled_err(Y[v], y64, mag))
+        ok, _ = orc.within_tol(Y[:, v], y64, mag, RTOL)
+        assert ok, (v, orc.max_scaled_err(Y[:, v], y64, mag))
 
 
 def _close(got, ref, mag):
@@ -82,7 +84,7 @@ def test_batched_forward(torch_cuda, problem, alpha):
     torch = torch_cuda
     A, xptr, xkey, xval = problem
     h = make_handle(A, torch, hola=False)
-    Y = torch.full((len(xptr) - 1, A.m), 5.0, device="cuda")
+    Y = torch.full((A.m, len(xptr) - 1), 5.0, device="cuda")
     h.spmspv_batched(dev(xptr, torch), dev(xkey, torch), dev(xval, torch), alpha, Y)
     h.check_device_error()
     _check_forward(A, xptr, xkey, xval, Y.cpu().numpy(), alpha)
@@ -94,7 +96,7 @@ def test_batched_backward(torch_cuda, problem):
     alpha = 0.75
     h = make_handle(A, torch, hola=False)
     nvec = len(xptr) - 1
-    dY = np.random.default_rng(9).standard_normal((nvec, A.m)).astype(np.float32)
+    dY = np.random.default_rng(9).standard_normal((A.m, nvec)).astype(np.float32)
     dxval = torch.full((len(xkey),), 7.0, device="cuda")
     dvals = torch.full((A.nnz,), 7.0, device="cuda")
     h.spmspv_batched_backward(dev(xptr, torch), dev(xkey, torch), dev(xval, torch), alpha,
@@ -112,21 +114,22 @@ def test_batched_graph_replay(torch_cuda, problem):
     h = make_handle(A, torch, hola=False)
     nvec = len(xptr) - 1
     xp, xk, xv = dev(xptr, torch), dev(xkey, torch), dev(xval, torch)
-    dY = dev(np.random.default_rng(4).standard_normal((nvec, A.m)).astype(np.float32), torch)
-    Y = torch.empty((nvec, A.m), device="cuda")
+    dY = dev(np.random.default_rng(4).standard_normal((A.m, nvec)).astype(np.float32), torch)
+    Y = torch.empty((A.m, nvec), device="cuda")
     dxval = torch.empty(len(xkey), device="cuda")
     dvals = torch.empty(A.nnz, device="cuda")
+    tot = int(xptr[-1])  # host-side entry count: nothing is read back during capture
     s = torch.cuda.Stream()
     h.set_stream(s)
     with torch.cuda.stream(s):
         # first calls outside capture allocate the handle's scratch
-        h.spmspv_batched(xp, xk, xv, 1.0, Y)
-        h.spmspv_batched_backward(xp, xk, xv, 1.0, dY, dxval, dvals)
+        h.spmspv_batched(xp, xk, xv, 1.0, Y, x_total=tot)
+        h.spmspv_batched_backward(xp, xk, xv, 1.0, dY, dxval, dvals, x_total=tot)
     s.synchronize()
     g = torch.cuda.CUDAGraph()
     with torch.cuda.graph(g, stream=s):
-        h.spmspv_batched(xp, xk, xv, 1.0, Y)
-        h.spmspv_batched_backward(xp, xk, xv, 1.0, dY, dxval, dvals)
+        h.spmspv_batched(xp, xk, xv, 1.0, Y, x_total=tot)
+        h.spmspv_batched_backward(xp, xk, xv, 1.0, dY, dxval, dvals, x_total=tot)
     for _ in range(2):
         Y.fill_(3.0)
         dxval.fill_(3.0)
@@ -147,18 +150,19 @@ def test_batched_matches_single_calls(torch_cuda, problem):
     A, xptr, xkey, xval = problem
     h = make_handle(A, torch, hola=False)
     nvec = len(xptr) - 1
-    Yb = torch.empty((nvec, A.m), device="cuda")
+    Yb = torch.empty((A.m, nvec), device="cuda")
     h.spmspv_batched(dev(xptr, torch), dev(xkey, torch), dev(xval, torch), 1.0, Yb)
+    Ybh = Yb.cpu().numpy()
     colptr, row, cval = A.to_csc()
     for v in range(nvec):
         a, b = xptr[v], xptr[v + 1]
-        y1 = torch.empty((1, A.m), device="cuda")
+        y1 = torch.empty((A.m, 1), device="cuda")
         h.spmspv_batched(dev(np.array([0, b - a], np.int32), torch), dev(xkey[a:b], torch),
                          dev(xval[a:b], torch), 1.0, y1)
         y64, mag, _ = orc.spmspv_csc_f64(A.m, colptr, row, cval, xkey[a:b], xval[a:b])
-        ok, _ = orc.within_tol(y1.cpu().numpy()[0], y64, mag, RTOL)
+        ok, _ = orc.within_tol(y1.cpu().numpy()[:, 0], y64, mag, RTOL)
         assert ok
-        ok, _ = orc.within_tol(Yb[v].cpu().numpy(), y64, mag, RTOL)
+        ok, _ = orc.within_tol(Ybh[:, v], y64, mag, RTOL)
         assert ok
 
 
@@ -170,7 +174,24 @@ def test_batched_out_of_range_key(torch_cuda):
     xptr = np.array([0, 2], np.int32)
     xkey = np.array([3, A.n], np.int32)  # second key is out of range
     xval = np.ones(2, np.float32)
-    Y = torch.empty((1, A.m), device="cuda")
+    Y = torch.empty((A.m, 1), device="cuda")
     h.spmspv_batched(dev(xptr, torch), dev(xkey, torch), dev(xval, torch), 1.0, Y)
     with pytest.raises(SpmxError):
         h.check_device_error()
+
+
+def test_batched_deterministic(torch_cuda, problem):
+    """Backward results are bit-identical across calls (no atomics)."""
+    torch = torch_cuda
+    A, xptr, xkey, xval = problem
+    h = make_handle(A, torch, hola=False)
+    nvec = len(xptr) - 1
+    dY = dev(np.random.default_rng(8).standard_normal((A.m, nvec)).astype(np.float32), torch)
+    xp, xk, xv = dev(xptr, torch), dev(xkey, torch), dev(xval, torch)
+    outs = []
+    for _ in range(2):
+        dxval = torch.empty(len(xkey), device="cuda")
+        dvals = torch.empty(A.nnz, device="cuda")
+        h.spmspv_batched_backward(xp, xk, xv, 1.0, dY, dxval, dvals)
+        outs.append((dxval.cpu().numpy(), dvals.cpu().numpy()))
+    assert np.array_equal(outs[0][0], outs[1][0]) and np.array_equal(outs[0][1], outs[1][1])
