@@ -15,6 +15,7 @@ differences:
 usage:
   python -m spmx.selector_train collect OUT.jsonl      (GPU)
   python -m spmx.selector_train fit DATA.jsonl OUT.inc  (host, scikit-learn)
+  python -m spmx.selector_train compare DATA.jsonl      (host: other learners)
 """
 import json
 import math
@@ -199,6 +200,47 @@ def fit(data_path, out_inc, report=True):
     return tree, stats
 
 
+def compare(data_path, report=True):
+    """Held-out regret of other learners on the same 70/30 split, beside the
+    decision tree (the reference compares SVM / GBDT / random forest in
+    model/*.py).  Features are log-scaled for the distance- and kernel-based
+    learners.  Only the tree is exported: it compiles to branches."""
+    from sklearn.ensemble import GradientBoostingClassifier, RandomForestClassifier
+    from sklearn.model_selection import train_test_split
+    from sklearn.neighbors import KNeighborsClassifier
+    from sklearn.pipeline import make_pipeline
+    from sklearn.preprocessing import FunctionTransformer, StandardScaler
+    from sklearn.svm import SVC
+    from sklearn.tree import DecisionTreeClassifier
+    recs, X, T = _load(data_path)
+    y = T.argmin(axis=1)
+    tr, te = train_test_split(np.arange(len(y)), test_size=0.3, random_state=4)
+    w = T[tr].max(axis=1) / T[tr].min(axis=1)
+    logx = FunctionTransformer(lambda a: np.log1p(np.abs(a)) * np.sign(a))
+    learners = {
+        "decision tree": (DecisionTreeClassifier(random_state=4, max_depth=6), True),
+        "random forest": (RandomForestClassifier(n_estimators=200, random_state=4), True),
+        "gradient boosting": (GradientBoostingClassifier(random_state=4), True),
+        "svm (rbf)": (make_pipeline(logx, StandardScaler(), SVC(C=10.0, gamma="scale")), False),
+        "k nearest (5)": (make_pipeline(logx, StandardScaler(), KNeighborsClassifier(5)), False),
+    }
+    out = {}
+    for name, (model, weighted) in learners.items():
+        if weighted:
+            model.fit(X[tr], y[tr], sample_weight=w)
+        else:
+            model.fit(X[tr], y[tr])
+        p = model.predict(X[te])
+        out[name] = {"test_regret": float(np.mean(T[te, p] / T[te].min(axis=1))),
+                     "test_accuracy": float(np.mean(p == y[te]))}
+    best = T[te].min(axis=1)
+    out["always the overall best kernel"] = {
+        "test_regret": float(np.mean(T[te, np.bincount(y[tr]).argmax()] / best)), "test_accuracy": None}
+    if report:
+        print(json.dumps(out, indent=1))
+    return out
+
+
 def export_cpp(tree, stats):
     """The fitted tree as nested if/else over the feature vector."""
     t = tree.tree_
@@ -241,6 +283,8 @@ def main(argv):
         collect(argv[1])
     elif len(argv) >= 3 and argv[0] == "fit":
         fit(argv[1], argv[2])
+    elif len(argv) >= 2 and argv[0] == "compare":
+        compare(argv[1])
     else:
         print(__doc__)
         return 2

@@ -7,6 +7,7 @@ import json
 import os
 
 import numpy as np
+import pytest
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 DATA = os.path.join(ROOT, "spmspv-adaptive_b200", "spmx", "data", "selector_b200.jsonl")
@@ -58,3 +59,18 @@ def test_picks_on_the_benchmark_matrix():
             assert k.value in (0, 1, 2, 3), r["density"]
         if r["density"] >= 1.0:
             assert k.value in (6, 7), r["density"]
+
+
+def test_learner_comparison():
+    """The other learners (random forest, gradient boosting, SVM, k nearest)
+    are fitted and scored on the same held-out split; every learner beats
+    always running the single best kernel, and the exported tree is within a
+    few percent of the best of them."""
+    pytest.importorskip("sklearn")
+    from spmx import selector_train
+    out = selector_train.compare(DATA, report=False)
+    base = out.pop("always the overall best kernel")["test_regret"]
+    for name, r in out.items():
+        assert r["test_regret"] < base, name
+    best = min(r["test_regret"] for r in out.values())
+    assert out["decision tree"]["test_regret"] <= best * 1.05
