@@ -364,6 +364,7 @@ def run_ours(args, world, rank, local):
     bfs64 = run_bfs_batched(torch, dev, stream, args) if rank == 0 and not args.no_bfs else None
     batched = run_batched_spmspv(torch, dev, stream, args) if rank == 0 and not args.no_batched else None
     adjoint = run_adjoint(torch, dev, stream, args) if rank == 0 and not args.no_batched else None
+    ingest = run_ingest(torch, dev, stream, args) if rank == 0 and not args.no_ingest else None
 
     line = None
     if rank == 0:
@@ -394,6 +395,7 @@ def run_ours(args, world, rank, local):
             "batched_bfs": bfs64,
             "batched_spmspv": batched,
             "adjoint": adjoint,
+            "ingest": ingest,
         }
         print(json.dumps(line), flush=True)
     h.Destroy()
@@ -652,6 +654,110 @@ def run_adjoint(torch, dev, stream, args):
             "forward_gbs": fb / (f_ms * 1e-3) / 1e9, "backward_gbs": bb / (b_ms * 1e-3) / 1e9}
 
 
+def _ref_host_lib():
+    """The reference's host routines compiled from its sources (oracle/_ref),
+    or None where they were not built."""
+    import ctypes
+    so = os.path.join(ROOT, "oracle", "_ref", "libref_host.so")
+    if not os.path.exists(so):
+        return None
+    lib = ctypes.CDLL(so)
+    lib.ref_read_mtx.argtypes = [ctypes.c_char_p] + [ctypes.c_void_p] * 6
+    lib.ref_read_mtx.restype = None
+    lib.ref_free.argtypes = [ctypes.c_void_p]
+    return lib
+
+
+def run_ingest(torch, dev, stream, args):
+    """Matrix ingestion: the 1M-row Zipf matrix (16,777,216 entries, entries
+    shuffled with seed 1) written once as a MatrixMarket file, then
+      parse   spmx_mtx_read on all host threads (file -> COO),
+      gpu     pinned host-to-device copy of the COO + spmx_input_coo (radix
+              sort by column, then by row, row pointers) -> device CSR,
+    against the reference's ReadMTX (fscanf + std::sort by (row, col), one
+    thread) compiled from its sources, or the oracle's restatement of it
+    where that library is absent, run once on the same file.  The device CSR
+    is checked bit for bit against the generator's CSR."""
+    import ctypes
+    import tempfile
+    import spmx
+    from spmx import gen, io
+    import oracle.oracle as orc
+    A = gen.zipf_1m()
+    row = np.repeat(np.arange(A.m, dtype=np.int32), np.diff(A.rowptr))
+    p = np.random.default_rng(1).permutation(A.nnz)
+    tmpdir = tempfile.mkdtemp(prefix="spmx_ingest_")
+    path = os.path.join(tmpdir, "zipf1m.mtx")
+    try:
+        io.write_mtx(path, io.Coo(A.m, A.n, row[p], A.col[p], A.val[p]))
+        fbytes = os.path.getsize(path)
+        parse = []
+        for _ in range(3):
+            t0 = time.perf_counter()
+            C = io.read_mtx(path)
+            parse.append(time.perf_counter() - t0)
+        parse_s = statistics.median(parse)
+        pinned = [torch.from_numpy(a).pin_memory() for a in (C.row, C.col, C.val)]
+        dbuf = [torch.empty(C.nnz, dtype=t.dtype, device=dev) for t in pinned]
+        h = spmx.SpmspvHandle(A.m, A.n, A.nnz, stream=stream)
+        e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+        h2d, sort = [], []
+        for it in range(3 + max(args.steps // 4, 3)):
+            stream.synchronize()
+            e0.record(stream)
+            with torch.cuda.stream(stream):
+                for d, t in zip(dbuf, pinned):
+                    d.copy_(t, non_blocking=True)
+            e1.record(stream)
+            h.InputCOO(C.nnz, *dbuf)  # synchronous
+            e2.record(stream)
+            stream.synchronize()
+            if it >= 3:
+                h2d.append(e0.elapsed_time(e1))
+                sort.append(e1.elapsed_time(e2))
+        rp, cl, vl = h.get_csr()
+        exact = bool(np.array_equal(rp.cpu().numpy(), A.rowptr) and
+                     np.array_equal(cl.cpu().numpy(), A.col) and
+                     np.array_equal(vl.cpu().numpy().view(np.uint32), A.val.view(np.uint32)))
+        h.check_device_error()
+        h.Destroy()
+        h2d_ms, sort_ms = statistics.median(h2d), statistics.median(sort)
+        ref = _ref_host_lib()
+        t0 = time.perf_counter()
+        if ref is not None:
+            m_, n_, k_ = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+            ptrs = [ctypes.c_void_p() for _ in range(3)]
+            ref.ref_read_mtx(os.fsencode(path), ctypes.byref(m_), ctypes.byref(n_), ctypes.byref(k_),
+                             *[ctypes.byref(q) for q in ptrs])
+            ref_s = time.perf_counter() - t0
+            for q in ptrs:
+                ref.ref_free(q)
+            ref_kind = "reference"
+        else:
+            orc.mtx_read_sorted(path)
+            ref_s = time.perf_counter() - t0
+            ref_kind = "port"
+    finally:
+        if os.path.exists(path):
+            os.remove(path)
+        os.rmdir(tmpdir)
+    nnz = A.nnz
+    e2e_s = parse_s + (h2d_ms + sort_ms) * 1e-3
+    # algorithmic bytes of COO -> CSR: read 12 B per entry, write 8 B per entry + rowptr
+    alg = 20 * nnz + 4 * (A.m + 1)
+    return {"matrix": "zipf-1M, %d entries, MatrixMarket real general, %.0f MB, entries shuffled"
+                      % (nnz, fbytes / 1e6),
+            "parse_s": parse_s, "parse_entries_per_s": nnz / parse_s,
+            "parse_mb_per_s": fbytes / 1e6 / parse_s, "parse_threads": orc.raw.cpu_threads(),
+            "h2d_ms": h2d_ms, "coo_to_csr_ms": sort_ms,
+            "coo_to_csr_entries_per_s": nnz / (sort_ms * 1e-3),
+            "coo_to_csr_alg_gbs": alg / (sort_ms * 1e-3) / 1e9,
+            "file_to_device_csr_s": e2e_s, "csr_bit_exact": exact,
+            "reference_readmtx_s": ref_s, "reference_kind": ref_kind,
+            "reference_cores": 1,
+            "speedup_file_to_csr_vs_reference": ref_s / e2e_s}
+
+
 def cpu_baseline(A, xs, binl):
     """The reference's serial CPU routines (restated), one core, one sweep."""
     import oracle.oracle as orc
@@ -679,7 +785,7 @@ def cpu_baseline(A, xs, binl):
             "ms": best * 1e3}
 
 
-ONLY = ("batched-spmspv", "adjoint", "hola-spmv", "csr5-spmv", "naive-spmv", "tiled-spmv", "hola-spmspv", "csc-lb-atomic",
+ONLY = ("ingest", "batched-spmspv", "adjoint", "hola-spmv", "csr5-spmv", "naive-spmv", "tiled-spmv", "hola-spmspv", "csc-lb-atomic",
         "csc-naive-atomic", "csc-bucket", "csc-lb-sort", "bfs-rmat14", "bfs-batched")
 
 
@@ -701,6 +807,9 @@ def run_only(args):
         return 0
     if args.only == "adjoint":
         print(json.dumps(run_adjoint(torch, dev, stream, args)))
+        return 0
+    if args.only == "ingest":
+        print(json.dumps(run_ingest(torch, dev, stream, args)))
         return 0
     A, xs = make_inputs()
     d = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)  # noqa: E731
@@ -757,6 +866,7 @@ def main():
     ap.add_argument("--no-bfs", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-batched", action="store_true")
+    ap.add_argument("--no-ingest", action="store_true")
     ap.add_argument("--only", choices=ONLY, help="run one kernel (profiling helper)")
     ap.add_argument("--density", type=float, default=0.1)
     args = ap.parse_args()

@@ -12,6 +12,7 @@
  *   H    = hice-spmspv/hice/la/include/spmspv/csc-spmspv/spmspv.h
  *   DEV  = hice-spmspv/hice/la/include/spmspv/csc-spmspv/detail/device/
  *   TEST = hice-spmspv/hice/la/test/
+ *   INC  = hice-spmspv/hice/la/include/spmspv/
  *
  * Ownership follows the reference: CSR arrays and x buffers are caller-owned
  * device memory; CSC built by spmx_to_csc, Hola / CSR5 tables and scratch are
@@ -124,6 +125,18 @@ int spmx_to_csc(spmx_handle_t h);
 /* copy the handle's CSC into caller buffers (row[nnz], colptr[n+1],
  * val[nnz]; any may be NULL); asynchronous on the handle's stream */
 int spmx_copy_csc(spmx_handle_t h, int* d_row, int* d_colptr, float* d_val);
+/* COO (device arrays, any order, duplicates kept) -> handle-owned CSR sorted
+ * by (row, col), duplicates in input order.  The GPU replacement of the host
+ * sort after ReadMTX (mtx.hpp:335-360) and the coo2csr of the reference's
+ * drivers.  Synchronous; d_val may be NULL (pattern).  An index outside
+ * [0,m) x [0,n) returns SPMX_ERR_INVALID_VALUE and leaves the handle as it
+ * was.  Replaces the handle's CSR like spmx_input_csr (a CSC derived from
+ * the previous CSR by spmx_to_csc is dropped). */
+int spmx_input_coo(spmx_handle_t h, int nnz, const int* d_row, const int* d_col,
+                   const float* d_val);
+/* copy the handle's CSR into caller buffers (rowptr[m+1], col[nnz],
+ * val[nnz]; any may be NULL); asynchronous on the handle's stream */
+int spmx_copy_csr(spmx_handle_t h, int* d_rowptr, int* d_col, float* d_val);
 /* read access to the handle's CSC (device pointers, valid until destroy) */
 int spmx_get_csc(spmx_handle_t h, const int** d_csc_row, const int** d_csc_col,
                  const float** d_csc_val);
@@ -406,6 +419,40 @@ int spmx_gen_sparse_vector(int n, int k, int dist, uint64_t seed, int* key,
 /* host CSR -> CSC (stable; rows sorted within columns); val/cval may be NULL */
 int spmx_host_csr2csc(int m, int n, const int* rowptr, const int* col,
                       const float* val, int* colptr, int* row, float* cval);
+
+/* ======================= matrix files (host, no GPU) ====================== */
+/* MatrixMarket coordinate file -> COO, 0-based, in file order: the reading
+ * half of ReadMTX (INC/mtx.hpp:218-333).  "real" values are parsed as double
+ * and rounded to float, "integer" values converted, "pattern" and "complex"
+ * entries store 1 (as the reference does).  For a "symmetric" file each
+ * off-diagonal entry is followed by its mirror; "skew-symmetric" and
+ * "hermitian" files are not expanded (as in the reference).  Duplicates are
+ * kept.  row/col/val are malloc'ed (release with spmx_host_free), NULL when
+ * *nnz is 0.  info (may be NULL) receives [0] field: 0 real, 1 integer,
+ * 2 pattern, 3 complex; [1] symmetry: 0 general, 1 symmetric, 2
+ * skew-symmetric, 3 hermitian.  Malformed files (bad banner, "array" format,
+ * missing size line, an index out of range, fewer or more entries than
+ * declared) return SPMX_ERR_INVALID_VALUE naming the line. */
+int spmx_mtx_read(const char* path, int* m, int* n, long long* nnz, int** row,
+                  int** col, float** val, int* info);
+/* COO (0-based, host) -> MatrixMarket coordinate file, "real" (or "pattern"
+ * when val is NULL), banner symmetry "symmetric" when symmetric != 0 (the
+ * caller passes one triangle) else "general".  Values are written as the
+ * shortest text that reads back to the same float. */
+int spmx_mtx_write(const char* path, int m, int n, long long nnz, const int* row,
+                   const int* col, const float* val, int symmetric);
+/* The reference's binary CSR cache (INC/mtx.hpp:706-808): 9-byte magic
+ * "Hola\1CSR\1", 3 padding bytes, int32 rows, cols, nnz, then float
+ * val[nnz], int32 col[nnz], int32 rowptr[rows+1].  Host arrays.
+ * storeCSR (mtx.hpp:795-808) */
+int spmx_csr_store(const char* path, int m, int n, int nnz, const int* rowptr,
+                   const int* col, const float* val);
+/* loadCSR_header (mtx.hpp:750-772) */
+int spmx_csr_load_header(const char* path, int* m, int* n, int* nnz);
+/* loadCSR (mtx.hpp:775-793); the sizes must match the header (the reference
+ * does not check); val may be NULL to skip the values */
+int spmx_csr_load(const char* path, int m, int n, int nnz, int* rowptr,
+                  int* col, float* val);
 
 #ifdef __cplusplus
 }

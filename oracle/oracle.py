@@ -49,6 +49,8 @@ _sigs = {
     "cpu_spmspv_csc_serial": (None, [_i, _P, _P, _P, _i, _P, _P, _P]),
     "cpu_spmspv_csc_omp": (None, [_i, _P, _P, _P, _i, _P, _P, _P]),
     "cpu_threads": (_i, []),
+    "oracle_free": (None, [_P]),
+    "oracle_mtx_read": (_i, [ctypes.c_char_p, _P, _P, _P, _P, _P, _P]),
 }
 for _n, (_r, _a) in _sigs.items():
     _fn = getattr(_lib, _n)
@@ -205,3 +207,23 @@ def max_scaled_err(y32, y64, mag):
     y32 = np.asarray(y32, np.float64)
     den = np.maximum(np.maximum(np.abs(y64), mag), 1e-300)
     return float(np.max(np.abs(y32 - y64) / den)) if len(y64) else 0.0
+
+
+def mtx_read_sorted(path):
+    """ReadMTX restated: (m, n, row, col, val) sorted by (row, col), stable."""
+    m, n, nnz = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+    rp, cp, vp = ctypes.c_void_p(), ctypes.c_void_p(), ctypes.c_void_p()
+    rc = _lib.oracle_mtx_read(os.fsencode(path), ctypes.byref(m), ctypes.byref(n),
+                              ctypes.byref(nnz), ctypes.byref(rp), ctypes.byref(cp),
+                              ctypes.byref(vp))
+    if rc != 0:
+        raise ValueError(f"oracle_mtx_read({path}) = {rc}")
+    k = nnz.value
+    out = []
+    for ptr, ct, dt in ((rp, ctypes.c_int32, np.int32), (cp, ctypes.c_int32, np.int32),
+                        (vp, ctypes.c_float, np.float32)):
+        a = np.frombuffer((ct * k).from_address(ptr.value), dtype=dt).copy() if k else \
+            np.zeros(0, dt)
+        _lib.oracle_free(ptr)
+        out.append(a)
+    return (m.value, n.value, *out)

@@ -6,6 +6,8 @@
 //   serialspmv              hice-spmspv/hice/la/test/test_application.cu:107-116
 //   computeMatFeture_serial include/spmspv/csc-spmspv/spmspv.h:2275-2335
 //   extractMatFeature       include/spmspv/csc-spmspv/spmspv.h:423-447
+//   ReadMTX (+ its sort)    include/spmspv/mtx.hpp:218-361
+//   storeCSR / loadCSR_header / loadCSR   include/spmspv/mtx.hpp:750-808
 #define main spmx_reference_test_application_main
 #include REF_TEST_APPLICATION
 #undef main
@@ -27,4 +29,31 @@ extern "C" void ref_mat_features(int m, int n, int nnz, int* rowptr, float* out7
 extern "C" float ref_std_row(int m, int n, int nnz, int* rowptr) {
   SpmspvHandle<int, unsigned, float> A(m, n, nnz);
   return A.extractMatFeature(rowptr);
+}
+
+// ReadMTX exits the process on a file it cannot open: pass readable files only.
+extern "C" void ref_read_mtx(const char* path, int* m, int* n, int* nnz, int** row, int** col,
+                             float** val) {
+  MTX<float> mtx;
+  ReadMTX<float>(path, &mtx, true);
+  *m = mtx.rows; *n = mtx.cols; *nnz = mtx.nnz;
+  *row = mtx.row; *col = mtx.col; *val = mtx.data;
+}
+
+extern "C" void ref_free(void* p) { free(p); }
+
+extern "C" void ref_store_csr(const char* path, int m, int n, int nnz, int* rowptr, int* col,
+                              float* val) {
+  storeCSR<float>(m, n, nnz, rowptr, col, val, path);
+}
+
+extern "C" int ref_load_csr(const char* path, int* m, int* n, int* nnz, int* rowptr, int* col,
+                            float* val, int cap_m, int cap_nnz) {
+  try {
+    loadCSR_header(path, m, n, nnz);
+    if (*m > cap_m || *nnz > cap_nnz) return -2;
+    return loadCSR<float>(path, *m, *n, *nnz, rowptr, col, val);
+  } catch (...) {
+    return -1;
+  }
 }

@@ -16,6 +16,7 @@
  *   - setSigma (auto rule)       include/spmspv/csc-spmspv/spmspv.h:1396-1416
  *   - updateFlag/streamCompact   include/spmspv/csc-spmspv/spmspv.h:1122-1175
  *   - scatter / bitvector        spmspv.h:1226-1308, detail/device/bitvector.h
+ *   - ReadMTX + its sort         include/spmspv/mtx.hpp:218-361
  * The reference has no BFS and no adjoint; those oracles are restated from
  * their definitions (level-synchronous Boolean SpMSpV with a visited mask, in
  * the loop structure of SpmSpvCSCHost; dx = A^T dy, dvals = dy[row]*x[col]).
@@ -32,6 +33,7 @@
  */
 #include <math.h>
 #include <stdint.h>
+#include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
 #include <float.h>
@@ -416,4 +418,116 @@ EXPORT int cpu_threads(void) {
 #else
   return 1;
 #endif
+}
+
+/* ---- matrix files --------------------------------------------------------
+ * ReadMTX (include/spmspv/mtx.hpp:218-361) restated: the banner is read as
+ * whitespace tokens, the 4th naming the field and the 5th the symmetry
+ * (only "symmetric" expands; any field other than real / pattern / integer
+ * reads as complex and stores 1); comment lines are skipped up to the size
+ * line; entries are read with fscanf, "real" through double; each
+ * off-diagonal entry of a symmetric file is followed by its mirror; then the
+ * entries are sorted by (row, col).
+ * Departure: the reference's std::sort is not stable, the oracle's sort is
+ * (counting sort by column, then by row), so entries with equal (row, col)
+ * keep file order here; only their order can differ from the reference.
+ * Returns 0, or < 0 for an unreadable file.  Arrays are malloc'ed
+ * (oracle_free). */
+static void counting_sort_by(int keys_n, int nnz, const int* key, const int* a, const int* b,
+                             const float* v, int* ka, int* kb, float* kv, int* out_key) {
+  int* cnt = (int*)calloc((size_t)keys_n + 1, sizeof(int));
+  for (int i = 0; i < nnz; i++) cnt[key[i] + 1]++;
+  for (int k = 0; k < keys_n; k++) cnt[k + 1] += cnt[k];
+  for (int i = 0; i < nnz; i++) {
+    const int o = cnt[key[i]]++;
+    ka[o] = a[i];
+    kb[o] = b[i];
+    kv[o] = v[i];
+    out_key[o] = key[i];
+  }
+  free(cnt);
+}
+
+EXPORT void oracle_free(void* p) { free(p); }
+
+EXPORT int oracle_mtx_read(const char* path, int* m_out, int* n_out, int* nnz_out, int** row_out,
+                           int** col_out, float** val_out) {
+  FILE* f = fopen(path, "r");
+  if (!f) return -1;
+  char tok[128], line[1030];
+  for (int t = 0; t < 4; t++)
+    if (fscanf(f, "%127s", tok) != 1) { fclose(f); return -2; }
+  const int is_real = strcmp(tok, "real") == 0;
+  const int is_pattern = strcmp(tok, "pattern") == 0;
+  const int is_int = strcmp(tok, "integer") == 0;
+  const int is_complex = !is_real && !is_pattern && !is_int;
+  if (fscanf(f, "%127s", tok) != 1) { fclose(f); return -2; }
+  const int sym = strcmp(tok, "symmetric") == 0;
+  int height = 0, width = 0, L = 0;
+  for (;;) {
+    if (fscanf(f, "%127s", tok) != 1) { fclose(f); return -3; }
+    if (tok[0] != '%') { height = atoi(tok); break; }
+    /* rest of the comment line */
+    while (fgets(line, sizeof line, f) && !strchr(line, '\n')) {}
+  }
+  if (fscanf(f, "%d %d", &width, &L) != 2 || L < 0) { fclose(f); return -3; }
+  int* r = (int*)malloc(sizeof(int) * (size_t)(L > 0 ? L : 1));
+  int* c = (int*)malloc(sizeof(int) * (size_t)(L > 0 ? L : 1));
+  float* v = (float*)malloc(sizeof(float) * (size_t)(L > 0 ? L : 1));
+  int diag = 0;
+  for (int i = 0; i < L; i++) {
+    int ri = 0, ci = 0;
+    if (fscanf(f, "%d %d", &ri, &ci) != 2) { free(r); free(c); free(v); fclose(f); return -4; }
+    r[i] = ri - 1;
+    c[i] = ci - 1;
+    v[i] = 1.0f;
+    if (is_real) {
+      double d = 0.0;
+      if (fscanf(f, "%lf", &d) != 1) { free(r); free(c); free(v); fclose(f); return -4; }
+      v[i] = (float)d;
+    } else if (is_int) {
+      int d = 0;
+      if (fscanf(f, "%d", &d) != 1) { free(r); free(c); free(v); fclose(f); return -4; }
+      v[i] = (float)d;
+    } else if (is_complex) {
+      double a = 0.0, b = 0.0;
+      if (fscanf(f, "%lf %lf", &a, &b) != 2) { free(r); free(c); free(v); fclose(f); return -4; }
+    }
+    if (r[i] == c[i]) diag++;
+    if (r[i] < 0 || r[i] >= height || c[i] < 0 || c[i] >= width) {
+      free(r); free(c); free(v); fclose(f); return -5;
+    }
+  }
+  fclose(f);
+  int nnz = L;
+  if (sym) {
+    nnz = 2 * L - diag;
+    int* r2 = (int*)malloc(sizeof(int) * (size_t)(nnz > 0 ? nnz : 1));
+    int* c2 = (int*)malloc(sizeof(int) * (size_t)(nnz > 0 ? nnz : 1));
+    float* v2 = (float*)malloc(sizeof(float) * (size_t)(nnz > 0 ? nnz : 1));
+    int o = 0;
+    for (int i = 0; i < L; i++) {
+      r2[o] = r[i]; c2[o] = c[i]; v2[o] = v[i]; o++;
+      if (r[i] != c[i]) { r2[o] = c[i]; c2[o] = r[i]; v2[o] = v[i]; o++; }
+    }
+    free(r); free(c); free(v);
+    r = r2; c = c2; v = v2;
+  }
+  /* stable sort by (row, col): by column, then by row */
+  const size_t sz = (size_t)(nnz > 0 ? nnz : 1);
+  int* r1 = (int*)malloc(sizeof(int) * sz);
+  int* c1 = (int*)malloc(sizeof(int) * sz);
+  float* v1 = (float*)malloc(sizeof(float) * sz);
+  int* kk = (int*)malloc(sizeof(int) * sz);
+  counting_sort_by(width, nnz, c, r, c, v, r1, c1, v1, kk);
+  counting_sort_by(height, nnz, r1, c1, r1, v1, c, r, v, kk);
+  /* after the second pass: c holds columns, r holds rows (key copy in kk) */
+  free(r1); free(c1); free(v1); free(kk);
+  *m_out = height;
+  *n_out = width;
+  *nnz_out = nnz;
+  *row_out = r;
+  *col_out = c;
+  *val_out = v;
+  return 0;
 }

@@ -187,6 +187,7 @@ extern "C" int spmx_destroy(spmx_handle_t h) {
   dfree(h->ls.status); dfree(h->ls.ticket);
   if (h->h_pinned) cudaFreeHost(h->h_pinned);
   dfree(h->own_colptr); dfree(h->own_row); dfree(h->own_cval);
+  dfree(h->own_csr_rowptr); dfree(h->own_csr_col); dfree(h->own_csr_val);
   dfree(h->own_xdense); dfree(h->own_bits);
   free_csc_scratch(h);
   free_sort_scratch(h);

@@ -16,11 +16,14 @@ struct spmx_handle_s {
   int num_sms = 148;
   cudaStream_t stream = nullptr;
 
-  // CSR (borrowed)
+  // CSR (borrowed via input_csr, or owned after input_coo)
   const int* rowptr = nullptr;
   const int* col = nullptr;
   const float* val = nullptr;
   bool has_csr = false;
+  int* own_csr_rowptr = nullptr;
+  int* own_csr_col = nullptr;
+  float* own_csr_val = nullptr;
   // CSC (borrowed via input_csc or owned via to_csc)
   const int* csc_colptr = nullptr;
   const int* csc_row = nullptr;

@@ -65,6 +65,8 @@ _SIGS = {
     "spmx_to_csc": (c_int, [P]),
     "spmx_get_csc": (c_int, [P, PP, PP, PP]),
     "spmx_copy_csc": (c_int, [P, P, P, P]),
+    "spmx_input_coo": (c_int, [P, c_int, P, P, P]),
+    "spmx_copy_csr": (c_int, [P, P, P, P]),
     "spmx_set_x": (c_int, [P, P]),
     "spmx_set_sparse_x": (c_int, [P, P, P, c_int]),
     "spmx_set_bitvector": (c_int, [P, P, c_int]),
@@ -138,6 +140,11 @@ _SIGS = {
     "spmx_gen_laplacian": (c_int, [c_int, c_double, c_u64, PLL, PP, PP, PP]),
     "spmx_gen_sparse_vector": (c_int, [c_int, c_int, c_int, c_u64, P, P]),
     "spmx_host_csr2csc": (c_int, [c_int, c_int, P, P, P, P, P, P]),
+    "spmx_mtx_read": (c_int, [ctypes.c_char_p, PI, PI, PLL, PP, PP, PP, PI]),
+    "spmx_mtx_write": (c_int, [ctypes.c_char_p, c_int, c_int, c_ll, P, P, P, c_int]),
+    "spmx_csr_store": (c_int, [ctypes.c_char_p, c_int, c_int, c_int, P, P, P]),
+    "spmx_csr_load_header": (c_int, [ctypes.c_char_p, PI, PI, PI]),
+    "spmx_csr_load": (c_int, [ctypes.c_char_p, c_int, c_int, c_int, P, P, P]),
 }
 
 # optional entry points (present once their components are built)

@@ -96,6 +96,23 @@ class SpmspvHandle:
               "InputCSC")
         self._keep["csc"] = (csc_row, csc_col, csc_val)
 
+    def InputCOO(self, nnz, row, col, val=None):
+        """COO device arrays (any order) -> handle-owned CSR sorted by (row, col).
+        Synchronous; the inputs are not kept."""
+        check(lib.spmx_input_coo(self._h, int(nnz), _i32(row), _i32(col), _f32(val)), "InputCOO")
+        self._keep.pop("csr", None)
+
+    def get_csr(self):
+        """(rowptr[m+1], col[nnz], val[nnz]) copied into new tensors (val is
+        left unwritten for a pattern-only matrix)."""
+        rowptr = torch.empty(self.m + 1, dtype=torch.int32, device="cuda")
+        col = torch.empty(self.nnz, dtype=torch.int32, device="cuda")
+        val = torch.empty(self.nnz, dtype=torch.float32, device="cuda")
+        check(lib.spmx_copy_csr(self._h, _ptr(rowptr), _ptr(col) if self.nnz else None,
+                                _ptr(val) if self.nnz else None), "copy_csr")
+        self._stream.synchronize()
+        return rowptr, col, val
+
     def ToCSC(self):
         check(lib.spmx_to_csc(self._h), "ToCSC")
 
