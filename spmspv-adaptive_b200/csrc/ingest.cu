@@ -103,44 +103,58 @@ extern "C" int spmx_input_coo(spmx_handle_t h, int nnz, const int* row, const in
   }
   if (oob) return set_error(SPMX_ERR_INVALID_VALUE, "COO index out of range");
 
-  // 2. the new CSR (swapped in only on success)
+  // 2. the new CSR (swapped in only on success).  The radix passes alternate
+  // between two buffer sets; the pass count is known here, so the set the
+  // last pass writes is the new CSR's column / value arrays themselves.  All
+  // other scratch is one allocation.
   int *nrp = nullptr, *ncol = nullptr;
   float* nval = nullptr;
   int rc = SPMX_SUCCESS;
   rc = rc ? rc : dalloc((void**)&nrp, 4 * ((size_t)m + 1), "csr rowptr");
   rc = rc ? rc : dalloc((void**)&ncol, b, "csr col");
   if (val) rc = rc ? rc : dalloc((void**)&nval, b, "csr val");
-  unsigned *k[2] = {nullptr, nullptr}, *r[2] = {nullptr, nullptr}, *v[2] = {nullptr, nullptr};
-  int *hist = nullptr, *hoff = nullptr;
+  char* scratch = nullptr;
   const int* rows_sorted = row;
   const void* cols_sorted = col;
   const void* vals_sorted = val;
   if (!rc && unsorted) {
+    const int bits_c = key_bits(n), bits_r = key_bits(m);
+    const int passes = (col_desc ? (bits_c + 7) / 8 : 0) + (bits_r + 7) / 8;
+    const int fin = passes & 1;  // set holding the result after the last pass
     const size_t hn = radix_hist_ints(nnz);
-    for (int s = 0; s < 2; ++s) {
-      rc = rc ? rc : dalloc((void**)&k[s], b, "coo col keys");
-      rc = rc ? rc : dalloc((void**)&r[s], b, "coo rows");
-      if (val) rc = rc ? rc : dalloc((void**)&v[s], b, "coo vals");
-    }
-    rc = rc ? rc : dalloc((void**)&hist, 4 * hn, "coo hist");
-    rc = rc ? rc : dalloc((void**)&hoff, 4 * hn, "coo hist off");
+    const size_t al = (b + 255) & ~(size_t)255;
+    const size_t hb = (4 * hn + 255) & ~(size_t)255;
+    rc = dalloc((void**)&scratch, al * (val ? 4 : 3) + 2 * hb, "coo sort scratch");
     if (!rc) {
+      unsigned *k[2], *r[2], *v[2] = {nullptr, nullptr};
+      char* q = scratch;
+      k[fin] = (unsigned*)ncol;
+      k[1 - fin] = (unsigned*)q; q += al;
+      r[0] = (unsigned*)q; q += al;
+      r[1] = (unsigned*)q; q += al;
+      if (val) {
+        v[fin] = (unsigned*)nval;
+        v[1 - fin] = (unsigned*)q; q += al;
+      }
+      int* hist = (int*)q; q += hb;
+      int* hoff = (int*)q;
       cudaMemcpyAsync(k[0], col, 4 * (size_t)nnz, cudaMemcpyDeviceToDevice, st);
       cudaMemcpyAsync(r[0], row, 4 * (size_t)nnz, cudaMemcpyDeviceToDevice, st);
       if (val) cudaMemcpyAsync(v[0], val, 4 * (size_t)nnz, cudaMemcpyDeviceToDevice, st);
       int s = 0;  // set holding the current order
       if (col_desc) {
         RadixBuffers ra{k[s], k[1 - s], r[s], r[1 - s], v[s], v[1 - s], hist, hoff, false};
-        if (radix_sort_pairs(ra, nnz, key_bits(n), h->ls, h->d_err, st))
+        if (radix_sort_pairs(ra, nnz, bits_c, h->ls, h->d_err, st))
           rc = set_error(SPMX_ERR_INVALID_VALUE, "radix capacity");
         if (ra.result_in_alt) s = 1 - s;
       }
       if (!rc) {
         RadixBuffers rb{r[s], r[1 - s], k[s], k[1 - s], v[s], v[1 - s], hist, hoff, false};
-        if (radix_sort_pairs(rb, nnz, key_bits(m), h->ls, h->d_err, st))
+        if (radix_sort_pairs(rb, nnz, bits_r, h->ls, h->d_err, st))
           rc = set_error(SPMX_ERR_INVALID_VALUE, "radix capacity");
         if (rb.result_in_alt) s = 1 - s;
       }
+      if (!rc && s != fin) rc = set_error(SPMX_ERR_INVALID_VALUE, "radix pass count");
       rows_sorted = (const int*)r[s];
       cols_sorted = k[s];
       vals_sorted = v[s];
@@ -150,7 +164,7 @@ extern "C" int spmx_input_coo(spmx_handle_t h, int nnz, const int* row, const in
   if (!rc) {
     note_launch();
     coo_rowptr_kernel<<<ingest_grid((long long)nnz + 1), kIngestNT, 0, st>>>(nnz, m, rows_sorted, nrp);
-    if (nnz > 0) {
+    if (nnz > 0 && cols_sorted != ncol) {
       cudaMemcpyAsync(ncol, cols_sorted, 4 * (size_t)nnz, cudaMemcpyDeviceToDevice, st);
       if (val) cudaMemcpyAsync(nval, vals_sorted, 4 * (size_t)nnz, cudaMemcpyDeviceToDevice, st);
     }
@@ -160,13 +174,7 @@ extern "C" int spmx_input_coo(spmx_handle_t h, int nnz, const int* row, const in
   } else {
     cudaStreamSynchronize(st);
   }
-  for (int s = 0; s < 2; ++s) {
-    dfree(k[s]);
-    dfree(r[s]);
-    dfree(v[s]);
-  }
-  dfree(hist);
-  dfree(hoff);
+  dfree(scratch);
   if (rc) {
     dfree(nrp);
     dfree(ncol);

@@ -13,9 +13,16 @@ differences:
     (`collect`), the split and the fit run on the host (`fit`).
 
 usage:
-  python -m spmx.selector_train collect OUT.jsonl      (GPU)
-  python -m spmx.selector_train fit DATA.jsonl OUT.inc  (host, scikit-learn)
-  python -m spmx.selector_train compare DATA.jsonl      (host: other learners)
+  python -m spmx.selector_train collect OUT.jsonl [A.mtx ...]   (GPU)
+  python -m spmx.selector_train features OUT.jsonl A.mtx ...    (GPU)
+  python -m spmx.selector_train fit DATA.jsonl OUT.inc          (host, scikit-learn)
+  python -m spmx.selector_train compare DATA.jsonl              (host: other learners)
+
+`collect` times all eight kernels on the synthetic spread below, or on the
+given MatrixMarket files (the reference's generate_model_data.cu:563-860 does
+the same over its matrix list).  `features` writes one JSON line of matrix
+features per file (generate_feature.cu:209-290 writes the same fields as a
+text line).
 """
 import json
 import math
@@ -46,7 +53,36 @@ def matrices():
     yield "laplacian-2048", gen.laplacian(2048, 0.01, seed=4)
 
 
-def collect(out_path, reps=7):
+def mtx_matrices(paths):
+    """(name, Csr) pairs read from MatrixMarket files: host parse, GPU sort."""
+    import os
+    from . import io
+    from .gen import Csr
+    for p in paths:
+        h = io.load_mtx(p)
+        rp, cl, vl = (t.cpu().numpy() for t in h.get_csr())
+        h.Destroy()
+        yield os.path.basename(p), Csr(h.m, h.n, rp, cl, vl)
+
+
+MAT_FEATURES = ("m", "n", "nnz", "maxRow", "minRow", "avgRow", "range", "stdRow",
+                "edge_equlity", "gini_coefficiency")
+
+
+def dump_features(out_path, paths):
+    """One JSON line of matrix features per MatrixMarket file."""
+    import os
+    from . import io
+    with open(out_path, "w") as out:
+        for p in paths:
+            h = io.load_mtx(p)
+            f = dict(zip(MAT_FEATURES, h.computeMatFeture()))
+            h.Destroy()
+            out.write(json.dumps({"matrix": os.path.basename(p), **f}) + "\n")
+            out.flush()
+
+
+def collect(out_path, reps=7, paths=None):
     import torch
     from .handle import SpmspvHandle
     from . import gen
@@ -55,9 +91,10 @@ def collect(out_path, reps=7):
     flush = torch.empty(64 << 20, device=dev)
     s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     with open(out_path, "w") as out:
-        for name, A in matrices():
+        for name, A in (mtx_matrices(paths) if paths else matrices()):
             t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)  # noqa: E731
-            rp, cl, vl = t(A.rowptr), t(A.col), t(A.val)
+            vals = A.val if A.val is not None else np.ones(A.nnz, np.float32)
+            rp, cl, vl = t(A.rowptr), t(A.col), t(vals)
             h = SpmspvHandle(A.m, A.n, A.nnz, stream=stream)
             h.InputCSR(A.nnz, rp, cl, vl)
             h.ToCSC()
@@ -280,7 +317,9 @@ def export_cpp(tree, stats):
 
 def main(argv):
     if len(argv) >= 2 and argv[0] == "collect":
-        collect(argv[1])
+        collect(argv[1], paths=argv[2:] or None)
+    elif len(argv) >= 3 and argv[0] == "features":
+        dump_features(argv[1], argv[2:])
     elif len(argv) >= 3 and argv[0] == "fit":
         fit(argv[1], argv[2])
     elif len(argv) >= 2 and argv[0] == "compare":

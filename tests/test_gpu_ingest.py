@@ -183,3 +183,32 @@ def test_load_mtx_then_kernels(torch_cuda, tmp_path):
     z64, zmag, _ = orc.spmspv_csc_f64(m, colptr, orow[t], oval[t], key, xv)
     assert orc.within_tol(z.cpu().numpy(), z64, zmag, RTOL)[0]
     h.check_device_error()
+
+
+def test_feature_dump_and_collect_from_files(torch_cuda, tmp_path):
+    """The training-data tools on MatrixMarket files: the feature dump matches
+    the oracle's matrix features, and collect writes one timed record per
+    density with a valid best kernel."""
+    import json
+    from spmx import gen, io, selector_train
+    A = gen.zipf_rows(1 << 14, 1.5, 16, 2000, seed=31)
+    p = str(tmp_path / "z.mtx")
+    io.write_mtx(p, A)
+    out = str(tmp_path / "f.jsonl")
+    selector_train.dump_features(out, [p])
+    rec = json.loads(open(out).read().splitlines()[0])
+    want = orc.mat_features(A.n, A.rowptr)
+    got = [rec[k] for k in selector_train.MAT_FEATURES]
+    assert rec["matrix"] == "z.mtx" and rec["nnz"] == A.nnz and rec["m"] == A.m
+    assert np.allclose(got, want, rtol=1e-9, atol=1e-12)
+    data = str(tmp_path / "c.jsonl")
+    old = selector_train.DENSITIES
+    selector_train.DENSITIES = [1e-3, 1.0]
+    try:
+        selector_train.collect(data, reps=2, paths=[p])
+    finally:
+        selector_train.DENSITIES = old
+    recs = [json.loads(ln) for ln in open(data)]
+    assert [r["density"] for r in recs] == [1e-3, 1.0]
+    for r in recs:
+        assert len(r["us"]) == 8 and r["best"] == int(np.argmin(r["us"])) and min(r["us"]) > 0
