@@ -598,9 +598,11 @@ def run_batched_spmspv(torch, dev, stream, args):
 def run_adjoint(torch, dev, stream, args):
     """Differentiable SpMV: the 5-point Laplacian on a 2048 x 2048 grid
     (4,194,304 rows, off-diagonals -1 + N(0, 0.01^2), seed 4), x and dy
-    N(0,1).  Forward = the autotuned load-balanced SpMV; backward = dx = A^T dy
-    and dvals on the pattern in one pass (dense dy), and the same for dy masked
-    to 1 % of the rows (sparse dy).  L2 flushed before every timed call."""
+    N(0,1).  Forward = the faster of the autotuned load-balanced SpMV and the
+    naive CSR kernel; backward with dense dy = dx = A^T dy as a gather over
+    the handle's CSC plus dvals on the pattern over the CSR (no atomics), and
+    with dy masked to 1 % of the rows (sparse dy).  L2 flushed before every
+    timed call."""
     import spmx
     from spmx import gen
     A = gen.laplacian(2048, 0.01, seed=4)
@@ -608,6 +610,7 @@ def run_adjoint(torch, dev, stream, args):
     t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)  # noqa: E731
     h = spmx.SpmspvHandle(m, n, A.nnz, stream=stream)
     h.InputCSR(A.nnz, t(A.rowptr), t(A.col), t(A.val))
+    h.ToCSC()
     h.holaPreprocess()
     backend = SPMV_BACKENDS.get(h.autotune(), "?")
     rng = np.random.default_rng(4)
@@ -647,7 +650,8 @@ def run_adjoint(torch, dev, stream, args):
     h.check_device_error()
     h.Destroy()
     fb = spmv_bytes(m, n, A.nnz)
-    bb = 4 * (m + 1) + 8 * A.nnz + 4 * m + 4 * n + 4 * A.nnz + 4 * n  # CSR, dy, x, dvals, dx
+    # dx pass: colptr, CSC rows + values, dy, dx; dvals pass: rowptr, columns, x, dy, dvals
+    bb = (4 * (n + 1) + 8 * A.nnz + 4 * m + 4 * n) + (4 * (m + 1) + 4 * A.nnz + 4 * n + 4 * m + 4 * A.nnz)
     return {"matrix": "5-point Laplacian 2048^2, nnz %d, off-diagonals -1 + N(0, 0.01^2)" % A.nnz,
             "forward_backend": backend, "forward_ms": f_ms, "backward_dense_dy_ms": b_ms,
             "backward_sparse_dy_1pct_ms": s_ms, "backward_over_forward": b_ms / f_ms,

@@ -352,8 +352,11 @@ int spmx_bfs_batched(spmx_handle_t h, const int* srcs, int nsrc, int* d_levels,
 /* ======================= adjoint (FP32) ==================================== */
 /* No reference counterpart (the reference has no differentiation).  For
  * y = A x and an upstream gradient dy[m]: dx[n] = A^T dy and dvals[nnz] =
- * dy[row_k] * x[col_k] on the CSR pattern, in one pass over the matrix.
- * Either output may be NULL.  Uses the Hola chunk table (built on demand). */
+ * dy[row_k] * x[col_k] on the CSR pattern.  Either output may be NULL.
+ * With a CSC on the handle (spmx_to_csc / spmx_input_csc, with values), dx is
+ * a gather over the CSC and dvals a pass over the CSR: no atomics,
+ * deterministic.  Without one, both come from one pass over the CSR with
+ * atomic adds into dx (Hola chunk table, built on demand). */
 int spmx_spmv_backward(spmx_handle_t h, const float* d_x, const float* d_dy,
                        float* d_dx, float* d_dvals);
 /* the same with a sparse dy (keys = rows); dvals is zero outside dy's rows */

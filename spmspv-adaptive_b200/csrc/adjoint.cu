@@ -3,15 +3,20 @@
 //   dx    = A^T dy                  (the transpose product)
 //   dvals = dy[row_k] * x[col_k]    (the gradient on the nonzero pattern)
 //
-// dense dy: ONE pass over the CSR, fixed 2048 nonzeros per CTA (the Hola
-//   chunks): every nonzero writes its dvals entry and adds val*dy[row] into
-//   dx[col] with an FP32 atomic, so the matrix is streamed once for both
-//   gradients.  The row of each nonzero comes from a max-scan of row-start
-//   marks in shared memory (no per-element search).
+// dense dy, handle with a CSC: dx is the row-ordered SpMV of the transpose
+//   (the CSC read as the CSR of A^T, dy as its x: a gather, no atomics) and
+//   dvals a streaming pass over the CSR.  Both are deterministic.
+// dense dy, CSR only: ONE pass over the CSR, fixed 2048 nonzeros per CTA
+//   (the Hola chunks): every nonzero writes its dvals entry and adds
+//   val*dy[row] into dx[col] with an FP32 atomic, so the matrix is streamed
+//   once for both gradients.  The row of each nonzero comes from a max-scan
+//   of row-start marks in shared memory (no per-element search).
 // sparse dy (dy_key, dy_val): only the rows in dy's support contribute, so a
 //   group of lanes per dy entry walks that row (the CSR of A is the CSC of
 //   A^T: this is the CSC SpMSpV of the transpose) after dx and dvals are
 //   zeroed.
+#include <algorithm>
+
 #include "common.cuh"
 #include "kernels.h"
 
@@ -77,6 +82,57 @@ spmv_backward_kernel(int m, int n, int nnz, const int* __restrict__ rowptr,
   }
 }
 
+// Dense-dy adjoint on a handle with a CSC, one launch: even CTAs compute dx
+// (G1 lanes per column of the CSC, a gather of dy with FP64 sums, every dx
+// entry written once), odd CTAs write dvals (G2 lanes per row of the CSR).
+// The two halves stream different arrays side by side; neither uses atomics.
+template <int G1, int G2>
+__global__ void __launch_bounds__(256)
+adjoint_csc_kernel(int m, int n, const int* __restrict__ rowptr, const int* __restrict__ col,
+                   const int* __restrict__ colptr, const int* __restrict__ crow,
+                   const float* __restrict__ cval, const float* __restrict__ x,
+                   const float* __restrict__ dy, float* __restrict__ dx,
+                   float* __restrict__ dvals, int* err) {
+  const long long gid = (long long)(blockIdx.x >> 1) * blockDim.x + threadIdx.x;
+  if ((blockIdx.x & 1) == 0) {
+    if (!dx || gid / G1 >= ((long long)n + 31) / 32 * 32) return;  // whole warps past the end
+    const long long j = gid / G1;
+    const int g = (int)(gid % G1);
+    double sum = 0.0;
+    if (j < n) {
+      const int a = __ldg(colptr + j), b = __ldg(colptr + j + 1);
+      for (int k = a + g; k < b; k += G1) {
+        const int r = __ldg(crow + k);
+        if ((unsigned)r >= (unsigned)m) {
+          flag_error(err, kDevErrOob);
+          continue;
+        }
+        sum += (double)__ldg(cval + k) * (double)__ldg(dy + r);
+      }
+    }
+    if (G1 > 1) {
+#pragma unroll
+      for (int o = G1 / 2; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o, G1);
+    }
+    if (j < n && g == 0) dx[j] = (float)sum;
+  } else {
+    const long long row = gid / G2;
+    if (!dvals || row >= m) return;
+    const int g = (int)(gid % G2);
+    const float d = __ldg(dy + row);
+    const int a = __ldg(rowptr + row), b = __ldg(rowptr + row + 1);
+    for (int k = a + g; k < b; k += G2) {
+      const int c = __ldg(col + k);
+      if ((unsigned)c >= (unsigned)n) {
+        flag_error(err, kDevErrOob);
+        dvals[k] = 0.f;
+        continue;
+      }
+      dvals[k] = d * __ldg(x + c);
+    }
+  }
+}
+
 template <int G>
 __global__ void __launch_bounds__(256)
 spmv_backward_sparse_kernel(int m, int n, const int* __restrict__ rowptr,
@@ -108,6 +164,38 @@ int launch_spmv_backward(int m, int n, int nnz, const int* rowptr, const int* co
   note_launch();
   spmv_backward_kernel<256, 8><<<t.nchunks, 256, 0, st>>>(m, n, nnz, rowptr, col, val, x, dy,
                                                           t.chunk_row, dx, dvals, err);
+  return 0;
+}
+
+template <int G1>
+static void adjoint_csc_g2(int g2, unsigned grid, cudaStream_t st, int m, int n, const int* rowptr,
+                           const int* col, const int* colptr, const int* crow, const float* cval,
+                           const float* x, const float* dy, float* dx, float* dvals, int* err) {
+  switch (g2) {
+    case 1: adjoint_csc_kernel<G1, 1><<<grid, 256, 0, st>>>(m, n, rowptr, col, colptr, crow, cval, x, dy, dx, dvals, err); break;
+    case 2: adjoint_csc_kernel<G1, 2><<<grid, 256, 0, st>>>(m, n, rowptr, col, colptr, crow, cval, x, dy, dx, dvals, err); break;
+    case 4: adjoint_csc_kernel<G1, 4><<<grid, 256, 0, st>>>(m, n, rowptr, col, colptr, crow, cval, x, dy, dx, dvals, err); break;
+    default: adjoint_csc_kernel<G1, 8><<<grid, 256, 0, st>>>(m, n, rowptr, col, colptr, crow, cval, x, dy, dx, dvals, err); break;
+  }
+}
+
+int launch_spmv_backward_csc(int m, int n, const int* rowptr, const int* col, const int* colptr,
+                             const int* crow, const float* cval, const float* x, const float* dy,
+                             int g1, int g2, float* dx, float* dvals, int* err, cudaStream_t st) {
+  if ((!dx || n <= 0) && (!dvals || m <= 0)) return 0;
+  const long long t1 = dx ? ((long long)n + 31) / 32 * 32 * g1 : 0;
+  const long long t2 = dvals ? (long long)m * g2 : 0;
+  const long long half = (std::max(t1, t2) + 255) / 256;
+  const unsigned grid = (unsigned)(2 * half);
+  note_launch();
+  switch (g1) {
+    case 1: adjoint_csc_g2<1>(g2, grid, st, m, n, rowptr, col, colptr, crow, cval, x, dy, dx, dvals, err); break;
+    case 2: adjoint_csc_g2<2>(g2, grid, st, m, n, rowptr, col, colptr, crow, cval, x, dy, dx, dvals, err); break;
+    case 4: adjoint_csc_g2<4>(g2, grid, st, m, n, rowptr, col, colptr, crow, cval, x, dy, dx, dvals, err); break;
+    case 8: adjoint_csc_g2<8>(g2, grid, st, m, n, rowptr, col, colptr, crow, cval, x, dy, dx, dvals, err); break;
+    case 16: adjoint_csc_g2<16>(g2, grid, st, m, n, rowptr, col, colptr, crow, cval, x, dy, dx, dvals, err); break;
+    default: adjoint_csc_g2<32>(g2, grid, st, m, n, rowptr, col, colptr, crow, cval, x, dy, dx, dvals, err); break;
+  }
   return 0;
 }
 

@@ -93,6 +93,13 @@ static int pow2_group(double mean) {
   return g;
 }
 
+// lanes per row for short-row streaming passes: about 4 nonzeros per lane
+static int stream_group(double mean) {
+  int g = 1;
+  while (g < 32 && 8.0 * g <= mean) g <<= 1;
+  return g;
+}
+
 static int ceil_log2(long long v) {
   int b = 0;
   while ((1LL << b) < v) ++b;
@@ -683,6 +690,15 @@ extern "C" int spmx_spmv_backward(spmx_handle_t h, const float* x, const float* 
   if (!h->has_csr || (!h->val && h->nnz > 0))
     return set_error(SPMX_ERR_NOT_READY, "backward needs the CSR input with values");
   if (!dy || (dvals && !x)) return set_error(SPMX_ERR_INVALID_VALUE, "NULL x / dy");
+  if (h->has_csc && (h->csc_val || h->nnz == 0)) {
+    // dx = A^T dy as a gather over the CSC and dvals over the CSR, one launch
+    const int g1 = h->naive_row_group > 0 ? h->naive_row_group
+                                          : stream_group(h->n ? (double)h->nnz / h->n : 1.0);
+    const int g2 = std::min(8, stream_group(h->m ? (double)h->nnz / h->m : 1.0));
+    launch_spmv_backward_csc(h->m, h->n, h->rowptr, h->col, h->csc_colptr, h->csc_row, h->csc_val, x, dy, g1,
+                             g2, dx, h->nnz > 0 ? dvals : nullptr, h->d_err, h->stream);
+    return launch_ok("spmv backward");
+  }
   if (!h->hola_ready || h->hola.K != 2048) {
     const int vt = h->hola_vt;
     h->hola_vt = 8;

@@ -42,6 +42,9 @@ int launch_spmv_backward(int m, int n, int nnz, const int* rowptr, const int* co
                          const float* val, const float* x, const float* dy,
                          const HolaTables& t, float* dx, float* dvals, int* err,
                          cudaStream_t st);
+int launch_spmv_backward_csc(int m, int n, const int* rowptr, const int* col, const int* colptr,
+                             const int* crow, const float* cval, const float* x, const float* dy,
+                             int g1, int g2, float* dx, float* dvals, int* err, cudaStream_t st);
 int launch_spmv_backward_sparse(int m, int n, const int* rowptr, const int* col,
                                 const float* val, const float* x, int dy_nnz,
                                 const int* dy_key, const float* dy_val, int group,

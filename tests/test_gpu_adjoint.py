@@ -14,13 +14,16 @@ pytestmark = pytest.mark.gpu
 RTOL = 1e-5
 
 
+@pytest.mark.parametrize("csc", [False, True])
 @pytest.mark.parametrize("kind", ["zipf", "laplacian"])
-def test_backward_dense_and_sparse_dy(torch_cuda, kind):
+def test_backward_dense_and_sparse_dy(torch_cuda, kind, csc):
+    """Dense dy goes through the one-pass atomic kernel without a CSC and
+    through the CSC gather + CSR dvals pass with one."""
     torch = torch_cuda
     from spmx import gen
     A = rand_csr(5000, 4000, lens=np.minimum(np.random.default_rng(1).zipf(1.6, 5000), 3000),
                  seed=2) if kind == "zipf" else gen.laplacian(64, 0.01, seed=4)
-    h = make_handle(A, torch, csc=False)
+    h = make_handle(A, torch, csc=csc)
     rng = np.random.default_rng(7)
     x = rng.normal(size=A.n).astype(np.float32)
     dy = rng.normal(size=A.m).astype(np.float32)
@@ -104,3 +107,24 @@ def test_autograd_laplacian_fd_and_dense(torch_cuda, g, masked):
         fd = (loss_rows(np.array([r0]), np.array([yy[r0] + d])) -
               loss_rows(np.array([r0]), np.array([yy[r0] - d]))) / (2 * h)
         assert abs(fd - gv[k]) <= 2 * tol_v[k] + 1e-6, (k, fd, gv[k])
+
+
+def test_backward_with_csc_is_deterministic(torch_cuda):
+    """With a CSC the dense-dy backward has no atomics: repeated calls are
+    bit-identical, and an empty column gives dx exactly 0."""
+    torch = torch_cuda
+    A = rand_csr(3000, 2500, lens=np.minimum(np.random.default_rng(3).zipf(1.5, 3000), 2000), seed=4)
+    A.col[A.col == 7] = 8  # column 7 empty (duplicates are allowed)
+    h = make_handle(A, torch, csc=True)
+    rng = np.random.default_rng(9)
+    x = dev(rng.normal(size=A.n).astype(np.float32), torch)
+    dy = dev(rng.normal(size=A.m).astype(np.float32), torch)
+    outs = []
+    for _ in range(2):
+        dx = torch.full((A.n,), 5.0, device="cuda")
+        dv = torch.full((A.nnz,), 5.0, device="cuda")
+        h.spmv_backward(x, dy, dx, dv)
+        outs.append((dx.cpu().numpy(), dv.cpu().numpy()))
+    h.check_device_error()
+    assert np.array_equal(outs[0][0], outs[1][0]) and np.array_equal(outs[0][1], outs[1][1])
+    assert outs[0][0][7] == 0.0
