@@ -205,6 +205,23 @@ int spmx_tiled_postprocess(spmx_handle_t h);
 int spmx_tiled_info(spmx_handle_t h, int* info);
 int spmx_tiledspmv(spmx_handle_t h, float alpha, float* d_y);
 int spmx_tiledspmspv(spmx_handle_t h, float alpha, float* d_y);
+/* Hybrid CSR/CSC split (a candidate ninth kernel; the reference's
+ * COO2Hybrid, INC/mtx.hpp:436-701, driven by TEST/test_coo2hybrid.cu:276-312).
+ * Preprocess: copies the CSR to the host and visits the nonzeros in (row,
+ * column) order with the current row and column counts: a nonzero joins the
+ * CSR part when count_row >= count_col (count_col is then decremented), else
+ * the CSC part (count_row decremented).  Row priority only (the reference's
+ * column-priority branch swaps its row and column indices).  hybridspmv:
+ * y = alpha * (A_csr x + A_csc x), the CSC part added with FP32 atomics. */
+int spmx_hybrid_preprocess(spmx_handle_t h);
+int spmx_hybrid_postprocess(spmx_handle_t h);
+/* nonzeros in the CSR and CSC parts */
+int spmx_hybrid_info(spmx_handle_t h, int* csr_nnz, int* csc_nnz);
+/* copy the parts into caller buffers (CSR: rowptr[m+1], col, val; CSC:
+ * colptr[n+1], row, cval; any may be NULL); asynchronous on the stream */
+int spmx_hybrid_copy(spmx_handle_t h, int* d_rowptr, int* d_col, float* d_val, int* d_colptr,
+                     int* d_row, float* d_cval);
+int spmx_hybridspmv(spmx_handle_t h, float alpha, float* d_y);
 /* set_spmv_type — H:1767 (0 Hola, 1 CSR5, 2 tiled) */
 int spmx_set_spmv_type(spmx_handle_t h, int code);
 

@@ -50,6 +50,7 @@ _sigs = {
     "cpu_spmspv_csc_omp": (None, [_i, _P, _P, _P, _i, _P, _P, _P]),
     "cpu_threads": (_i, []),
     "oracle_free": (None, [_P]),
+    "oracle_coo2hybrid": (_i, [_i, _i, _P, _P, _P]),
     "oracle_mtx_read": (_i, [ctypes.c_char_p, _P, _P, _P, _P, _P, _P]),
 }
 for _n, (_r, _a) in _sigs.items():
@@ -227,3 +228,11 @@ def mtx_read_sorted(path):
         _lib.oracle_free(ptr)
         out.append(a)
     return (m.value, n.value, *out)
+
+
+def coo2hybrid(n, rowptr, col):
+    """COO2Hybrid (row priority) restated: (csr_nnz, to_csr flags in CSR order)."""
+    rowptr, col = _a(rowptr, np.int32), _a(col, np.int32)
+    flags = np.zeros(max(len(col), 1), np.uint8)
+    k = _lib.oracle_coo2hybrid(len(rowptr) - 1, n, _p(rowptr), _p(col), _p(flags))
+    return k, flags[:len(col)].astype(bool)

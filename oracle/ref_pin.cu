@@ -8,6 +8,7 @@
 //   extractMatFeature       include/spmspv/csc-spmspv/spmspv.h:423-447
 //   ReadMTX (+ its sort)    include/spmspv/mtx.hpp:218-361
 //   storeCSR / loadCSR_header / loadCSR   include/spmspv/mtx.hpp:750-808
+//   COO2Hybrid              include/spmspv/mtx.hpp:436-701
 #define main spmx_reference_test_application_main
 #include REF_TEST_APPLICATION
 #undef main
@@ -56,4 +57,11 @@ extern "C" int ref_load_csr(const char* path, int* m, int* n, int* nnz, int* row
   } catch (...) {
     return -1;
   }
+}
+
+// COO2Hybrid sizes its count arrays by nnz: pass nnz >= max(rows, cols).
+// On return the first *csr_nnz entries are the CSR part, sorted by (row,
+// column), the rest the CSC part, sorted by (column, row).
+extern "C" void ref_coo2hybrid(int m, int n, int nnz, int* row, int* col, float* val, int* csr_nnz) {
+  COO2Hybrid<float>(1, m, n, nnz, row, col, val, csr_nnz);
 }

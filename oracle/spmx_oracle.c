@@ -17,6 +17,7 @@
  *   - updateFlag/streamCompact   include/spmspv/csc-spmspv/spmspv.h:1122-1175
  *   - scatter / bitvector        spmspv.h:1226-1308, detail/device/bitvector.h
  *   - ReadMTX + its sort         include/spmspv/mtx.hpp:218-361
+ *   - COO2Hybrid (row priority)  include/spmspv/mtx.hpp:436-701
  * The reference has no BFS and no adjoint; those oracles are restated from
  * their definitions (level-synchronous Boolean SpMSpV with a visited mask, in
  * the loop structure of SpmSpvCSCHost; dx = A^T dy, dvals = dy[row]*x[col]).
@@ -530,4 +531,33 @@ EXPORT int oracle_mtx_read(const char* path, int* m_out, int* n_out, int* nnz_ou
   *col_out = c;
   *val_out = v;
   return 0;
+}
+
+/* COO2Hybrid with row priority (include/spmspv/mtx.hpp:436-701, the branch
+ * test/test_coo2hybrid.cu:276 uses), restated over a CSR: nonzeros visited in
+ * (row, column) order with running row and column counts; to_csr[k] = 1 when
+ * count_row[r] >= count_col[c] (then count_col[c]--), else 0 (count_row[r]--).
+ * Returns the number of CSR-part nonzeros.  The reference sizes its count
+ * arrays by nnz; here they are sized by m and n. */
+EXPORT int oracle_coo2hybrid(int m, int n, const int* rowptr, const int* col, unsigned char* to_csr) {
+  int* cr = (int*)malloc(sizeof(int) * (size_t)(m > 0 ? m : 1));
+  int* cc = (int*)calloc((size_t)(n > 0 ? n : 1), sizeof(int));
+  for (int r = 0; r < m; r++) cr[r] = rowptr[r + 1] - rowptr[r];
+  for (int k = 0; k < rowptr[m]; k++) cc[col[k]]++;
+  int csr = 0;
+  for (int r = 0; r < m; r++)
+    for (int k = rowptr[r]; k < rowptr[r + 1]; k++) {
+      const int c = col[k];
+      if (cr[r] >= cc[c]) {
+        to_csr[k] = 1;
+        csr++;
+        cc[c]--;
+      } else {
+        to_csr[k] = 0;
+        cr[r]--;
+      }
+    }
+  free(cr);
+  free(cc);
+  return csr;
 }

@@ -201,6 +201,7 @@ extern "C" int spmx_destroy(spmx_handle_t h) {
   spmx_hola_postprocess(h);
   spmx_csr5_postprocess(h);
   spmx_tiled_postprocess(h);
+  spmx_hybrid_postprocess(h);
   dfree(h->bfs_visited); dfree(h->bfs_front); dfree(h->bfs_q[0]); dfree(h->bfs_q[1]);
   dfree(h->bfs_cnt); dfree(h->bfs_edges); dfree(h->bfs_fb1); dfree(h->bfs_fb2); dfree(h->bfs_ctrl);
   dfree(h->ms_visit); dfree(h->ms_front0); dfree(h->ms_front1); dfree(h->ms_next);

@@ -79,6 +79,7 @@ struct spmx_handle_s {
   // CSR5 tile tables (csr5.cu) and tiled-SpMV tables (tiled.cu)
   void* csr5 = nullptr;
   void* tiled = nullptr;
+  void* hybrid = nullptr;  // CSR/CSC split tables (hybrid.cu)
 
   // Hola tables
   spmx::HolaTables hola{};

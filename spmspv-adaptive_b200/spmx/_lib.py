@@ -66,6 +66,11 @@ _SIGS = {
     "spmx_get_csc": (c_int, [P, PP, PP, PP]),
     "spmx_copy_csc": (c_int, [P, P, P, P]),
     "spmx_input_coo": (c_int, [P, c_int, P, P, P]),
+    "spmx_hybrid_preprocess": (c_int, [P]),
+    "spmx_hybrid_postprocess": (c_int, [P]),
+    "spmx_hybrid_info": (c_int, [P, PI, PI]),
+    "spmx_hybrid_copy": (c_int, [P, P, P, P, P, P, P]),
+    "spmx_hybridspmv": (c_int, [P, c_float, P]),
     "spmx_copy_csr": (c_int, [P, P, P, P]),
     "spmx_set_x": (c_int, [P, P]),
     "spmx_set_sparse_x": (c_int, [P, P, P, c_int]),

@@ -113,6 +113,36 @@ class SpmspvHandle:
         self._stream.synchronize()
         return rowptr, col, val
 
+    # -- hybrid CSR/CSC split (a candidate ninth kernel) ------------------------
+    def hybridPreprocess(self):
+        check(lib.spmx_hybrid_preprocess(self._h), "hybridPreprocess")
+
+    def hybridPostprocess(self):
+        check(lib.spmx_hybrid_postprocess(self._h), "hybridPostprocess")
+
+    def hybrid_info(self):
+        """(nonzeros in the CSR part, nonzeros in the CSC part)"""
+        a, b = c_int(), c_int()
+        check(lib.spmx_hybrid_info(self._h, ctypes.byref(a), ctypes.byref(b)), "hybrid_info")
+        return a.value, b.value
+
+    def hybrid_parts(self):
+        """((rowptr, col, val) of the CSR part, (colptr, row, val) of the CSC
+        part) copied into new tensors."""
+        a, b = self.hybrid_info()
+        i32 = dict(dtype=torch.int32, device="cuda")
+        rp, cl, vl = (torch.empty(self.m + 1, **i32), torch.empty(max(a, 1), **i32),
+                      torch.empty(max(a, 1), device="cuda"))
+        cp, rw, cv = (torch.empty(self.n + 1, **i32), torch.empty(max(b, 1), **i32),
+                      torch.empty(max(b, 1), device="cuda"))
+        check(lib.spmx_hybrid_copy(self._h, _ptr(rp), _ptr(cl), _ptr(vl), _ptr(cp), _ptr(rw),
+                                   _ptr(cv)), "hybrid_copy")
+        self._stream.synchronize()
+        return (rp, cl[:a], vl[:a]), (cp, rw[:b], cv[:b])
+
+    def hybridspmv(self, alpha, y):
+        check(lib.spmx_hybridspmv(self._h, float(alpha), _f32(y)), "hybridspmv")
+
     def ToCSC(self):
         check(lib.spmx_to_csc(self._h), "ToCSC")
 

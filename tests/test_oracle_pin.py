@@ -85,3 +85,33 @@ def test_std_row_intmean(ref, idx):
     assert r == np.float32(orc.std_row_intmean_faithful(A.rowptr))
     # the exact (FP64) value the engine reports differs only by float drift
     assert float(r) == pytest.approx(orc.std_row_intmean(A.rowptr), rel=1e-3)
+
+
+@pytest.mark.parametrize("idx", range(3))
+def test_coo2hybrid_split_matches_reference(ref, idx):
+    """The oracle's COO2Hybrid restatement (row priority) against the
+    reference's own COO2Hybrid: the same CSR-part count, the same CSR part in
+    (row, column) order and the same CSC part in (column, row) order.  The
+    reference sizes its count arrays by nnz, so every case has
+    nnz >= max(m, n)."""
+    from spmx import gen
+    rng = np.random.default_rng(11)
+    A = [rand_csr(600, 500, density=0.02, seed=12),
+         rand_csr(3000, 2000, lens=np.minimum(rng.zipf(1.4, 3000), 1500) + 1, seed=13),
+         gen.laplacian(40, 0.01, seed=4)][idx]
+    assert A.nnz >= max(A.m, A.n)
+    ref.ref_coo2hybrid.argtypes = [ctypes.c_int] * 3 + [ctypes.c_void_p] * 4
+    ref.ref_coo2hybrid.restype = None
+    row = np.repeat(np.arange(A.m, dtype=np.int32), np.diff(A.rowptr))
+    col, val = A.col.copy(), A.val.copy()
+    k = ctypes.c_int()
+    ref.ref_coo2hybrid(A.m, A.n, A.nnz, row.ctypes.data, col.ctypes.data, val.ctypes.data,
+                       ctypes.byref(k))
+    kk, flags = orc.coo2hybrid(A.n, A.rowptr, A.col)
+    assert kk == k.value
+    r0 = np.repeat(np.arange(A.m, dtype=np.int32), np.diff(A.rowptr))
+    assert np.array_equal(row[:kk], r0[flags]) and np.array_equal(col[:kk], A.col[flags])
+    assert np.array_equal(val[:kk].view(np.uint32), A.val[flags].view(np.uint32))
+    o = np.lexsort((r0[~flags], A.col[~flags]))
+    assert np.array_equal(row[kk:], r0[~flags][o]) and np.array_equal(col[kk:], A.col[~flags][o])
+    assert np.array_equal(val[kk:].view(np.uint32), A.val[~flags][o].view(np.uint32))
