@@ -156,6 +156,57 @@ def make_inputs():
     return A, xs
 
 
+def ref_gpu_sweep(A, xs, colptr, row, cval, binl, reps=7):
+    """The reference's own GPU kernels (oracle/_ref, rebuilt for sm_100a from
+    its sources) on the same sweep: per density the fastest of the kernels
+    that run here (CSC naive atomic SpMSpV for every density; Hola and naive
+    CSR SpMV for the dense x), each result checked against the FP64 oracle.
+    Left out: the merge-path and sort CSC SpMSpV, whose chained scan spins
+    without a bound on the previous block's sum, and CSR5, whose
+    preprocessing made an illegal memory access on this matrix."""
+    import ctypes
+    import oracle.oracle as orc
+    so = os.path.join(ROOT, "oracle", "_ref", "libref_host.so")
+    if not os.path.exists(so):
+        return {"unavailable": "oracle/_ref/libref_host.so not built"}
+    lib = ctypes.CDLL(so)
+    P = ctypes.c_void_p
+    lib.ref_gpu_time.argtypes = [ctypes.c_int] * 4 + [P] * 7 + [ctypes.c_int, P, P, ctypes.c_int, P, P]
+    lib.ref_gpu_time.restype = ctypes.c_int
+    m, n, nnz = A.m, A.n, A.nnz
+    names = {0: "hola-spmv", 1: "csr5-spmv", 2: "naive-spmv", 3: "csc-naive-atomic"}
+    per = []
+    tot_ms, tot_bytes = 0.0, 0
+    for (d, key, val), b in zip(xs, binl):
+        xd = orc.sparse2dense_bits(n, key, val)[0].astype(np.float32)
+        y64, mag = orc.spmv_f64(A.rowptr, A.col, A.val, xd)
+        kinds = (3, 0, 2) if d >= 1.0 else (3,)
+        times = {}
+        for w in kinds:
+            ms = np.zeros(reps, np.float32)
+            y = np.zeros(m, np.float32)
+            rc = lib.ref_gpu_time(w, m, n, nnz, A.rowptr.ctypes.data, A.col.ctypes.data, A.val.ctypes.data,
+                                  colptr.ctypes.data, row.ctypes.data, cval.ctypes.data, xd.ctypes.data,
+                                  len(key), key.ctypes.data, val.ctypes.data, reps, ms.ctypes.data,
+                                  y.ctypes.data)
+            ok = rc == 0 and bool(orc.within_tol(y, y64, mag, 1e-5)[0])
+            times[names[w]] = {"ms": float(np.median(ms)), "within_1e-5": ok}
+        good = [(v["ms"], k) for k, v in times.items() if v["within_1e-5"]]
+        if not good:
+            per.append({"density": d, "best": None, "kernels": times})
+            continue
+        best = min(good)
+        per.append({"density": d, "best": best[1], "ms": best[0], "kernels": times})
+        tot_ms += best[0]
+        tot_bytes += eff_bytes(m, n, nnz, len(key), b)
+    if any(p["best"] is None for p in per):
+        return {"unavailable": "a density had no result within 1e-5", "sweep": per}
+    return {"value": tot_bytes / (tot_ms * 1e-3) / 1e9, "unit": "GB/s", "ms_per_step": tot_ms,
+            "what": "the reference's kernels rebuilt for sm_100a, fastest correct one per density "
+                    "(an exhaustive pick, no selector cost), L2 flushed before each call",
+            "sweep": per}
+
+
 # ---------------------------------------------------------------------------
 # reference arm: the reference's CPU routines on all host threads
 # ---------------------------------------------------------------------------
@@ -200,6 +251,8 @@ def run_reference(args, world, rank):
                                        "sparse x and serialspmv for dense x (oracle restatement, "
                                        "OpenMP over all host threads)"},
             "e2e": {"value": gbs, "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    if args.ref_gpu:
+        line["ref_gpu_sm100a"] = ref_gpu_sweep(A, xs, colptr, row, cval, binl)
     print(json.dumps(line), flush=True)
     return 0
 
@@ -927,6 +980,9 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-batched", action="store_true")
     ap.add_argument("--no-ingest", action="store_true")
+    ap.add_argument("--ref-gpu", action="store_true",
+                    help="with --impl reference: also time the reference's own GPU kernels, rebuilt "
+                         "for sm_100a, on the same sweep")
     ap.add_argument("--tune-cache", default=None,
                     help="autotuner cache file: a second run with the same file (e.g. under a profiler, "
                          "whose serialised timings would mislead the tuner) reuses the first run's choices")

@@ -65,3 +65,90 @@ extern "C" int ref_load_csr(const char* path, int* m, int* n, int* nnz, int* row
 extern "C" void ref_coo2hybrid(int m, int n, int nnz, int* row, int* col, float* val, int* csr_nnz) {
   COO2Hybrid<float>(1, m, n, nnz, row, col, val, csr_nnz);
 }
+
+// GPU comparator (test infrastructure): the reference's own SpMV / SpMSpV
+// kernels, compiled for sm_100a from its sources, timed with CUDA events on
+// the default stream, with a 256 MiB memset before each call to flush L2.
+// Only kernels without waits between thread blocks run here: Hola SpMV
+// (holaspmv.h), CSR5 SpMV (csr5_spmv_cuda.h), the naive CSR SpMV
+// (naivespmv.h) and the atomic naive CSC SpMSpV (CscBasedNoSortNaiveSpmspv,
+// csc_sort_spmspv.cuh:98-119).  The merge-path and sort CSC variants use a
+// chained scan whose blocks spin without a bound on the previous block's sum
+// (scan_kernel.cuh:99, :232), so they are not run.  The CSR5 path (which 1)
+// made an illegal memory access in its preprocessing on the 1M-row Zipf
+// matrix; callers leave it out.
+//   which: 0 Hola SpMV, 1 CSR5 SpMV, 2 naive SpMV, 3 CSC naive atomic SpMSpV
+// All arrays are host arrays; the function makes its own device copies.
+// ms_out[reps] receives each call's time, y_out[m] the last result.
+// Returns 0, or -1 after a CUDA error.
+namespace {
+template <class T>
+T* dcopy(const T* h, size_t count) {
+  T* d = nullptr;
+  if (cudaMalloc((void**)&d, sizeof(T) * (count ? count : 1)) != cudaSuccess) return nullptr;
+  if (count && h) cudaMemcpy(d, h, sizeof(T) * count, cudaMemcpyHostToDevice);
+  return d;
+}
+}  // namespace
+
+extern "C" int ref_gpu_time(int which, int m, int n, int nnz, const int* rowptr, const int* col,
+                            const float* val, const int* colptr, const int* crow, const float* cval,
+                            const float* x, int x_nnz, const int* xkey, const float* xval, int reps,
+                            float* ms_out, float* y_out) {
+  int* d_rp = dcopy(rowptr, (size_t)m + 1);
+  int* d_col = dcopy(col, (size_t)nnz);
+  float* d_val = dcopy(val, (size_t)nnz);
+  int* d_cp = which == 3 ? dcopy(colptr, (size_t)n + 1) : nullptr;
+  int* d_crow = which == 3 ? dcopy(crow, (size_t)nnz) : nullptr;
+  float* d_cval = which == 3 ? dcopy(cval, (size_t)nnz) : nullptr;
+  float* d_x = dcopy(x, (size_t)n);
+  int* d_xkey = which == 3 ? dcopy(xkey, (size_t)x_nnz) : nullptr;
+  float* d_xval = which == 3 ? dcopy(xval, (size_t)x_nnz) : nullptr;
+  float* d_y = dcopy<float>(nullptr, (size_t)m);
+  char* flush = dcopy<char>(nullptr, (size_t)256 << 20);
+  SpmspvHandle<int, unsigned int, float> A(m, n, nnz);
+  if (which == 3) {
+    A.InputCSC(nnz, d_crow, d_cp, d_cval);
+    A.set_sparse_x(d_xkey, d_xval, x_nnz);
+    A.allocPreBuffer();
+  } else {
+    A.InputCSR(nnz, d_rp, d_col, d_val);
+    if (which == 1) {
+      A.setX(d_x);
+      A.setSigma(ANONYMOUSLIB_AUTO_TUNED_SIGMA);  // as the reference's drivers do
+      A.CSR5Preprocess();
+    } else {
+      A.set_x(d_x);
+      if (which == 0) A.holaPreprocess();
+    }
+  }
+  auto call = [&]() {
+    int ynnz = 0;
+    if (which == 0) A.holaspmv(1.0f, d_y);
+    else if (which == 1) A.csr5spmv(1.0f, d_y);
+    else if (which == 2) A.naivespmv(1.0f, d_y);
+    else A.CscBasedNoSortNaiveSpmspv(1.0f, &ynnz, d_y);
+  };
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  for (int w = 0; w < 2; ++w) call();
+  for (int r = 0; r < reps; ++r) {
+    cudaMemset(flush, r & 0xff, (size_t)256 << 20);
+    cudaEventRecord(e0, 0);
+    call();
+    cudaEventRecord(e1, 0);
+    cudaEventSynchronize(e1);
+    cudaEventElapsedTime(&ms_out[r], e0, e1);
+  }
+  if (y_out) cudaMemcpy(y_out, d_y, sizeof(float) * (size_t)m, cudaMemcpyDeviceToHost);
+  const cudaError_t err = cudaDeviceSynchronize();
+  if (which == 0) A.holaPostprocess();
+  if (which == 1) A.CSR5Postprocess();
+  if (which == 3) A.deallocPreBuffer();
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFree(d_rp); cudaFree(d_col); cudaFree(d_val); cudaFree(d_cp); cudaFree(d_crow); cudaFree(d_cval);
+  cudaFree(d_x); cudaFree(d_xkey); cudaFree(d_xval); cudaFree(d_y); cudaFree(flush);
+  return err == cudaSuccess ? 0 : -1;
+}
