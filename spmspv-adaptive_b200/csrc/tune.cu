@@ -4,7 +4,8 @@
 // of every tunable choice on the handle's matrix with CUDA events and keeps
 // the fastest:
 //   - the load-balanced SpMV back-end: Hola (4, 8 or 16 nonzeros per thread),
-//     CSR5 (sigma by the reference's rule) or tiled (x window width);
+//     CSR5 (sigma: the reference's rule or 4, 8, 16, 32 nonzeros per lane)
+//     or tiled (x window width);
 //   - the lanes per row of the naive CSR kernel and per column of the naive
 //     CSC kernel;
 //   - merge-path vs fixed-nonzero blocks for the load-balanced CSC kernel;
@@ -41,6 +42,7 @@ __global__ void stride_keys_kernel(int* key, float* val, int k, int n) {
 struct Params {
   int spmv_type = SPMX_SPMV_HOLA, hola_vt = 8, tiled_rb = 0, tiled_win = 8192;
   int row_group = 0, col_group = 0, lb_variant = SPMX_CSC_LB_MERGE, buckets = 256;
+  int csr5_sigma = -1;  // -1: the reference's rule
 };
 
 unsigned long long fingerprint(spmx_handle_t h) {
@@ -70,9 +72,12 @@ bool cache_lookup(const char* path, unsigned long long fp, Params* p) {
   while (fgets(line, sizeof(line), f)) {
     unsigned long long k = 0;
     Params q;
-    if (sscanf(line, "%llx %d %d %d %d %d %d %d %d", &k, &q.spmv_type, &q.hola_vt, &q.tiled_rb,
-               &q.tiled_win, &q.row_group, &q.col_group, &q.lb_variant, &q.buckets) == 9 &&
-        k == fp) {
+    // 10 fields; lines written before CSR5 sigma was tuned have 9
+    const int got = sscanf(line, "%llx %d %d %d %d %d %d %d %d %d", &k, &q.spmv_type, &q.hola_vt,
+                           &q.tiled_rb, &q.tiled_win, &q.row_group, &q.col_group, &q.lb_variant,
+                           &q.buckets, &q.csr5_sigma);
+    if (got == 9) q.csr5_sigma = -1;
+    if (got >= 9 && k == fp) {
       *p = q;
       found = true;
     }
@@ -85,8 +90,8 @@ void cache_store(const char* path, unsigned long long fp, const Params& q) {
   if (!path) return;
   FILE* f = fopen(path, "a");
   if (!f) return;
-  fprintf(f, "%llx %d %d %d %d %d %d %d %d\n", fp, q.spmv_type, q.hola_vt, q.tiled_rb, q.tiled_win,
-          q.row_group, q.col_group, q.lb_variant, q.buckets);
+  fprintf(f, "%llx %d %d %d %d %d %d %d %d %d\n", fp, q.spmv_type, q.hola_vt, q.tiled_rb, q.tiled_win,
+          q.row_group, q.col_group, q.lb_variant, q.buckets, q.csr5_sigma);
   fclose(f);
 }
 
@@ -108,7 +113,11 @@ static int apply_params(spmx_handle_t h, const Params& p) {
       rc = spmx_hola_preprocess(h);
     }
   } else if (p.spmv_type == SPMX_SPMV_CSR5) {
-    if (!h->csr5) rc = spmx_csr5_preprocess(h);
+    if (!h->csr5 || h->sigma != p.csr5_sigma) {
+      spmx_csr5_postprocess(h);
+      h->sigma = p.csr5_sigma;
+      rc = spmx_csr5_preprocess(h);
+    }
   } else if (p.spmv_type == SPMX_SPMV_TILED) {
     rc = spmx_tiled_preprocess(h, p.tiled_rb, p.tiled_win, 0, 0);
   }
@@ -174,11 +183,16 @@ extern "C" int spmx_autotune(spmx_handle_t h, const char* cache_path, int* spmv_
       const float t = time_us([&] { return spmx_holaspmv(h, 1.0f, y); });
       if (t < best_t) { best_t = t; best.spmv_type = SPMX_SPMV_HOLA; best.hola_vt = vt; }
     }
-    if (spmx_csr5_preprocess(h) == SPMX_SUCCESS) {
-      const float t = time_us([&] { return spmx_csr5spmv(h, 1.0f, y); });
-      if (t < best_t) { best_t = t; best.spmv_type = SPMX_SPMV_CSR5; }
+    const int saved_sigma = h->sigma;
+    for (int sg : {-1, 4, 8, 16, 32}) {
       spmx_csr5_postprocess(h);
+      h->sigma = sg;
+      if (spmx_csr5_preprocess(h) != SPMX_SUCCESS) continue;
+      const float t = time_us([&] { return spmx_csr5spmv(h, 1.0f, y); });
+      if (t < best_t) { best_t = t; best.spmv_type = SPMX_SPMV_CSR5; best.csr5_sigma = sg; }
     }
+    spmx_csr5_postprocess(h);
+    h->sigma = saved_sigma;
     for (int win : {4096, 8192}) {
       const int rb = 0;  // rows per block: as many as shared memory holds
       if (spmx_tiled_preprocess(h, rb, win, 0, 0) != SPMX_SUCCESS) continue;
