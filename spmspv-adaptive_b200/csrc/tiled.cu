@@ -20,11 +20,13 @@
 //     window, packed (row, column) words, values) into a ring of shared
 //     memory buffers with cp.async.bulk, completion tracked by mbarriers;
 //   - consumer warps each own a fixed range of the block's rows (equal
-//     nonzero counts).  A warp reads its slice of the stage (128 entries per
-//     step, 4 per lane), gathers x from the shared window, reduces equal rows
-//     with a lane-level segmented scan and adds each row sum into the shared
-//     y with a plain read-modify-write: no two warps ever touch a row, and a
-//     warp updates a row in stage order, so the result is deterministic;
+//     nonzero counts).  A warp's slice of a stage is cut into 32 contiguous
+//     lane ranges, stored lane-interleaved; each lane gathers x from the
+//     shared window, sums its runs of equal rows in registers and adds them
+//     into the shared y with a plain read-modify-write; a run that crosses
+//     into the next lane is joined with shuffles and added once.  No two
+//     warps ever touch a row, and a warp updates a row in stage order, so
+//     the result is deterministic;
 //   - at the end the cluster's partial y vectors are added in CTA-rank order
 //     through distributed shared memory and each row is stored once.
 //
