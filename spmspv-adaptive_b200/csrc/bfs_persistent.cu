@@ -414,10 +414,16 @@ __global__ void levels_transpose_kernel(int n, int ns, const int* __restrict__ v
 // to 1024 vertices per CTA) and a large one the whole resident capacity.
 template <class K>
 static int coop_grid(K kernel, int num_sms, int min_ctas, long long work_items) {
-  int per = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, 256, 0) != cudaSuccess) {
-    cudaGetLastError();
-    return 0;
+  // the occupancy query costs host time on every launch otherwise; one value
+  // per kernel (the same on every GPU of a node)
+  static int per = -1;
+  if (per < 0) {
+    int p = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&p, kernel, 256, 0) != cudaSuccess) {
+      cudaGetLastError();
+      return 0;
+    }
+    per = p;
   }
   const long long cap = (long long)per * num_sms;
   long long want = (work_items + 255) / 256;
