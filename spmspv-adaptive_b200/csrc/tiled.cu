@@ -118,15 +118,12 @@ __device__ __forceinline__ void l2_prefetch(const void* src, unsigned bytes) {
   asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(src), "r"(bytes) : "memory");
 }
 
-// Shared memory layout (dynamic): full[NB] and empty[NB] barriers,
-// offs[NB][NW+1], then per buffer the x window (win floats), the bitmap
-// window (win/32 words), packed words and values (chunk each), then y
-// (rmax floats).
+// Shared memory layout (dynamic): full[NB] and empty[NB] barriers, then per
+// buffer the x window (win floats), the bitmap window (win/32 words), packed
+// words and values (chunk each), then y (rmax floats).
 template <int NW>
 struct TileSmem {
-  static constexpr int kOffs = 2 * kTileBuf * 8;
-  static constexpr int kOffsBytes = ((kTileBuf * (NW + 1) * 4) + 15) & ~15;
-  static constexpr int kBufBase = ((kOffs + kOffsBytes) + 127) & ~127;
+  static constexpr int kBufBase = ((2 * kTileBuf * 8) + 127) & ~127;
   __host__ __device__ static int buf_bytes(const TileGeom& g) { return 4 * g.win + g.win / 8 + 8 * g.chunk; }
   __host__ __device__ static int total(const TileGeom& g) {
     return kBufBase + kTileBuf * buf_bytes(g) + 4 * g.rmax;
@@ -254,7 +251,6 @@ tiled_spmv_kernel(int n, TileGeom g, int cs, const int* __restrict__ rb_row,
   __shared__ volatile int s_abort;
   unsigned long long* full = reinterpret_cast<unsigned long long*>(smem);
   unsigned long long* empty = full + kTileBuf;
-  int* offs = reinterpret_cast<int*>(smem + L::kOffs);
   unsigned char* bufs = smem + L::kBufBase;
   const int bb = L::buf_bytes(g);
   float* ys = reinterpret_cast<float*>(bufs + kTileBuf * bb);
@@ -283,21 +279,19 @@ tiled_spmv_kernel(int n, TileGeom g, int cs, const int* __restrict__ rb_row,
   __syncthreads();
 
   if (warp == NW) {
-    // producer warp.  Lane l keeps the descriptor and warp offsets of stage
-    // (batch * 32 + l) in registers, fetched one batch of 32 stages ahead so
-    // that no global load sits between a free buffer and its refill.
+    // producer warp.  Lane l keeps the descriptor of stage (batch * 32 + l) in
+    // registers, fetched one batch of 32 stages ahead, and that lane issues
+    // the stage: it waits for the free buffer, arms the full barrier and
+    // starts the bulk copies.  Only the window index is broadcast (the whole
+    // warp copies an unaligned x tail), so a stage costs the producer a few
+    // instructions and no global load.
     int4 cur_d = make_int4(0, 0, 0, 0), nxt_d = make_int4(0, 0, 0, 0);
-    int cur_o[NW + 1], nxt_o[NW + 1];
-    auto fetch = [&](int first, int4& d, int (&o)[NW + 1]) {
+    auto fetch = [&](int first, int4& d) {
       const int s = first + lane;
-      if (s < cnt) {
-        d = __ldg(reinterpret_cast<const int4*>(stages) + s0 + s);
-#pragma unroll
-        for (int k = 0; k <= NW; ++k) o[k] = __ldg(offsets + (size_t)(s0 + s) * (NW + 1) + k);
-      }
+      if (s < cnt) d = __ldg(reinterpret_cast<const int4*>(stages) + s0 + s);
     };
-    fetch(0, cur_d, cur_o);
-    fetch(32, nxt_d, nxt_o);
+    fetch(0, cur_d);
+    fetch(32, nxt_d);
     if (lane < kTilePrefetch && lane < cnt && cur_d.z > 0) {
       l2_prefetch(packed + cur_d.y, 4u * cur_d.z);
       l2_prefetch(val + cur_d.y, 4u * cur_d.z);
@@ -307,46 +301,32 @@ tiled_spmv_kernel(int n, TileGeom g, int cs, const int* __restrict__ rb_row,
       const int b = i % kTileBuf;
       if (i > 0 && (i & 31) == 0) {
         cur_d = nxt_d;
-#pragma unroll
-        for (int k = 0; k <= NW; ++k) cur_o[k] = nxt_o[k];
-        fetch(i + 32, nxt_d, nxt_o);
+        fetch(i + 32, nxt_d);
       }
-      // L2 prefetch of the nonzeros of stage i + kTilePrefetch
+      // L2 prefetch of the nonzeros of stage i + kTilePrefetch, by its lane
       {
         const int j = i + kTilePrefetch;
-        const int jl = j & 31;
-        const bool in_cur = (j >> 5) == (i >> 5);
-        const int pe0 = __shfl_sync(0xffffffffu, in_cur ? cur_d.y : nxt_d.y, jl);
-        const int plen = __shfl_sync(0xffffffffu, in_cur ? cur_d.z : nxt_d.z, jl);
-        if (lane == 0 && j < cnt && plen > 0) {
-          l2_prefetch(packed + pe0, 4u * plen);
-          l2_prefetch(val + pe0, 4u * plen);
-        }
-      }
-      const int src = i & 31;
-      TileStage sd;
-      sd.window = __shfl_sync(0xffffffffu, cur_d.x, src);
-      sd.e0 = __shfl_sync(0xffffffffu, cur_d.y, src);
-      sd.len = __shfl_sync(0xffffffffu, cur_d.z, src);
-      int my_off = 0;
-#pragma unroll
-      for (int k = 0; k <= NW; ++k) {
-        const int v = __shfl_sync(0xffffffffu, cur_o[k], src);
-        if (lane == k) my_off = v;
-      }
-      if (i >= kTileBuf) {
-        bool ok = true;
-        if (lane == 0) ok = bar_wait(empty + b, ((i / kTileBuf) - 1) & 1, &s_abort);
-        ok = __shfl_sync(0xffffffffu, ok, 0);
-        if (!ok) {
-          if (lane == 0) {
-            flag_error(err, kDevErrTimeout);
-            s_abort = 1;
+        if (j < cnt && lane == (j & 31)) {
+          const int4 d = (j >> 5) == (i >> 5) ? cur_d : nxt_d;
+          if (d.z > 0) {
+            l2_prefetch(packed + d.y, 4u * d.z);
+            l2_prefetch(val + d.y, 4u * d.z);
           }
-          break;
         }
       }
-      const int cbase = sd.window * g.win;
+      const int owner = i & 31;
+      bool ok = true;
+      if (lane == owner && i >= kTileBuf) ok = bar_wait(empty + b, ((i / kTileBuf) - 1) & 1, &s_abort);
+      ok = __shfl_sync(0xffffffffu, ok, owner);
+      if (!ok) {
+        if (lane == owner) {
+          flag_error(err, kDevErrTimeout);
+          s_abort = 1;
+        }
+        break;
+      }
+      const int window = __shfl_sync(0xffffffffu, cur_d.x, owner);
+      const int cbase = window * g.win;
       const int xw = min(g.win, n - cbase);
       float* xs = xs_of(b);
       unsigned* bits = bits_of(b);
@@ -359,15 +339,15 @@ tiled_spmv_kernel(int n, TileGeom g, int cs, const int* __restrict__ rb_row,
         wb = x_aligned ? ((nwd * 4) & ~15) : 0;
         for (int q = wb / 4 + lane; q < nwd; q += 32) bits[q] = __ldg(xbits + (cbase >> 5) + q);
       }
-      if (lane <= NW) offs[b * (NW + 1) + lane] = my_off;
       __syncwarp();
-      if (lane == 0) {
-        bar_arrive_tx(full + b, (unsigned)(xb + wb + 8 * sd.len));
+      if (lane == owner) {
+        const int e0 = cur_d.y, len = cur_d.z;
+        bar_arrive_tx(full + b, (unsigned)(xb + wb + 8 * len));
         if (xb) bulk_load(xs, x + cbase, (unsigned)xb, full + b);
         if (wb) bulk_load(bits, xbits + (cbase >> 5), (unsigned)wb, full + b);
-        if (sd.len) {
-          bulk_load(pk_of(b), packed + sd.e0, 4u * sd.len, full + b);
-          bulk_load(vv_of(b), val + sd.e0, 4u * sd.len, full + b);
+        if (len) {
+          bulk_load(pk_of(b), packed + e0, 4u * len, full + b);
+          bulk_load(vv_of(b), val + e0, 4u * len, full + b);
         }
       }
       issued = i + 1;
@@ -379,9 +359,26 @@ tiled_spmv_kernel(int n, TileGeom g, int cs, const int* __restrict__ rb_row,
         if (!bar_wait(full + (i % kTileBuf), (i / kTileBuf) & 1, &never)) flag_error(err, kDevErrTimeout);
     }
   } else {
-    // consumer warps
+    // consumer warps.  Lane l keeps this warp's entry range in stage
+    // (batch * 32 + l), fetched one batch of 32 stages ahead.
+    int2 cur_r = make_int2(0, 0), nxt_r = make_int2(0, 0);
+    auto fetch = [&](int first, int2& r) {
+      const int s = first + lane;
+      if (s < cnt) {
+        const int* o = offsets + (size_t)(s0 + s) * (NW + 1) + warp;
+        r = make_int2(__ldg(o), __ldg(o + 1));
+      }
+    };
+    fetch(0, cur_r);
+    fetch(32, nxt_r);
     for (int i = 0; i < cnt; ++i) {
       const int b = i % kTileBuf;
+      if (i > 0 && (i & 31) == 0) {
+        cur_r = nxt_r;
+        fetch(i + 32, nxt_r);
+      }
+      const int lo = __shfl_sync(0xffffffffu, cur_r.x, i & 31);
+      const int hi = __shfl_sync(0xffffffffu, cur_r.y, i & 31);
       bool ok = true;
       if (lane == 0) ok = bar_wait(full + b, (i / kTileBuf) & 1, &s_abort);
       ok = __shfl_sync(0xffffffffu, ok, 0);
@@ -392,7 +389,6 @@ tiled_spmv_kernel(int n, TileGeom g, int cs, const int* __restrict__ rb_row,
         }
         break;
       }
-      const int lo = offs[b * (NW + 1) + warp], hi = offs[b * (NW + 1) + warp + 1];
       tile_warp_slice<(NW <= 4 ? 16 : 8), GATED>(lo, hi, pk_of(b), vv_of(b), xs_of(b), bits_of(b), ys);
       if (lane == 0) bar_arrive(empty + b);
     }
