@@ -67,7 +67,8 @@ class Clocks:
     def __init__(self, index):
         self.index = index
         self.proc = None
-        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_{os.getpid()}.csv")
+        import tempfile
+        self.path = os.path.join(tempfile.gettempdir(), f"spmx_clocks_{os.getpid()}.csv")
 
     def __enter__(self):
         try:
