@@ -357,6 +357,26 @@ def run_ours(args, world, rank, local):
         with open(tp) as f:
             traffic = json.load(f).get(f"{kname}_spmv_zipf1m")
 
+    # --- correctness of the sweep (rank 0): each density's y against the FP64
+    # oracle with the parity tests' magnitude-scaled bound, plus the raw
+    # relative and normwise errors ---
+    correctness = []
+    if rank == 0:
+        import oracle.oracle as orc
+        colptr_h, row_h, cval_h = A.to_csc()
+        for (dd, kd, vd, k), (_, key, val) in zip(dx, xs):
+            h.set_sparse_x(kd, vd, k)
+            h.run_adaptive(1.0, y)
+            yh = y.cpu().numpy().astype(np.float64)
+            y64, mag, _ = orc.spmspv_csc_f64(m, colptr_h, row_h, cval_h, key, val)
+            nz = y64 != 0
+            rel = float(np.max(np.abs(yh[nz] - y64[nz]) / np.abs(y64[nz]))) if nz.any() else 0.0
+            top = float(np.max(np.abs(y64))) if len(y64) else 0.0
+            correctness.append({"density": dd, "within_1e-5": bool(orc.within_tol(yh, y64, mag, 1e-5)[0]),
+                                "max_scaled_err": orc.max_scaled_err(yh, y64, mag), "max_rel_err": rel,
+                                "normwise_err": float(np.max(np.abs(yh - y64))) / top if top else 0.0})
+        h.check_device_error()
+
     # --- e2e through the public API with host buffers.  Per call: the
     # pinned host->device copy of x, the adaptive call, and the read-back of
     # y: for a sparse x the nonzeros of y (dense2sparse_outer, which returns
@@ -452,6 +472,9 @@ def run_ours(args, world, rank, local):
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic",
             "config": {"workload": WORKLOAD, "l2": "flushed (256 MiB write) before every timed call",
+                       "row_lengths": {"mean": float(np.mean(np.diff(A.rowptr))),
+                                       "max": int(np.max(np.diff(A.rowptr))),
+                                       "std": float(np.std(np.diff(A.rowptr)))},
                        "spmv_backend": kname,
                        "parallelism": f"replicas x{world}" if world > 1 else "single"},
             "roofline": {"bound": "hbm", "kernel": f"{kname} SpMV (autotuned back-end), dense x",
@@ -463,6 +486,7 @@ def run_ours(args, world, rank, local):
             "gpu_launches": int(launches // max(args.steps, 1)),
             "clocks": clk.summary(),
             "sweep": sweep,
+            "correctness": correctness,
             "selector_vs_exhaustive": exhaustive,
             "cpu_baseline": cpu,
             "bfs": bfs,
