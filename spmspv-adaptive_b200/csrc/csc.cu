@@ -231,6 +231,14 @@ __global__ void zero_fill_kernel(float* __restrict__ y, long long m) {
   }
 }
 
+int launch_zero_fill(float* y, long long m, int num_sms, cudaStream_t st) {
+  if (m <= 0) return 0;
+  const long long blocks = std::min<long long>((m + 1023) / 1024, (long long)num_sms * 4);
+  note_launch();
+  zero_fill_kernel<<<(unsigned)std::max(1LL, blocks), 256, 0, st>>>(y, m);
+  return 0;
+}
+
 // zero y, then the naive CSC SpMSpV as a programmatic dependent launch
 int launch_csc_naive_zeroed(const CscArgs& a, int group, float* y, int num_sms, cudaStream_t st) {
   if (a.m > 0) {

@@ -456,8 +456,9 @@ static int ensure_bits(spmx_handle_t h) {
 extern "C" int spmx_sparse2dense(spmx_handle_t h) {
   SPMX_CHECK_HANDLE(h);
   SPMX_TRY(ensure_dense_x(h));
-  SPMX_CUDA(cudaMemsetAsync(h->x_dense, 0, 4 * (size_t)h->n, h->stream));
-  launch_scatter(h->x_nnz, h->n, h->x_key, h->x_val, h->x_dense, nullptr, h->d_err, h->stream);
+  if (launch_dense_from_sparse(h->x_nnz, h->n, h->x_key, h->x_val, h->x_dense, h->d_err, h->num_sms,
+                               h->stream))
+    return set_error(SPMX_ERR_CUDA, "sparse2dense launch");
   h->vec_type = SPMX_VEC_DENSE;
   return launch_ok("sparse2dense");
 }

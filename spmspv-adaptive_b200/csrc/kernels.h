@@ -109,6 +109,13 @@ int launch_csc_naive_pairs(const CscArgs& a, const CscScratch& s, int group,
                            int* pairs_row, float* pairs_val, cudaStream_t st);
 
 // ---- vecconv.cu
+// y[0..m) = 0 with a kernel that lets the next grid launch early
+int launch_zero_fill(float* y, long long m, int num_sms, cudaStream_t st);
+// dense[0..len) from (key, val): a zero fill, then the scatter as a
+// programmatic dependent launch that reads its keys and values while the
+// fill runs; the scatter in turn lets the next grid start early
+int launch_dense_from_sparse(int nvals, int len, const int* key, const float* val, float* dense,
+                             int* err, int num_sms, cudaStream_t st);
 int launch_scatter(int nvals, int len, const int* key, const float* val,
                    float* dense, int* bits, int* err, cudaStream_t st);
 int launch_dense2bits(int len, const float* dense, int* bits, cudaStream_t st);

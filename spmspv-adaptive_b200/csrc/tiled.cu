@@ -277,6 +277,9 @@ tiled_spmv_kernel(int n, TileGeom g, int cs, const int* __restrict__ rb_row,
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   __syncthreads();
+  // launched as a programmatic dependent of the grid that writes x: nothing
+  // above touches x or y
+  asm volatile("griddepcontrol.wait;" ::: "memory");
 
   if (warp == NW) {
     // producer warp.  Lane l keeps the descriptor of stage (batch * 32 + l) in
@@ -890,13 +893,15 @@ static cudaError_t tiled_launch(spmx_handle_t h, TiledTables* t, float alpha, fl
   cfg.blockDim = dim3((NW + 1) * 32);
   cfg.dynamicSmemBytes = t->smem;
   cfg.stream = h->stream;
-  cudaLaunchAttribute at[1];
+  cudaLaunchAttribute at[2];
   at[0].id = cudaLaunchAttributeClusterDimension;
   at[0].val.clusterDim.x = t->cs;
   at[0].val.clusterDim.y = 1;
   at[0].val.clusterDim.z = 1;
+  at[1].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[1].val.programmaticStreamSerializationAllowed = 1;
   cfg.attrs = at;
-  cfg.numAttrs = 1;
+  cfg.numAttrs = 2;
   return cudaLaunchKernelEx(&cfg, tiled_spmv_kernel<NW, GATED>, h->n, t->g, t->cs, (const int*)t->rb_row,
                             (const int*)t->cta_stage, (const TileStage*)t->stages, (const int*)t->offsets,
                             (const unsigned*)t->packed, (const float*)t->val, (const float*)h->x_dense, bits,

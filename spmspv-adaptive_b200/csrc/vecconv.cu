@@ -25,6 +25,28 @@ __global__ void scatter_kernel(int nvals, int len, const int* __restrict__ key,
   if (bits) atomicOr(bits + (k >> 5), (int)(1u << (k & 31)));
 }
 
+// scatter after a zero fill of `dense` launched just before (programmatic
+// dependent launch): keys and values are read before the wait
+__global__ void scatter_after_fill_kernel(int nvals, int len, const int* __restrict__ key,
+                                          const float* __restrict__ val, float* __restrict__ dense,
+                                          int* err) {
+  asm volatile("griddepcontrol.launch_dependents;");
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  int k = 0;
+  float v = 0.f;
+  if (i < nvals) {
+    k = __ldg(key + i);
+    v = val ? __ldg(val + i) : 1.0f;
+  }
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  if (i >= nvals) return;
+  if ((unsigned)k >= (unsigned)len) {
+    flag_error(err, kDevErrOob);
+    return;
+  }
+  dense[k] = v;
+}
+
 __global__ void dense2bits_kernel(int len, const float* __restrict__ dense,
                                   int* __restrict__ bits) {
   const long long gid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -89,6 +111,25 @@ int launch_scatter(int nvals, int len, const int* key, const float* val,
   scatter_kernel<<<(nvals + 255) / 256, 256, 0, st>>>(nvals, len, key, val, dense,
                                                      bits, err);
   return 0;
+}
+
+int launch_dense_from_sparse(int nvals, int len, const int* key, const float* val, float* dense,
+                             int* err, int num_sms, cudaStream_t st) {
+  launch_zero_fill(dense, len, num_sms, st);
+  if (nvals <= 0) return 0;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)((nvals + 255) / 256));
+  cfg.blockDim = dim3(256);
+  cfg.stream = st;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  note_launch();
+  return cudaLaunchKernelEx(&cfg, scatter_after_fill_kernel, nvals, len, key, val, dense, err) == cudaSuccess
+             ? 0
+             : -2;
 }
 
 int launch_dense2bits(int len, const float* dense, int* bits, cudaStream_t st) {
