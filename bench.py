@@ -39,7 +39,7 @@ METRIC = "SpMSpV/SpMV effective HBM GB/s vs x density; batched BFS GTEPS vs plai
 WORKLOAD = ("zipf-1M density sweep: 1,048,576^2 CSR+CSC, nnz 16,777,216, Zipf(1.5) rows "
             "(mean 16, cap 10,000), x density 1e-5..1.0, adaptive kernel per call")
 DENSITIES = (1e-5, 1e-4, 1e-3, 1e-2, 1e-1, 1.0)
-SPMV_BACKENDS = {0: "hola", 1: "csr5", 2: "tiled"}
+SPMV_BACKENDS = {0: "hola", 1: "csr5", 2: "tiled", 3: "round"}
 
 
 def peaks():
@@ -945,7 +945,7 @@ def cpu_baseline(A, xs, binl):
             "ms": best * 1e3}
 
 
-ONLY = ("hybrid", "ingest", "batched-spmspv", "adjoint", "hola-spmv", "csr5-spmv", "naive-spmv", "tiled-spmv", "hola-spmspv", "csc-lb-atomic",
+ONLY = ("hybrid", "ingest", "batched-spmspv", "adjoint", "hola-spmv", "csr5-spmv", "naive-spmv", "tiled-spmv", "round-spmv", "hola-spmspv", "csc-lb-atomic",
         "csc-naive-atomic", "csc-bucket", "csc-lb-sort", "bfs-rmat14", "bfs-batched")
 
 
@@ -983,6 +983,7 @@ def run_only(args):
     h.holaPreprocess()
     h.CSR5Preprocess()
     h.tiledPreprocess()
+    h.roundPreprocess()
     h.allocPreBuffer()
     dens = 1.0 if args.only.endswith("spmv") else args.density
     k = [x for x in xs if abs(x[0] - dens) < 1e-12][0]
@@ -997,6 +998,7 @@ def run_only(args):
         "csr5-spmv": lambda: h.csr5spmv(1.0, y),
         "naive-spmv": lambda: h.naivespmv(1.0, y),
         "tiled-spmv": lambda: h.tiledspmv(1.0, y),
+        "round-spmv": lambda: h.roundspmv(1.0, y),
         "hola-spmspv": lambda: h.holaspmspv(1.0, y),
         "csc-lb-atomic": lambda: h.spmspv_csc(1, 0, 1.0, y, sync=False),
         "csc-naive-atomic": lambda: h.spmspv_csc(0, 0, 1.0, y, sync=False),
@@ -1016,6 +1018,8 @@ def run_only(args):
     out = {"only": args.only, "density": dens, "ms": statistics.mean(ts), "min_ms": min(ts)}
     if args.only.startswith("tiled"):
         out["tiled"] = h.tiled_info()
+    if args.only.startswith("round"):
+        out["round"] = h.round_info()
     print(json.dumps(out))
     return 0
 

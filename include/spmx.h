@@ -62,6 +62,7 @@ extern "C" {
 #define SPMX_SPMV_HOLA 0
 #define SPMX_SPMV_CSR5 1
 #define SPMX_SPMV_TILED 2  /* row-block x column-window tiles (no reference counterpart) */
+#define SPMX_SPMV_ROUND 3  /* column-ordered rounds, row-owner reduction (no reference counterpart) */
 
 /* ---- CSC SpMSpV work distributions and write-backs (H:1824-2201) */
 #define SPMX_CSC_NAIVE     0  /* group of threads per x nonzero            */
@@ -205,6 +206,25 @@ int spmx_tiled_postprocess(spmx_handle_t h);
 int spmx_tiled_info(spmx_handle_t h, int* info);
 int spmx_tiledspmv(spmx_handle_t h, float alpha, float* d_y);
 int spmx_tiledspmspv(spmx_handle_t h, float alpha, float* d_y);
+/* Round SpMV / bitmap-gated SpMSpV (no reference counterpart; a fourth
+ * back-end for the load-balanced SpMV of the selector, spmv_type 3).  Rows
+ * are cut into row blocks whose y fits in shared memory (at most rb_rows
+ * rows; 0 = as many as fit), one per cluster of 2 CTAs; each CTA streams half
+ * of its block's nonzeros sorted by (column, row) in rounds of 8192: warps
+ * gather x in column order and store each product to a row-order slot in
+ * shared memory, then each warp reduces the rows it owns.  Deterministic.
+ * Fails with SPMX_ERR_INVALID_VALUE (the other back-ends still apply) when a
+ * column index is out of range, when a round of 8192 nonzeros spans 2^19
+ * columns or more (a very sparse row block), or when row blocks x columns
+ * need a sort key of more than 32 bits. */
+int spmx_round_preprocess(spmx_handle_t h, int rb_rows);
+int spmx_round_postprocess(spmx_handle_t h);
+/* geometry chosen by spmx_round_preprocess: info[0..7] = row blocks, CTAs
+ * per cluster, rounds, nonzeros per round, warps per CTA, shared y rows,
+ * shared bytes, grid */
+int spmx_round_info(spmx_handle_t h, int* info);
+int spmx_roundspmv(spmx_handle_t h, float alpha, float* d_y);
+int spmx_roundspmspv(spmx_handle_t h, float alpha, float* d_y);
 /* Hybrid CSR/CSC split (a candidate ninth kernel; the reference's
  * COO2Hybrid, INC/mtx.hpp:436-701, driven by TEST/test_coo2hybrid.cu:276-312).
  * Preprocess: copies the CSR to the host and visits the nonzeros in (row,
@@ -222,7 +242,7 @@ int spmx_hybrid_info(spmx_handle_t h, int* csr_nnz, int* csc_nnz);
 int spmx_hybrid_copy(spmx_handle_t h, int* d_rowptr, int* d_col, float* d_val, int* d_colptr,
                      int* d_row, float* d_cval);
 int spmx_hybridspmv(spmx_handle_t h, float alpha, float* d_y);
-/* set_spmv_type — H:1767 (0 Hola, 1 CSR5, 2 tiled) */
+/* set_spmv_type — H:1767 (0 Hola, 1 CSR5, 2 tiled, 3 round) */
 int spmx_set_spmv_type(spmx_handle_t h, int code);
 
 /* ======================= SpMV / CSR SpMSpV (y = alpha*A*x) =============== */

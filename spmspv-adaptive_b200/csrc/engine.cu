@@ -185,6 +185,8 @@ extern "C" int spmx_hola_postprocess(spmx_handle_t h);
 extern "C" int spmx_csr5_postprocess(spmx_handle_t h);
 extern "C" int spmx_tiled_postprocess(spmx_handle_t h);
 int tiled_spmv_impl(spmx_handle_t h, float alpha, float* y, bool gated);
+extern "C" int spmx_round_postprocess(spmx_handle_t h);
+int round_spmv_impl(spmx_handle_t h, float alpha, float* y, bool gated);
 
 extern "C" int spmx_destroy(spmx_handle_t h) {
   if (!h) return SPMX_SUCCESS;
@@ -201,6 +203,7 @@ extern "C" int spmx_destroy(spmx_handle_t h) {
   spmx_hola_postprocess(h);
   spmx_csr5_postprocess(h);
   spmx_tiled_postprocess(h);
+  spmx_round_postprocess(h);
   spmx_hybrid_postprocess(h);
   dfree(h->bfs_visited); dfree(h->bfs_front); dfree(h->bfs_q[0]); dfree(h->bfs_q[1]);
   dfree(h->bfs_cnt); dfree(h->bfs_edges); dfree(h->bfs_fb1); dfree(h->bfs_fb2); dfree(h->bfs_ctrl);
@@ -606,8 +609,8 @@ extern "C" int spmx_hola_postprocess(spmx_handle_t h) {
 
 extern "C" int spmx_set_spmv_type(spmx_handle_t h, int code) {
   SPMX_CHECK_HANDLE(h);
-  if (code != SPMX_SPMV_HOLA && code != SPMX_SPMV_CSR5 && code != SPMX_SPMV_TILED)
-    return set_error(SPMX_ERR_INVALID_VALUE, "spmv type must be 0 (Hola), 1 (CSR5) or 2 (tiled)");
+  if (code != SPMX_SPMV_HOLA && code != SPMX_SPMV_CSR5 && code != SPMX_SPMV_TILED && code != SPMX_SPMV_ROUND)
+    return set_error(SPMX_ERR_INVALID_VALUE, "spmv type must be 0 (Hola), 1 (CSR5), 2 (tiled) or 3 (round)");
   h->spmv_type = code;
   return SPMX_SUCCESS;
 }
@@ -674,11 +677,13 @@ extern "C" int spmx_csr5spmspv(spmx_handle_t h, float alpha, float* y) {
 extern "C" int spmx_spmv(spmx_handle_t h, float alpha, float* y) {
   SPMX_CHECK_HANDLE(h);
   if (h->spmv_type == SPMX_SPMV_TILED) return tiled_spmv_impl(h, alpha, y, false);
+  if (h->spmv_type == SPMX_SPMV_ROUND) return round_spmv_impl(h, alpha, y, false);
   return h->spmv_type == SPMX_SPMV_HOLA ? spmx_holaspmv(h, alpha, y) : spmx_csr5spmv(h, alpha, y);
 }
 extern "C" int spmx_spmspv(spmx_handle_t h, float alpha, float* y) {
   SPMX_CHECK_HANDLE(h);
   if (h->spmv_type == SPMX_SPMV_TILED) return tiled_spmv_impl(h, alpha, y, true);
+  if (h->spmv_type == SPMX_SPMV_ROUND) return round_spmv_impl(h, alpha, y, true);
   return h->spmv_type == SPMX_SPMV_HOLA ? spmx_holaspmspv(h, alpha, y) : spmx_csr5spmspv(h, alpha, y);
 }
 

@@ -79,6 +79,8 @@ struct spmx_handle_s {
   // CSR5 tile tables (csr5.cu) and tiled-SpMV tables (tiled.cu)
   void* csr5 = nullptr;
   void* tiled = nullptr;
+  // round-SpMV tables (round.cu)
+  void* round = nullptr;
   void* hybrid = nullptr;  // CSR/CSC split tables (hybrid.cu)
 
   // Hola tables

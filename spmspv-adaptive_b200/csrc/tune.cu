@@ -4,8 +4,8 @@
 // of every tunable choice on the handle's matrix with CUDA events and keeps
 // the fastest:
 //   - the load-balanced SpMV back-end: Hola (4, 8 or 16 nonzeros per thread),
-//     CSR5 (sigma: the reference's rule or 4, 8, 16, 32 nonzeros per lane)
-//     or tiled (x window width);
+//     CSR5 (sigma: the reference's rule or 4, 8, 16, 32 nonzeros per lane),
+//     tiled (x window width) or round;
 //   - the lanes per row of the naive CSR kernel and per column of the naive
 //     CSC kernel;
 //   - merge-path vs fixed-nonzero blocks for the load-balanced CSC kernel;
@@ -120,6 +120,8 @@ static int apply_params(spmx_handle_t h, const Params& p) {
     }
   } else if (p.spmv_type == SPMX_SPMV_TILED) {
     rc = spmx_tiled_preprocess(h, p.tiled_rb, p.tiled_win, 0, 0);
+  } else if (p.spmv_type == SPMX_SPMV_ROUND) {
+    rc = spmx_round_preprocess(h, p.tiled_rb);
   }
   return rc;
 }
@@ -204,6 +206,16 @@ extern "C" int spmx_autotune(spmx_handle_t h, const char* cache_path, int* spmv_
         best.tiled_win = win;
       }
       spmx_tiled_postprocess(h);
+    }
+    // round back-end (refuses very sparse row blocks; then it is skipped)
+    if (spmx_round_preprocess(h, 0) == SPMX_SUCCESS) {
+      const float t = time_us([&] { return spmx_roundspmv(h, 1.0f, y); });
+      if (t < best_t) {
+        best_t = t;
+        best.spmv_type = SPMX_SPMV_ROUND;
+        best.tiled_rb = 0;
+      }
+      spmx_round_postprocess(h);
     }
     // naive CSR lanes per row
     float bt = 1e30f;

@@ -38,7 +38,7 @@ ERR_NOT_READY = -25
 ERR_NO_DEVICE = -26
 
 VEC_SPARSE, VEC_DENSE, VEC_BITARRAY = 0, 1, 2
-SPMV_HOLA, SPMV_CSR5, SPMV_TILED = 0, 1, 2
+SPMV_HOLA, SPMV_CSR5, SPMV_TILED, SPMV_ROUND = 0, 1, 2, 3
 CSC_NAIVE, CSC_LB_MERGE, CSC_LB_TWOLAYER, CSC_BUCKET = 0, 1, 2, 3
 WB_ATOMIC, WB_SORT = 0, 1
 (K_CSC_NAIVE_SORT, K_CSC_NAIVE_ATOMIC, K_CSC_LB_SORT, K_CSC_LB_ATOMIC,
@@ -100,6 +100,11 @@ _SIGS = {
     "spmx_spmspv_batched_backward": (c_int, [P, c_int, c_int, P, P, P, c_float, P, P, P]),
     "spmx_tiledspmv": (c_int, [P, c_float, P]),
     "spmx_tiledspmspv": (c_int, [P, c_float, P]),
+    "spmx_round_preprocess": (c_int, [P, c_int]),
+    "spmx_round_postprocess": (c_int, [P]),
+    "spmx_round_info": (c_int, [P, P]),
+    "spmx_roundspmv": (c_int, [P, c_float, P]),
+    "spmx_roundspmspv": (c_int, [P, c_float, P]),
     "spmx_naivespmv": (c_int, [P, c_float, P]),
     "spmx_holaspmv": (c_int, [P, c_float, P]),
     "spmx_csr5spmv": (c_int, [P, c_float, P]),

@@ -250,6 +250,26 @@ class SpmspvHandle:
     def tiledspmspv(self, alpha, y):
         check(lib.spmx_tiledspmspv(self._h, float(alpha), _f32(y)), "tiledspmspv")
 
+    def roundPreprocess(self, rb_rows=0):
+        check(lib.spmx_round_preprocess(self._h, int(rb_rows)), "roundPreprocess")
+
+    def roundPostprocess(self):
+        check(lib.spmx_round_postprocess(self._h), "roundPostprocess")
+
+    def round_info(self):
+        """Geometry of the round format: row blocks, CTAs per cluster, rounds,
+        nonzeros per round, warps, shared y rows, shared bytes, grid."""
+        info = (ctypes.c_int * 8)()
+        check(lib.spmx_round_info(self._h, info), "round_info")
+        names = ("row_blocks", "cluster", "rounds", "round", "warps", "rmax", "smem", "grid")
+        return dict(zip(names, list(info)))
+
+    def roundspmv(self, alpha, y):
+        check(lib.spmx_roundspmv(self._h, float(alpha), _f32(y)), "roundspmv")
+
+    def roundspmspv(self, alpha, y):
+        check(lib.spmx_roundspmspv(self._h, float(alpha), _f32(y)), "roundspmspv")
+
     def set_spmv_type(self, code):
         check(lib.spmx_set_spmv_type(self._h, int(code)), "set_spmv_type")
 
@@ -395,7 +415,7 @@ class SpmspvHandle:
 
     def autotune(self, cache_path=None):
         """Time the tunable choices on this matrix and keep the fastest;
-        returns the chosen SpMV back-end (0 Hola, 1 CSR5, 2 tiled)."""
+        returns the chosen SpMV back-end (0 Hola, 1 CSR5, 2 tiled, 3 round)."""
         t = c_int()
         check(lib.spmx_autotune(self._h, cache_path.encode() if cache_path else None,
                                 ctypes.byref(t)), "autotune")

@@ -1,0 +1,132 @@
+"""Round SpMV / bitmap-gated SpMSpV (spmv_type 3) against the FP64 oracle.
+
+Tolerance (FP32 vs FP64, per row): |y32 - y64| <= 1e-5 * max(|y64|,
+sum_j |a_ij x_j|).  Cases: the SpMV suite's matrices (long rows spanning many
+rounds, empty and trailing empty rows, a single row, all rows empty), hub rows
+that span every warp of several rounds, row blocks capped small enough that
+the grid runs in several waves, a tall thin matrix, the 1M-row Zipf matrix;
+alpha values; the gated form through the dispatcher; determinism (bitwise
+equal results of repeated calls); and the preprocessing's refusals (a column
+out of range, rounds spanning too many columns), after which the handle still
+serves the other back-ends."""
+import numpy as np
+import pytest
+
+from conftest import rand_csr
+from gpu_util import dev, make_handle
+import oracle.oracle as orc
+from test_gpu_spmv import CASES
+
+pytestmark = pytest.mark.gpu
+RTOL = 1e-5
+
+
+def _extra():
+    rng = np.random.default_rng(40)
+    # hub rows of 20,000 nonzeros: several rounds, every lane of a warp part
+    lens = rng.integers(0, 12, 30000)
+    lens[[5, 17, 29000]] = 20000
+    yield "hubs", rand_csr(30000, 40000, lens=lens, seed=41)
+    yield "tall-thin", rand_csr(200000, 3, density=0.4, seed=42)
+    from spmx import gen
+    yield "zipf-64k", gen.zipf_rows(1 << 16, 1.5, 16, 5000, seed=43)
+
+
+EXTRA = list(_extra())
+ALL = CASES + EXTRA
+
+
+def _check_spmv(torch, h, A, alpha, x):
+    y64, mag = orc.spmv_f64(A.rowptr, A.col, A.val, x, alpha=alpha)
+    outs = []
+    for _ in range(2):
+        y = torch.full((A.m,), 3.0, device="cuda")
+        h.roundspmv(alpha, y)
+        h.check_device_error()
+        yh = y.cpu().numpy()
+        ok, _ = orc.within_tol(yh, y64, mag, RTOL)
+        assert ok, orc.max_scaled_err(yh, y64, mag)
+        outs.append(yh)
+    assert np.array_equal(outs[0].view(np.uint32), outs[1].view(np.uint32))  # deterministic
+
+
+@pytest.mark.parametrize("name,A", ALL, ids=[c[0] for c in ALL])
+@pytest.mark.parametrize("rb", [0, 64])
+def test_round_spmv(torch_cuda, name, A, rb):
+    torch = torch_cuda
+    h = make_handle(A, torch, csc=False, hola=False)
+    h.roundPreprocess(rb)
+    info = h.round_info()
+    assert info["cluster"] == 2 and info["round"] == 8192 and info["warps"] == 32
+    assert info["grid"] == 2 * info["row_blocks"]
+    assert info["rounds"] >= (A.nnz + 8191) // 8192
+    if rb:
+        assert info["rmax"] <= 64
+    x = np.random.default_rng(17).uniform(-1, 1, A.n).astype(np.float32)
+    h.set_x(dev(x, torch))
+    _check_spmv(torch, h, A, -1.5 if rb else 1.0, x)
+    # bitmap-gated form through the dispatcher
+    h.set_spmv_type(3)
+    rng = np.random.default_rng(2)
+    k = max(1, A.n // 30)
+    key = np.sort(rng.choice(A.n, k, replace=False)).astype(np.int32)
+    val = rng.uniform(-1, 1, k).astype(np.float32)
+    h.set_sparse_x(dev(key, torch), dev(val, torch), k)
+    h.sparse2bitarray()
+    y = torch.empty(A.m, device="cuda")
+    h.spmspv(1.0, y)
+    h.check_device_error()
+    xd, bits = orc.sparse2dense_bits(A.n, key, val)
+    y64, mag = orc.spmv_f64(A.rowptr, A.col, A.val, xd, bits=bits.view(np.int32))
+    ok, _ = orc.within_tol(y.cpu().numpy(), y64, mag, RTOL)
+    assert ok
+    # dense x through the dispatcher
+    h.set_x(dev(x, torch))
+    y = torch.empty(A.m, device="cuda")
+    h.spmv(0.5, y)
+    y64, mag = orc.spmv_f64(A.rowptr, A.col, A.val, x, alpha=0.5)
+    assert orc.within_tol(y.cpu().numpy(), y64, mag, RTOL)[0]
+    h.roundPostprocess()
+
+
+def test_round_zipf_full_size(torch_cuda):
+    torch = torch_cuda
+    from spmx import gen
+    A = gen.zipf_1m()
+    h = make_handle(A, torch, csc=False, hola=False)
+    h.roundPreprocess()
+    info = h.round_info()
+    assert info["row_blocks"] == 74 and info["grid"] == 148
+    x = np.random.default_rng(2).uniform(-1, 1, A.n).astype(np.float32)
+    h.set_x(dev(x, torch))
+    _check_spmv(torch, h, A, 1.0, x)
+
+
+def test_round_refusals_keep_handle_usable(torch_cuda):
+    torch = torch_cuda
+    from spmx import SpmxError
+    # a column outside [0, n)
+    A = rand_csr(500, 400, density=0.02, seed=44)
+    bad = A.col.copy()
+    bad[len(bad) // 2] = A.n
+    from spmx import SpmspvHandle
+    h = SpmspvHandle(A.m, A.n, A.nnz)
+    h.InputCSR(A.nnz, dev(A.rowptr, torch), dev(bad, torch), dev(A.val, torch))
+    with pytest.raises(SpmxError):
+        h.roundPreprocess()
+    with pytest.raises(SpmxError):
+        h.round_info()  # nothing kept
+    # rounds spanning more than 2^19 columns: 8,192+ nonzeros spread over 16M columns
+    B = rand_csr(4, 1 << 24, lens=[6000, 6000, 6000, 6000], seed=45)
+    hb = make_handle(B, torch, csc=False, hola=False)
+    with pytest.raises(SpmxError):
+        hb.roundPreprocess()
+    # the other back-ends still serve the handle
+    x = np.random.default_rng(3).uniform(-1, 1, B.n).astype(np.float32)
+    hb.set_x(dev(x, torch))
+    hb.holaPreprocess()
+    y = torch.empty(B.m, device="cuda")
+    hb.holaspmv(1.0, y)
+    hb.check_device_error()
+    y64, mag = orc.spmv_f64(B.rowptr, B.col, B.val, x)
+    assert orc.within_tol(y.cpu().numpy(), y64, mag, RTOL)[0]
