@@ -121,3 +121,48 @@ def test_graph_bfs(torch_cuda):
         h.check_device_error()
         assert np.array_equal(lv.cpu().numpy(), ref)
     del graph
+
+
+def test_graph_round_spmv_chain(torch_cuda):
+    """The round back-end launched as the dependent of the sparse-to-dense
+    scatter (cluster and programmatic-dependent-launch attributes) replays
+    from a graph: sparse x -> dense x -> SpMV, and the gated form."""
+    torch = torch_cuda
+    from spmx import gen
+    A = gen.zipf_rows(1 << 15, 1.5, 16, 3000, seed=24)
+    h = make_handle(A, torch, csc=False, hola=False)
+    h.roundPreprocess()
+    h.set_spmv_type(3)
+    rng = np.random.default_rng(25)
+    k = A.n // 3
+    key = np.sort(rng.choice(A.n, k, replace=False)).astype(np.int32)
+    val = rng.uniform(-1, 1, k).astype(np.float32)
+    kd, vd = dev(key, torch), dev(val, torch)
+    xdense = torch.zeros(A.n, device="cuda")
+    bits = torch.zeros((A.n + 31) // 32, dtype=torch.int32, device="cuda")
+    h.set_x(xdense)
+    h.set_bitvector(bits, (A.n + 31) // 32)
+    y0 = torch.empty(A.m, device="cuda")
+    y1 = torch.empty(A.m, device="cuda")
+
+    def work():
+        h.set_sparse_x(kd, vd, k)
+        h.sparse2dense()
+        h.spmv(1.0, y0)
+        h.sparse2bitarray()
+        h.spmspv(2.0, y1)
+
+    g, s = _capture(torch, h, work)
+    xd, bm = orc.sparse2dense_bits(A.n, key, val)
+    y64, mag = orc.spmv_f64(A.rowptr, A.col, A.val, xd)
+    z64, zmag = orc.spmv_f64(A.rowptr, A.col, A.val, xd, alpha=2.0, bits=bm.view(np.int32))
+    for _ in range(2):
+        y0.fill_(9.0)
+        y1.fill_(9.0)
+        xdense.fill_(5.0)  # the replayed scatter rebuilds x from the sparse vector
+        g.replay()
+        s.synchronize()
+        h.check_device_error()
+        assert orc.within_tol(y0.cpu().numpy(), y64, mag, RTOL)[0]
+        assert orc.within_tol(y1.cpu().numpy(), z64, zmag, RTOL)[0]
+    del g
