@@ -208,20 +208,23 @@ int spmx_tiledspmv(spmx_handle_t h, float alpha, float* d_y);
 int spmx_tiledspmspv(spmx_handle_t h, float alpha, float* d_y);
 /* Round SpMV / bitmap-gated SpMSpV (no reference counterpart; a fourth
  * back-end for the load-balanced SpMV of the selector, spmv_type 3).  Rows
- * are cut into row blocks whose y fits in shared memory (at most rb_rows
- * rows; 0 = as many as fit), one per cluster of 2 CTAs; each CTA streams half
- * of its block's nonzeros sorted by (column, row) in rounds of 8192: warps
- * gather x in column order and store each product to a row-order slot in
- * shared memory, then each warp reduces the rows it owns.  Deterministic.
- * Fails with SPMX_ERR_INVALID_VALUE (the other back-ends still apply) when a
- * column index is out of range, when a round of 8192 nonzeros spans 2^19
- * columns or more (a very sparse row block), or when row blocks x columns
+ * are cut into row blocks (at most rb_rows rows; 0 = as many as fit), one per
+ * cluster of 2 CTAs; each CTA streams half of its block's nonzeros sorted by
+ * (column, row) in rounds of 4096.  Every row owns as many shared-memory
+ * accumulators as it has nonzeros in its densest round; the k-th nonzero of
+ * a row in a round adds into the row's k-th accumulator with a plain
+ * read-modify-write (all distinct within a round), one barrier per round;
+ * at the end each row's accumulators are summed.  Deterministic.  Fails with
+ * SPMX_ERR_INVALID_VALUE (the other back-ends still apply) when a column
+ * index is out of range, when 128 consecutive nonzeros of a row block span
+ * 2^16 columns or more (a very sparse row block), when a row block needs
+ * more accumulators than shared memory holds, or when row blocks x columns
  * need a sort key of more than 32 bits. */
 int spmx_round_preprocess(spmx_handle_t h, int rb_rows);
 int spmx_round_postprocess(spmx_handle_t h);
 /* geometry chosen by spmx_round_preprocess: info[0..7] = row blocks, CTAs
- * per cluster, rounds, nonzeros per round, warps per CTA, shared y rows,
- * shared bytes, grid */
+ * per cluster, rounds, nonzeros per round, accumulator slots per CTA, shared
+ * y rows, shared bytes, grid */
 int spmx_round_info(spmx_handle_t h, int* info);
 int spmx_roundspmv(spmx_handle_t h, float alpha, float* d_y);
 int spmx_roundspmspv(spmx_handle_t h, float alpha, float* d_y);

@@ -7,38 +7,32 @@
 // windows in shared memory, pays a producer/consumer handshake per (row
 // block, x window) tile.  Here the nonzeros of a row block are streamed in
 // COLUMN order, so the 32 lanes of a warp gather x from a few neighbouring
-// cache lines, and the accumulation into y is made race-free without atomics
-// by a transpose through shared memory:
+// cache lines, and the accumulation into y needs neither atomics nor a
+// reduction pass:
 //
-//   - rows are cut into row blocks whose y fits in shared memory; a row block
-//     is processed by a cluster of 2 CTAs, each taking one half (in column
-//     order) of the block's nonzeros, sorted by (column, row);
-//   - a CTA's nonzeros are cut into rounds of E = 8192.  Phase 1: each of the
-//     32 warps takes 256 consecutive nonzeros of the round (16-byte loads of
-//     the stream, lanes interleaved so that consecutive lanes hold
-//     consecutive nonzeros), gathers x, multiplies and stores the product
-//     into the nonzero's slot of a shared product buffer.  The slots put the
-//     round's products in row order, the rows of each warp together, each
-//     warp's part lane-interleaved (entry j of lane l's contiguous range at
-//     32 j + l);
-//   - after a CTA barrier, phase 2: every warp reduces the products of the
-//     rows it owns (fixed row ranges of equal nonzero counts) into the shared
-//     y: a lane adds each run of equal rows that ends inside its range, and
-//     the runs still open at the range ends are summed with a segmented scan.
-//     No two lanes or warps ever update one row at once, and every row's
-//     additions happen in a fixed order: the result is deterministic;
-//   - the products are double-buffered, so one barrier per round suffices;
-//     the row indices of a round (2 bytes per nonzero, in slot order) arrive
-//     by a bulk copy issued one round ahead, the stream words of the next
-//     round are loaded during the current one and L2 prefetches run three
-//     rounds ahead;
-//   - at the end the 2 CTAs of a cluster add their partial y vectors in rank
-//     order through distributed shared memory and store each row once.
+//   - rows are cut into row blocks; a row block is processed by a cluster of
+//     2 CTAs, each taking one half (in column order) of the block's
+//     nonzeros, sorted by (column, row) and cut into rounds of E = 4096;
+//   - every row owns as many shared-memory accumulators ("slots") as it has
+//     nonzeros in any single round; the k-th nonzero of a row inside a round
+//     (column order) adds into the row's k-th slot.  Within a round every
+//     nonzero therefore has its own slot, so each lane adds v * x[c] into
+//     its slot with a plain read-modify-write, and one CTA barrier per round
+//     separates the rounds.  A row of a few nonzeros has one slot; a hub row
+//     has one per nonzero it has in its densest round;
+//   - each of the 32 warps takes 128 consecutive nonzeros of a round (16-byte
+//     loads of the stream, interleaved so that consecutive lanes hold
+//     consecutive nonzeros); the gathers of round k + 1 are issued before the
+//     additions of round k, so their latency overlaps the round's barrier,
+//     and the stream is loaded two rounds ahead;
+//   - at the end each CTA sums every row's slots in slot order, and the 2
+//     CTAs of a cluster add their row sums in rank order through distributed
+//     shared memory; each row is stored once.  Every addition has a fixed
+//     order: the result is deterministic.
 //
-// Stream per nonzero: a 32-bit word (column offset from the round's first
-// column << 13 | slot), the value (4 bytes) and the local row (2 bytes).
-// Every wait is bounded: a timeout sets the device error word and the kernel
-// keeps every thread on the same barrier sequence until it returns.
+// Stream per nonzero: a 32-bit word (slot << 16 | column offset from the
+// first column of its 128-nonzero chunk) and the value: 8 bytes, as CSR, plus
+// one chunk base column per 128 nonzeros.
 #include <algorithm>
 #include <cooperative_groups.h>
 #include <string>
@@ -53,243 +47,125 @@ namespace cg = cooperative_groups;
 
 namespace spmx {
 
-constexpr int kRoundE = 8192;             // nonzeros per round
-constexpr int kRoundSlotBits = 13;        // log2(kRoundE)
-constexpr int kRoundNW = 32;              // warps per CTA
-constexpr int kRoundCS = 2;               // CTAs per cluster (per row block)
-constexpr int kRoundPL = kRoundE / (kRoundNW * 32);  // phase-1 nonzeros per lane
-constexpr unsigned kRoundSpan = 1u << (32 - kRoundSlotBits);  // column offsets must stay below
-constexpr long long kRoundSpin = 1LL << 22;
-static_assert(kRoundPL % 4 == 0, "16-byte stream loads");
+constexpr int kRoundE = 4096;     // nonzeros per round
+constexpr int kRoundChunk = 128;  // nonzeros per chunk (one base column each)
+constexpr int kRoundNW = 32;      // warps per CTA
+constexpr int kRoundCS = 2;       // CTAs per cluster (per row block)
+constexpr int kRoundCPW = kRoundE / kRoundChunk / kRoundNW;  // chunks per warp per round
+constexpr int kRoundDummy = 32;   // padding slots after the real ones (one per lane)
+static_assert(kRoundCPW >= 1, "round geometry");
 
 struct RoundTables {
-  int nrb = 0, grid = 0, rmax = 0, nrounds = 0;
+  int nrb = 0, grid = 0, rmax = 0, nrounds = 0, nslots = 0;
   size_t smem = 0;
-  int* rb_row = nullptr;     // nrb + 1 row block boundaries
-  int* cta_round = nullptr;  // grid + 1: rounds of CTA c are [cta_round[c], cta_round[c + 1])
-  unsigned* packed = nullptr;        // nrounds * E stream words (phase-1 order, interleaved)
-  float* val = nullptr;              // nrounds * E values (same order)
-  unsigned short* row16 = nullptr;   // nrounds * E local rows (slot order)
-  int* rbase = nullptr;              // nrounds first columns
-  int* roff = nullptr;               // nrounds * (NW + 1) warp part offsets (slot order)
+  int* rb_row = nullptr;          // nrb + 1 row block boundaries
+  int* cta_round = nullptr;       // grid + 1: rounds of CTA c are [cta_round[c], cta_round[c + 1])
+  unsigned* packed = nullptr;     // nrounds * E stream words (chunk-interleaved)
+  float* val = nullptr;           // nrounds * E values (same order)
+  int* cbase = nullptr;           // nrounds * E / 128 chunk base columns
+  int* vbg = nullptr;             // m + 1 slot prefix over all rows
 };
 
 static RoundTables* rtab(spmx_handle_t h) { return reinterpret_cast<RoundTables*>(h->round); }
 
 namespace {
 
-__device__ __forceinline__ unsigned rsa(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
-
-__device__ __forceinline__ bool round_wait(unsigned long long* b, int parity) {
-  for (long long it = 0; it < kRoundSpin; ++it) {
-    unsigned done;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-        "selp.u32 %0, 1, 0, p;\n\t}"
-        : "=r"(done)
-        : "r"(rsa(b)), "r"(parity)
-        : "memory");
-    if (done) return true;
-  }
-  return false;
-}
-
-// bulk copy of one round's rows into shared memory, counted on barrier b
-__device__ __forceinline__ void round_copy_rows(unsigned short* dst, const unsigned short* src,
-                                                unsigned long long* b) {
-  constexpr unsigned bytes = 2u * kRoundE;
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(rsa(b)), "r"(bytes) : "memory");
-  asm volatile(
-      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(rsa(dst)),
-      "l"(src), "r"(bytes), "r"(rsa(b))
-      : "memory");
-}
-
-__device__ __forceinline__ void round_l2_prefetch(const void* p, unsigned bytes) {
-  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
-}
-
-// A warp reduces its part [lo, hi) of a round's products (row order,
-// lane-interleaved: entry j of lane l's contiguous range at lo + 32 j + l;
-// the first (hi - lo) % 32 lanes hold one entry more) into ys.  A run of
-// equal rows that ends inside a lane's range is added by that lane when it
-// ends; no other lane ends it, and the warp's instructions are ordered, so
-// two lanes never update one row in one instruction.  The runs open at the
-// range ends have non-decreasing rows across the lanes; a segmented scan sums
-// each group and its last lane adds the sum.
-template <int G>
-__device__ __forceinline__ void round_warp_reduce(int lo, int hi, const unsigned short* __restrict__ R,
-                                                  const float* __restrict__ Pp, float* __restrict__ ys) {
-  const int lane = threadIdx.x & 31;
-  const int len = hi - lo;
-  if (len <= 0) return;  // warp-uniform
-  const int per = len >> 5, rem = len & 31;
-  const int cnt = per + (lane < rem ? 1 : 0);
-  int cur = -1;
-  float acc = 0.f;
-  for (int j0 = 0; j0 < cnt; j0 += G) {
-    const int ng = min(G, cnt - j0);
-    int rw[G];
-    float pr[G];
-#pragma unroll
-    for (int j = 0; j < G; ++j) {
-      rw[j] = j < ng ? (int)R[lo + 32 * (j0 + j) + lane] : 0;
-      pr[j] = j < ng ? Pp[lo + 32 * (j0 + j) + lane] : 0.f;
-    }
-#pragma unroll
-    for (int j = 0; j < G; ++j) {
-      if (j < ng) {
-        if (rw[j] != cur) {
-          if (cur >= 0) ys[cur] += acc;
-          cur = rw[j];
-          acc = pr[j];
-        } else {
-          acc += pr[j];
-        }
-      }
-    }
-  }
-  float S = acc;
-#pragma unroll
-  for (int d = 1; d < 32; d <<= 1) {
-    const float oS = __shfl_up_sync(0xffffffffu, S, d);
-    const int oc = __shfl_up_sync(0xffffffffu, cur, d);
-    if (lane >= d && oc == cur) S += oS;
-  }
-  const int nc = __shfl_down_sync(0xffffffffu, cur, 1);
-  if (cur >= 0 && (lane == 31 || nc != cur)) ys[cur] += S;
-  __syncwarp();
-}
-
-// shared memory: 2 mbarriers (128 bytes), products 2 x E floats, rows 2 x E
-// shorts, y (rmax floats)
-__host__ __device__ constexpr size_t round_smem_fixed() { return 128 + 4 * 2 * kRoundE + 2 * 2 * kRoundE; }
+// shared memory: nslots accumulators (rounded to 4), then rmax row sums
+size_t round_smem(int nslots, int rmax) { return 4 * (size_t)(((nslots + 3) & ~3) + rmax); }
 
 template <bool GATED>
 __global__ void __launch_bounds__(kRoundNW * 32, 1)
-round_spmv_kernel(const int* __restrict__ rb_row, const int* __restrict__ cta_round,
-                  const unsigned* __restrict__ packed, const float* __restrict__ val,
-                  const unsigned short* __restrict__ row16, const int* __restrict__ rbase,
-                  const int* __restrict__ roff, const float* __restrict__ x, const unsigned* __restrict__ xbits,
-                  float alpha, float* __restrict__ y, int* err) {
-  constexpr int E = kRoundE, NW = kRoundNW, PL = kRoundPL, DB = kRoundSlotBits;
-  extern __shared__ __align__(128) unsigned char smem[];
-  unsigned long long* bars = reinterpret_cast<unsigned long long*>(smem);
-  float* P = reinterpret_cast<float*>(smem + 128);
-  unsigned short* Rs = reinterpret_cast<unsigned short*>(P + 2 * E);
-  float* ys = reinterpret_cast<float*>(Rs + 2 * E);
+round_spmv_kernel(int nslots, const int* __restrict__ rb_row, const int* __restrict__ cta_round,
+                  const uint4* __restrict__ packed, const float4* __restrict__ val,
+                  const int* __restrict__ cbase, const int* __restrict__ vbg, const float* __restrict__ x,
+                  const unsigned* __restrict__ xbits, float alpha, float* __restrict__ y) {
+  constexpr int E = kRoundE, CPW = kRoundCPW, NW = kRoundNW;
+  extern __shared__ __align__(16) float ys[];
+  float* F = ys + ((nslots + 3) & ~3);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int rb = blockIdx.x / kRoundCS;
   const int row0 = __ldg(rb_row + rb), rows = __ldg(rb_row + rb + 1) - row0;
-  const int rows4 = (rows + 3) & ~3;
-  for (int r = threadIdx.x; r < rows4; r += blockDim.x) ys[r] = 0.f;
+  for (int r = threadIdx.x; r < nslots; r += blockDim.x) ys[r] = 0.f;
   const int k0 = __ldg(cta_round + blockIdx.x), k1 = __ldg(cta_round + blockIdx.x + 1);
-  if (threadIdx.x == 0) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(rsa(bars)) : "memory");
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(rsa(bars + 1)) : "memory");
-    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-  }
-  __syncthreads();
+  // two register sets, used alternately: a round's stream words, values,
+  // chunk bases and gathered x
+  uint4 pa[CPW], pb[CPW];
+  float4 va[CPW], vb[CPW];
+  int ba[CPW], bb[CPW];
+  float xa[CPW][4], xb[CPW][4];
+  auto load = [&](int q, uint4 (&p)[CPW], float4 (&v)[CPW], int (&b)[CPW]) {
+#pragma unroll
+    for (int u = 0; u < CPW; ++u) {
+      const size_t c = (size_t)q * (E / kRoundChunk) + warp * CPW + u;
+      p[u] = __ldcs(packed + c * 32 + lane);
+      v[u] = __ldcs(val + c * 32 + lane);
+      b[u] = __ldg(cbase + c);
+    }
+  };
+  auto gather = [&](const uint4 (&p)[CPW], const int (&b)[CPW], float (&xv)[CPW][4]) {
+#pragma unroll
+    for (int u = 0; u < CPW; ++u) {
+      const unsigned w[4] = {p[u].x, p[u].y, p[u].z, p[u].w};
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const int c = b[u] + (int)(w[j] & 0xffffu);
+        float xx = __ldg(x + c);
+        if (GATED && !((__ldg(xbits + (c >> 5)) >> (c & 31)) & 1u)) xx = 0.f;
+        xv[u][j] = xx;
+      }
+    }
+  };
+  // the stream does not depend on the grid this one is launched after
+  if (k0 < k1) load(k0, pa, va, ba);
+  if (k0 + 1 < k1) load(k0 + 1, pb, vb, bb);
   // launched as a programmatic dependent of the grid that writes x: nothing
   // above touches x or y
   asm volatile("griddepcontrol.wait;" ::: "memory");
-  if (threadIdx.x == 0 && k0 < k1) {
-    round_copy_rows(Rs, row16 + (size_t)k0 * E, bars);
-    for (int q = k0 + 1; q < min(k1, k0 + 4); ++q) {
-      round_l2_prefetch(packed + (size_t)q * E, 4u * E);
-      round_l2_prefetch(val + (size_t)q * E, 4u * E);
-      round_l2_prefetch(row16 + (size_t)q * E, 2u * E);
-    }
-  }
-  unsigned pw[PL];
-  float pv[PL];
-  int nbase = 0, nlo = 0, nhi = 0;
-  auto load_round = [&](int q) {
-#pragma unroll
-    for (int i = 0; i < PL / 4; ++i) {
-      const size_t e = (size_t)q * E + warp * (E / NW) + 128 * i + 4 * lane;
-      const uint4 a = __ldcs(reinterpret_cast<const uint4*>(packed + e));
-      const float4 v = __ldcs(reinterpret_cast<const float4*>(val + e));
-      pw[4 * i] = a.x;
-      pw[4 * i + 1] = a.y;
-      pw[4 * i + 2] = a.z;
-      pw[4 * i + 3] = a.w;
-      pv[4 * i] = v.x;
-      pv[4 * i + 1] = v.y;
-      pv[4 * i + 2] = v.z;
-      pv[4 * i + 3] = v.w;
-    }
-    nbase = __ldg(rbase + q);
-    nlo = __ldg(roff + (size_t)q * (NW + 1) + warp);
-    nhi = __ldg(roff + (size_t)q * (NW + 1) + warp + 1);
-  };
-  if (k0 < k1) load_round(k0);
-  bool timed_out = false;
-  for (int k = k0; k < k1; ++k) {
-    const int b = (k - k0) & 1;
-    float* Pk = P + b * E;
-    const int base = nbase, lo = nlo, hi = nhi;
-    // phase 1: gather in column order, products to their row-order slots
-    float xv[PL];
-#pragma unroll
-    for (int i = 0; i < PL; ++i) xv[i] = __ldg(x + base + (int)(pw[i] >> DB));
-    unsigned dst[PL];
-    float pr[PL];
-#pragma unroll
-    for (int i = 0; i < PL; ++i) {
-      dst[i] = pw[i] & (E - 1);
-      float p = pv[i] * xv[i];
-      if (GATED) {
-        const int c = base + (int)(pw[i] >> DB);
-        if (!((__ldg(xbits + (c >> 5)) >> (c & 31)) & 1u)) p = 0.f;
-      }
-      pr[i] = p;
-    }
-    if (k + 1 < k1) load_round(k + 1);
-#pragma unroll
-    for (int i = 0; i < PL; ++i) Pk[dst[i]] = pr[i];
-    __syncthreads();
-    // every warp has finished phase 2 of round k - 1: refill its row buffer
-    if (threadIdx.x == 0 && k + 1 < k1) {
-      round_copy_rows(Rs + (1 - b) * E, row16 + (size_t)(k + 1) * E, bars + (1 - b));
-      if (k + 4 < k1) {
-        round_l2_prefetch(packed + (size_t)(k + 4) * E, 4u * E);
-        round_l2_prefetch(val + (size_t)(k + 4) * E, 4u * E);
-        round_l2_prefetch(row16 + (size_t)(k + 4) * E, 2u * E);
-      }
-    }
-    // phase 2: every lane waits for the rows (acquire); a timeout skips the
-    // reduction but keeps the barrier sequence
-    const bool got = __all_sync(0xffffffffu, round_wait(bars + b, ((k - k0) >> 1) & 1));
-    if (got) {
-      round_warp_reduce<8>(lo, hi, Rs + b * E, Pk, ys);
-    } else if (!timed_out) {
-      timed_out = true;
-      if (lane == 0) flag_error(err, kDevErrTimeout);
-    }
-  }
+  if (k0 < k1) gather(pa, ba, xa);
   __syncthreads();
+  // one round: issue the next round's gathers, add this round into its
+  // slots, load the stream two rounds ahead into this round's registers
+  auto step = [&](int k, uint4 (&pc)[CPW], float4 (&vc)[CPW], int (&bc)[CPW], float (&xc)[CPW][4],
+                  const uint4 (&pn)[CPW], const int (&bn)[CPW], float (&xn)[CPW][4]) {
+    if (k + 1 < k1) gather(pn, bn, xn);
+#pragma unroll
+    for (int u = 0; u < CPW; ++u) {
+      const unsigned w[4] = {pc[u].x, pc[u].y, pc[u].z, pc[u].w};
+      const float vv[4] = {vc[u].x, vc[u].y, vc[u].z, vc[u].w};
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const int s = (int)(w[j] >> 16);
+        ys[s] = fmaf(vv[j], xc[u][j], ys[s]);
+      }
+    }
+    if (k + 2 < k1) load(k + 2, pc, vc, bc);
+    __syncthreads();
+  };
+  for (int k = k0; k < k1; k += 2) {
+    step(k, pa, va, ba, xa, pb, bb, xb);
+    if (k + 1 < k1) step(k + 1, pb, vb, bb, xb, pa, ba, xa);
+  }
+  // each row's slots, summed in slot order
+  const int base0 = __ldg(vbg + row0);
+  for (int r = threadIdx.x; r < rows; r += blockDim.x) {
+    const int s0 = __ldg(vbg + row0 + r) - base0, s1 = __ldg(vbg + row0 + r + 1) - base0;
+    float acc = 0.f;
+    for (int s = s0; s < s1; ++s) acc += ys[s];
+    F[r] = acc;
+  }
+  // the cluster's row sums, added in rank order; each CTA stores a slice
   cg::cluster_group cl = cg::this_cluster();
   cl.sync();
   const int rank = (int)cl.block_rank();
-  const int slice = (((rows + kRoundCS - 1) / kRoundCS) + 3) & ~3;
+  const int slice = (rows + kRoundCS - 1) / kRoundCS;
   const int r0 = rank * slice, r1 = min(rows, r0 + slice);
-  for (int r = r0 + 4 * (int)threadIdx.x; r < r1; r += 4 * (int)blockDim.x) {
-    float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
-    for (int q = 0; q < kRoundCS; ++q) {
-      const float4 v = *reinterpret_cast<const float4*>(cl.map_shared_rank(ys + r, q));
-      acc.x += v.x;
-      acc.y += v.y;
-      acc.z += v.z;
-      acc.w += v.w;
-    }
-    const float a4[4] = {acc.x, acc.y, acc.z, acc.w};
+  for (int r = r0 + (int)threadIdx.x; r < r1; r += blockDim.x) {
+    float acc = 0.f;
 #pragma unroll
-    for (int j = 0; j < 4; ++j)
-      if (r + j < r1) y[row0 + r + j] = alpha * a4[j];
+    for (int q = 0; q < kRoundCS; ++q) acc += *cl.map_shared_rank(F + r, q);
+    y[row0 + r] = alpha * acc;
   }
-  cl.sync();  // peers read this CTA's shared y until here
+  cl.sync();  // peers read this CTA's row sums until here
 }
 
 // ---------------------------------------------------------------------------
@@ -346,90 +222,89 @@ __global__ void round_bounds_kernel(int nnz, const unsigned* __restrict__ skey, 
 }
 
 // one CTA per round: the second sort's keys (round << 16 | local row, stable
-// over the round's column order) and positions; the round's first column;
-// a column span beyond the slot word's offset field sets flags bit 1
+// over the round's column order) and the column-order positions
 __global__ void round_key2_kernel(const int* __restrict__ rstart, const int* __restrict__ rlen,
-                                  const unsigned* __restrict__ skey, const unsigned* __restrict__ slrow, unsigned cmask,
-                                  unsigned* __restrict__ key2, unsigned* __restrict__ pos2, int* __restrict__ rbase,
-                                  int* __restrict__ flags) {
+                                  const unsigned* __restrict__ slrow, unsigned* __restrict__ key2,
+                                  unsigned* __restrict__ pos2) {
   const int q = blockIdx.x;
   const int s = __ldg(rstart + q), len = __ldg(rlen + q);
   for (int i = threadIdx.x; i < len; i += blockDim.x) {
     key2[s + i] = ((unsigned)q << 16) | __ldg(slrow + s + i);
     pos2[s + i] = (unsigned)i;
   }
-  if (threadIdx.x == 0) {
-    const unsigned c0 = __ldg(skey + s) & cmask, c1 = __ldg(skey + s + len - 1) & cmask;
-    rbase[q] = (int)c0;
-    if (c1 - c0 >= kRoundSpan) atomicOr(flags, 2);
+}
+
+// one CTA per round: the occurrence of every nonzero among its row's
+// nonzeros in the round (column order), stored by column-order position, and
+// the row's slot count (the largest occurrence + 1 over all rounds)
+__global__ void round_occurrence_kernel(const int* __restrict__ rstart, const int* __restrict__ rlen,
+                                        const int* __restrict__ rrb, const int* __restrict__ rb_row,
+                                        const unsigned* __restrict__ key2, const unsigned* __restrict__ pos2,
+                                        int* __restrict__ occ, int* __restrict__ slots_per_row) {
+  const int q = blockIdx.x;
+  const int s = __ldg(rstart + q), len = __ldg(rlen + q);
+  const int row0 = __ldg(rb_row + __ldg(rrb + q));
+  for (int t = threadIdx.x; t < len; t += blockDim.x) {
+    const unsigned k = __ldg(key2 + s + t);
+    int lo = 0, hi = t;  // first entry of the round with this key
+    while (lo < hi) {
+      const int mid = (lo + hi) >> 1;
+      if (__ldg(key2 + s + mid) < k) lo = mid + 1;
+      else hi = mid;
+    }
+    const int o = t - lo;
+    occ[s + (int)__ldg(pos2 + s + t)] = o;
+    atomicMax(slots_per_row + row0 + (int)(k & 0xffffu), o + 1);
   }
 }
 
-// storage position of phase-1 position p: each 128-entry block is stored so
-// that a lane's 16-byte word holds entries l, l + 32, l + 64, l + 96
+// storage position of chunk-local position p: a lane's 16-byte word holds
+// entries l, l + 32, l + 64, l + 96 of the chunk
 __device__ __forceinline__ int round_vperm(int p) {
   const int blk = p >> 7, c = (p >> 5) & 3, l = p & 31;
   return (blk << 7) + 4 * l + c;
 }
 
-// one CTA per round: warp part offsets (row order), slots, and the streams
+// one CTA per round: stream words (slot << 16 | column offset from the
+// chunk's first column), values and chunk bases; a chunk spanning 2^16
+// columns or more sets flags bit 1
 __global__ void __launch_bounds__(256)
 round_layout_kernel(const int* __restrict__ rstart, const int* __restrict__ rlen, const int* __restrict__ rrb,
-                    const int* __restrict__ wsp, const unsigned* __restrict__ skey, const unsigned* __restrict__ sval,
-                    unsigned cmask, const unsigned* __restrict__ key2, const unsigned* __restrict__ pos2,
-                    const int* __restrict__ rbase, unsigned* __restrict__ packed, float* __restrict__ val,
-                    unsigned short* __restrict__ row16, int* __restrict__ roff) {
-  constexpr int NW = kRoundNW, E = kRoundE, DB = kRoundSlotBits;
-  __shared__ int off[NW + 1];
+                    const int* __restrict__ rb_row, const int* __restrict__ vbg, const unsigned* __restrict__ skey,
+                    const unsigned* __restrict__ slrow, const unsigned* __restrict__ sval, unsigned cmask,
+                    const int* __restrict__ occ, int dummy, unsigned* __restrict__ packed, float* __restrict__ val,
+                    int* __restrict__ cbase, int* __restrict__ flags) {
+  constexpr int E = kRoundE;
   const int q = blockIdx.x;
   const int s = __ldg(rstart + q), len = __ldg(rlen + q);
-  const int base = __ldg(rbase + q);
-  const int* ws = wsp + (size_t)__ldg(rrb + q) * (NW + 1);
-  if (threadIdx.x <= NW) {
-    // first entry of the round (row order) whose local row >= the split
-    const unsigned split = (unsigned)__ldg(ws + threadIdx.x);
-    int lo = 0, hi = len;
-    while (lo < hi) {
-      const int mid = (lo + hi) >> 1;
-      if ((__ldg(key2 + s + mid) & 0xffffu) < split) lo = mid + 1;
-      else hi = mid;
-    }
-    off[threadIdx.x] = threadIdx.x == NW ? len : lo;
-    roff[(size_t)q * (NW + 1) + threadIdx.x] = threadIdx.x == NW ? len : lo;
-  }
-  __syncthreads();
+  const int row0 = __ldg(rb_row + __ldg(rrb + q));
+  const int vb0 = __ldg(vbg + row0);
   const size_t o = (size_t)q * E;
-  for (int t = threadIdx.x; t < E; t += blockDim.x) {
-    if (t < len) {
-      // row-order index t: owner warp, lane range, slot
-      int w = 0;
-      while (w < NW - 1 && off[w + 1] <= t) ++w;
-      const int L = off[w + 1] - off[w], u = t - off[w];
-      const int per = L >> 5, rem = L & 31;
-      int lane, j;
-      if (u < rem * (per + 1)) {
-        lane = u / (per + 1);
-        j = u - lane * (per + 1);
-      } else {
-        const int u2 = u - rem * (per + 1);
-        lane = rem + u2 / per;
-        j = u2 - (lane - rem) * per;
-      }
-      const int slot = off[w] + 32 * j + lane;
-      const int pos = (int)__ldg(pos2 + s + t);
-      row16[o + slot] = (unsigned short)(__ldg(key2 + s + t) & 0xffffu);
-      const unsigned c = __ldg(skey + s + pos) & cmask;
-      const int sp = round_vperm(pos);
-      packed[o + sp] = ((c - (unsigned)base) << DB) | (unsigned)slot;
-      val[o + sp] = __uint_as_float(__ldg(sval + s + pos));
+  for (int p = threadIdx.x; p < E; p += blockDim.x) {
+    const int first = p & ~(kRoundChunk - 1);  // the chunk's first position
+    const unsigned cb = first < len ? (__ldg(skey + s + first) & cmask) : 0u;
+    const int sp = round_vperm(p);
+    if (p == first) cbase[o / kRoundChunk + p / kRoundChunk] = (int)cb;
+    if (p < len) {
+      const int i = s + p;
+      const unsigned c = __ldg(skey + i) & cmask;
+      const int slot = __ldg(vbg + row0 + (int)__ldg(slrow + i)) - vb0 + __ldg(occ + i);
+      if (c - cb >= 65536u) atomicOr(flags, 2);
+      packed[o + sp] = ((unsigned)slot << 16) | ((c - cb) & 0xffffu);
+      val[o + sp] = __uint_as_float(__ldg(sval + i));
     } else {
-      // padding: the unused slots [len, E), column offset 0, value 0
-      const int sp = round_vperm(t);
-      packed[o + sp] = (unsigned)t;
+      // padding: a lane's own dummy slot, the chunk's base column, value 0
+      packed[o + sp] = (unsigned)(dummy + (p & 31)) << 16;
       val[o + sp] = 0.f;
-      row16[o + t] = 0;
     }
   }
+}
+
+// slots of each row block: out[b] = vbg[rb_row[b + 1]] - vbg[rb_row[b]]
+__global__ void round_block_slots_kernel(int nrb, const int* __restrict__ rb_row, const int* __restrict__ vbg,
+                                         int* __restrict__ out) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b < nrb) out[b] = __ldg(vbg + __ldg(rb_row + b + 1)) - __ldg(vbg + __ldg(rb_row + b));
 }
 
 int bits_for(long long v) {  // bits to hold values in [0, v)
@@ -465,9 +340,8 @@ extern "C" int spmx_round_postprocess(spmx_handle_t h) {
   dfree(t->cta_round);
   dfree(t->packed);
   dfree(t->val);
-  dfree(t->row16);
-  dfree(t->rbase);
-  dfree(t->roff);
+  dfree(t->cbase);
+  dfree(t->vbg);
   delete t;
   h->round = nullptr;
   return SPMX_SUCCESS;
@@ -478,12 +352,12 @@ extern "C" int spmx_round_preprocess(spmx_handle_t h, int rb_rows) {
   if (!h->has_csr || (!h->val && h->nnz > 0))
     return set_error(SPMX_ERR_NOT_READY, "round SpMV needs the CSR input with values");
   if (rb_rows < 0) return set_error(SPMX_ERR_INVALID_VALUE, "round SpMV: rb_rows must be >= 0");
-  constexpr int NW = kRoundNW, E = kRoundE;
+  constexpr int E = kRoundE;
   int optin = 0;
   cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, h->device);
-  const long long fixed = (long long)round_smem_fixed() + round_static_smem();
-  long long rcap = ((long long)optin - fixed) / 4;
-  rcap = std::min<long long>(rcap & ~3LL, 65532);
+  const long long avail = (long long)optin - round_static_smem();
+  // every nonempty row needs a slot and a row sum: at most avail / 8 rows
+  long long rcap = std::min<long long>((avail / 8) & ~3LL, 65532);
   if (rb_rows > 0) rcap = std::min<long long>(rcap, std::max(4, (rb_rows + 3) & ~3));
   if (rcap < 4) return set_error(SPMX_ERR_INVALID_VALUE, "round SpMV: no shared memory left for y");
   spmx_round_postprocess(h);
@@ -520,33 +394,16 @@ extern "C" int spmx_round_preprocess(spmx_handle_t h, int rb_rows) {
   for (int k = 0; k < nrb; ++k) rmax = std::max(rmax, rbr[k + 1] - rbr[k]);
   if (rmax > rcap) return set_error(SPMX_ERR_INVALID_VALUE, "round SpMV: row blocks do not fit shared memory");
   rmax = (rmax + 3) & ~3;
-  // warp row splits inside each row block (about equal nonzeros)
-  std::vector<int> wsp((size_t)nrb * (NW + 1), 0);
-  for (int k = 0; k < nrb; ++k) {
-    const int a = rbr[k], b = rbr[k + 1];
-    const long long z0 = rp[a], z1 = rp[b];
-    for (int w = 0; w <= NW; ++w) {
-      int r;
-      if (w == 0) r = a;
-      else if (w == NW) r = b;
-      else
-        r = (int)(std::lower_bound(rp.begin() + a, rp.begin() + b, (int)(z0 + (z1 - z0) * w / NW)) - rp.begin());
-      wsp[(size_t)k * (NW + 1) + w] = std::max(r - a, w ? wsp[(size_t)k * (NW + 1) + w - 1] : 0);
-    }
-  }
   RoundTables* t = new RoundTables();
   h->round = t;
   t->nrb = nrb;
   t->grid = nrb * kRoundCS;
   t->rmax = rmax;
-  t->smem = round_smem_fixed() + 4 * (size_t)rmax;
-  round_set_smem<false>(t->smem);
-  round_set_smem<true>(t->smem);
 
   const size_t b4 = 4 * (size_t)std::max(nnz, 1);
   unsigned *k0 = nullptr, *k1 = nullptr, *a0 = nullptr, *a1 = nullptr, *v0 = nullptr, *v1 = nullptr;
   unsigned *q0 = nullptr, *q1 = nullptr;
-  int *hist = nullptr, *hoff = nullptr, *d_wsp = nullptr, *flags = nullptr, *d_bounds = nullptr;
+  int *hist = nullptr, *hoff = nullptr, *flags = nullptr, *d_bounds = nullptr, *spr = nullptr;
   const size_t hn = radix_hist_ints(std::max(nnz, 1));
   int rc = SPMX_SUCCESS;
   rc = rc ? rc : dalloc((void**)&k0, b4, "round keys");
@@ -559,16 +416,17 @@ extern "C" int spmx_round_preprocess(spmx_handle_t h, int rb_rows) {
   rc = rc ? rc : dalloc((void**)&q1, b4, "round row keys alt");
   rc = rc ? rc : dalloc((void**)&hist, 4 * hn, "round hist");
   rc = rc ? rc : dalloc((void**)&hoff, 4 * hn, "round hist off");
-  rc = rc ? rc : dalloc((void**)&d_wsp, 4 * wsp.size(), "round warp splits");
   rc = rc ? rc : dalloc((void**)&flags, 4 * sizeof(int), "round flags");
   rc = rc ? rc : dalloc((void**)&d_bounds, 4 * ((size_t)nrb + 1), "round block bounds");
+  rc = rc ? rc : dalloc((void**)&spr, 4 * ((size_t)m + 1), "round slots per row");
   rc = rc ? rc : dalloc((void**)&t->rb_row, 4 * ((size_t)nrb + 1), "round row blocks");
+  rc = rc ? rc : dalloc((void**)&t->vbg, 4 * ((size_t)m + 1), "round slot prefix");
   std::vector<int> bounds((size_t)nrb + 1, 0);
   unsigned *skey = nullptr, *slrow = nullptr, *sval = nullptr;
   if (!rc) {
     cudaMemcpyAsync(t->rb_row, rbr.data(), 4 * ((size_t)nrb + 1), cudaMemcpyHostToDevice, st);
-    cudaMemcpyAsync(d_wsp, wsp.data(), 4 * wsp.size(), cudaMemcpyHostToDevice, st);
     cudaMemsetAsync(flags, 0, 4 * sizeof(int), st);
+    cudaMemsetAsync(spr, 0, 4 * ((size_t)m + 1), st);
   }
   if (!rc && nnz > 0) {
     note_launch();
@@ -614,31 +472,31 @@ extern "C" int spmx_round_preprocess(spmx_handle_t h, int rb_rows) {
   }
   const int nrounds = (int)rstart.size();
   t->nrounds = nrounds;
-  int *d_rstart = nullptr, *d_rlen = nullptr, *d_rrb = nullptr;
+  int *d_rstart = nullptr, *d_rlen = nullptr, *d_rrb = nullptr, *occ = nullptr, *d_bslots = nullptr;
   const size_t qn = (size_t)std::max(nrounds, 1);
   rc = rc ? rc : dalloc((void**)&t->cta_round, 4 * cta.size(), "round CTA runs");
   rc = rc ? rc : dalloc((void**)&t->packed, 4 * qn * E, "round stream words");
   rc = rc ? rc : dalloc((void**)&t->val, 4 * qn * E, "round values");
-  rc = rc ? rc : dalloc((void**)&t->row16, 2 * qn * E, "round rows");
-  rc = rc ? rc : dalloc((void**)&t->rbase, 4 * qn, "round first columns");
-  rc = rc ? rc : dalloc((void**)&t->roff, 4 * qn * (NW + 1), "round warp offsets");
+  rc = rc ? rc : dalloc((void**)&t->cbase, 4 * qn * (E / kRoundChunk), "round chunk bases");
   rc = rc ? rc : dalloc((void**)&d_rstart, 4 * qn, "round starts");
   rc = rc ? rc : dalloc((void**)&d_rlen, 4 * qn, "round lengths");
   rc = rc ? rc : dalloc((void**)&d_rrb, 4 * qn, "round blocks");
+  rc = rc ? rc : dalloc((void**)&occ, b4, "round occurrences");
+  rc = rc ? rc : dalloc((void**)&d_bslots, 4 * ((size_t)nrb + 1), "round block slots");
+  const unsigned cmask = (unsigned)((1ULL << cbits) - 1);
+  int nslots_real = 0;
   if (!rc) {
     cudaMemcpyAsync(t->cta_round, cta.data(), 4 * cta.size(), cudaMemcpyHostToDevice, st);
     if (nrounds > 0) {
       cudaMemcpyAsync(d_rstart, rstart.data(), 4 * (size_t)nrounds, cudaMemcpyHostToDevice, st);
       cudaMemcpyAsync(d_rlen, rlen.data(), 4 * (size_t)nrounds, cudaMemcpyHostToDevice, st);
       cudaMemcpyAsync(d_rrb, rrb.data(), 4 * (size_t)nrounds, cudaMemcpyHostToDevice, st);
-      const unsigned cmask = (unsigned)((1ULL << cbits) - 1);
       const int nvalid = bounds[nrb];
-      note_launch();
-      round_key2_kernel<<<nrounds, 256, 0, st>>>(d_rstart, d_rlen, skey, slrow, cmask, q0, a1 == slrow ? a0 : a1,
-                                                 t->rbase, flags);
-      // second stable sort: by (round, local row), payload the column-order position
       unsigned* pos_in = a1 == slrow ? a0 : a1;
       unsigned* pos_alt = k1 == skey ? k0 : k1;
+      note_launch();
+      round_key2_kernel<<<nrounds, 256, 0, st>>>(d_rstart, d_rlen, slrow, q0, pos_in);
+      // second stable sort: by (round, local row), payload the column-order position
       RadixBuffers r2{q0, q1, pos_in, pos_alt, nullptr, nullptr, hist, hoff, false};
       if (radix_sort_pairs(r2, nvalid, 16 + bits_for((long long)nrounds), h->ls, h->d_err, st))
         rc = set_error(SPMX_ERR_INVALID_VALUE, "round SpMV: sort capacity");
@@ -646,9 +504,33 @@ extern "C" int spmx_round_preprocess(spmx_handle_t h, int rb_rows) {
         const unsigned* key2 = r2.result_in_alt ? q1 : q0;
         const unsigned* pos2 = r2.result_in_alt ? pos_alt : pos_in;
         note_launch();
-        round_layout_kernel<<<nrounds, 256, 0, st>>>(d_rstart, d_rlen, d_rrb, d_wsp, skey, sval, cmask, key2, pos2,
-                                                    t->rbase, t->packed, t->val, t->row16, t->roff);
+        round_occurrence_kernel<<<nrounds, 256, 0, st>>>(d_rstart, d_rlen, d_rrb, t->rb_row, key2, pos2, occ, spr);
       }
+    }
+    // slot prefix over all rows; slots of the largest row block
+    if (!rc && m > 0 && launch_scan_exclusive(spr, t->vbg, m, t->vbg + m, h->ls, h->d_err, st))
+      rc = set_error(SPMX_ERR_INVALID_VALUE, "round SpMV: scan capacity");
+    if (!rc && m == 0) cudaMemsetAsync(t->vbg, 0, 4, st);
+    std::vector<int> bslots((size_t)nrb, 0);
+    if (!rc) {
+      note_launch();
+      round_block_slots_kernel<<<(nrb + 255) / 256, 256, 0, st>>>(nrb, t->rb_row, t->vbg, d_bslots);
+      cudaMemcpyAsync(bslots.data(), d_bslots, 4 * (size_t)nrb, cudaMemcpyDeviceToHost, st);
+      se = cudaStreamSynchronize(st);
+      if (se != cudaSuccess) rc = set_error(SPMX_ERR_CUDA, std::string("round SpMV: ") + cudaGetErrorString(se));
+    }
+    if (!rc) {
+      for (int k = 0; k < nrb; ++k) nslots_real = std::max(nslots_real, bslots[k]);
+      t->nslots = nslots_real + kRoundDummy;
+      t->smem = round_smem(t->nslots, rmax);
+      if (t->nslots >= 65536 || (long long)t->smem > avail)
+        rc = set_error(SPMX_ERR_INVALID_VALUE,
+                       "round SpMV: a row block needs more accumulator slots than shared memory holds");
+    }
+    if (!rc && nrounds > 0) {
+      note_launch();
+      round_layout_kernel<<<nrounds, 256, 0, st>>>(d_rstart, d_rlen, d_rrb, t->rb_row, t->vbg, skey, slrow, sval,
+                                                  cmask, occ, nslots_real, t->packed, t->val, t->cbase, flags);
     }
     int hflags[4] = {0, 0, 0, 0};
     if (cudaMemcpyAsync(hflags, flags, sizeof(hflags), cudaMemcpyDeviceToHost, st) != cudaSuccess)
@@ -657,15 +539,18 @@ extern "C" int spmx_round_preprocess(spmx_handle_t h, int rb_rows) {
     if (!rc && se != cudaSuccess) rc = set_error(SPMX_ERR_CUDA, std::string("round SpMV: ") + cudaGetErrorString(se));
     if (!rc && (hflags[0] & 1)) rc = set_error(SPMX_ERR_INVALID_VALUE, "round SpMV: column index out of range");
     if (!rc && (hflags[0] & 2))
-      rc = set_error(SPMX_ERR_INVALID_VALUE, "round SpMV: a round spans too many columns (matrix too sparse)");
+      rc = set_error(SPMX_ERR_INVALID_VALUE,
+                     "round SpMV: 128 consecutive nonzeros of a row block span 2^16 columns (matrix too sparse)");
   }
   dfree(k0); dfree(k1); dfree(a0); dfree(a1); dfree(v0); dfree(v1); dfree(q0); dfree(q1);
-  dfree(hist); dfree(hoff); dfree(d_wsp); dfree(flags); dfree(d_bounds);
-  dfree(d_rstart); dfree(d_rlen); dfree(d_rrb);
+  dfree(hist); dfree(hoff); dfree(flags); dfree(d_bounds); dfree(spr);
+  dfree(d_rstart); dfree(d_rlen); dfree(d_rrb); dfree(occ); dfree(d_bslots);
   if (rc) {
     spmx_round_postprocess(h);
     return rc;
   }
+  round_set_smem<false>(t->smem);
+  round_set_smem<true>(t->smem);
   return SPMX_SUCCESS;
 }
 
@@ -685,10 +570,9 @@ static cudaError_t round_launch(spmx_handle_t h, RoundTables* t, float alpha, fl
   at[1].val.programmaticStreamSerializationAllowed = 1;
   cfg.attrs = at;
   cfg.numAttrs = 2;
-  return cudaLaunchKernelEx(&cfg, round_spmv_kernel<GATED>, (const int*)t->rb_row, (const int*)t->cta_round,
-                            (const unsigned*)t->packed, (const float*)t->val, (const unsigned short*)t->row16,
-                            (const int*)t->rbase, (const int*)t->roff, (const float*)h->x_dense, bits, alpha, y,
-                            h->d_err);
+  return cudaLaunchKernelEx(&cfg, round_spmv_kernel<GATED>, t->nslots, (const int*)t->rb_row,
+                            (const int*)t->cta_round, (const uint4*)t->packed, (const float4*)t->val,
+                            (const int*)t->cbase, (const int*)t->vbg, (const float*)h->x_dense, bits, alpha, y);
 }
 
 int round_spmv_impl(spmx_handle_t h, float alpha, float* y, bool gated) {
@@ -713,7 +597,7 @@ extern "C" int spmx_round_info(spmx_handle_t h, int* info) {
   info[1] = kRoundCS;
   info[2] = t->nrounds;
   info[3] = kRoundE;
-  info[4] = kRoundNW;
+  info[4] = t->nslots;
   info[5] = t->rmax;
   info[6] = (int)t->smem;
   info[7] = t->grid;

@@ -258,10 +258,11 @@ class SpmspvHandle:
 
     def round_info(self):
         """Geometry of the round format: row blocks, CTAs per cluster, rounds,
-        nonzeros per round, warps, shared y rows, shared bytes, grid."""
+        nonzeros per round, accumulator slots per CTA, shared y rows, shared
+        bytes, grid."""
         info = (ctypes.c_int * 8)()
         check(lib.spmx_round_info(self._h, info), "round_info")
-        names = ("row_blocks", "cluster", "rounds", "round", "warps", "rmax", "smem", "grid")
+        names = ("row_blocks", "cluster", "rounds", "round", "slots", "rmax", "smem", "grid")
         return dict(zip(names, list(info)))
 
     def roundspmv(self, alpha, y):
