@@ -214,12 +214,14 @@ int spmx_tiledspmspv(spmx_handle_t h, float alpha, float* d_y);
  * accumulators as it has nonzeros in its densest round; the k-th nonzero of
  * a row in a round adds into the row's k-th accumulator with a plain
  * read-modify-write (all distinct within a round), one barrier per round;
- * at the end each row's accumulators are summed.  Deterministic.  Fails with
- * SPMX_ERR_INVALID_VALUE (the other back-ends still apply) when a column
+ * at the end each row's accumulators are summed.  Deterministic.  When a
+ * row block needs more accumulators than shared memory holds, the
+ * preprocessing retries with row blocks half as tall (up to 5 times).  Fails
+ * with SPMX_ERR_INVALID_VALUE (the other back-ends still apply) when a column
  * index is out of range, when 128 consecutive nonzeros of a row block span
- * 2^16 columns or more (a very sparse row block), when a row block needs
- * more accumulators than shared memory holds, or when row blocks x columns
- * need a sort key of more than 32 bits. */
+ * 2^16 columns or more (a very sparse row block), when the accumulators
+ * still do not fit, or when row blocks x columns need a sort key of more
+ * than 32 bits. */
 int spmx_round_preprocess(spmx_handle_t h, int rb_rows);
 int spmx_round_postprocess(spmx_handle_t h);
 /* geometry chosen by spmx_round_preprocess: info[0..7] = row blocks, CTAs

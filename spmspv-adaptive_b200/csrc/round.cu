@@ -79,7 +79,7 @@ round_spmv_kernel(int nslots, const int* __restrict__ rb_row, const int* __restr
                   const uint4* __restrict__ packed, const float4* __restrict__ val,
                   const int* __restrict__ cbase, const int* __restrict__ vbg, const float* __restrict__ x,
                   const unsigned* __restrict__ xbits, float alpha, float* __restrict__ y) {
-  constexpr int E = kRoundE, CPW = kRoundCPW, NW = kRoundNW;
+  constexpr int E = kRoundE, CPW = kRoundCPW;
   extern __shared__ __align__(16) float ys[];
   float* F = ys + ((nslots + 3) & ~3);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -347,19 +347,10 @@ extern "C" int spmx_round_postprocess(spmx_handle_t h) {
   return SPMX_SUCCESS;
 }
 
-extern "C" int spmx_round_preprocess(spmx_handle_t h, int rb_rows) {
-  if (!h) return set_error(SPMX_ERR_INVALID_VALUE, "NULL handle");
-  if (!h->has_csr || (!h->val && h->nnz > 0))
-    return set_error(SPMX_ERR_NOT_READY, "round SpMV needs the CSR input with values");
-  if (rb_rows < 0) return set_error(SPMX_ERR_INVALID_VALUE, "round SpMV: rb_rows must be >= 0");
+// builds the round format with row blocks of at most rcap rows; *overflow is
+// set when a row block needs more accumulator slots than shared memory holds
+static int round_build(spmx_handle_t h, long long rcap, long long avail, bool* overflow) {
   constexpr int E = kRoundE;
-  int optin = 0;
-  cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, h->device);
-  const long long avail = (long long)optin - round_static_smem();
-  // every nonempty row needs a slot and a row sum: at most avail / 8 rows
-  long long rcap = std::min<long long>((avail / 8) & ~3LL, 65532);
-  if (rb_rows > 0) rcap = std::min<long long>(rcap, std::max(4, (rb_rows + 3) & ~3));
-  if (rcap < 4) return set_error(SPMX_ERR_INVALID_VALUE, "round SpMV: no shared memory left for y");
   spmx_round_postprocess(h);
   const int m = h->m, n = h->n, nnz = h->nnz;
   cudaStream_t st = h->stream;
@@ -523,9 +514,11 @@ extern "C" int spmx_round_preprocess(spmx_handle_t h, int rb_rows) {
       for (int k = 0; k < nrb; ++k) nslots_real = std::max(nslots_real, bslots[k]);
       t->nslots = nslots_real + kRoundDummy;
       t->smem = round_smem(t->nslots, rmax);
-      if (t->nslots >= 65536 || (long long)t->smem > avail)
+      if (t->nslots >= 65536 || (long long)t->smem > avail) {
+        *overflow = true;
         rc = set_error(SPMX_ERR_INVALID_VALUE,
                        "round SpMV: a row block needs more accumulator slots than shared memory holds");
+      }
     }
     if (!rc && nrounds > 0) {
       note_launch();
@@ -552,6 +545,29 @@ extern "C" int spmx_round_preprocess(spmx_handle_t h, int rb_rows) {
   round_set_smem<false>(t->smem);
   round_set_smem<true>(t->smem);
   return SPMX_SUCCESS;
+}
+
+extern "C" int spmx_round_preprocess(spmx_handle_t h, int rb_rows) {
+  if (!h) return set_error(SPMX_ERR_INVALID_VALUE, "NULL handle");
+  if (!h->has_csr || (!h->val && h->nnz > 0))
+    return set_error(SPMX_ERR_NOT_READY, "round SpMV needs the CSR input with values");
+  if (rb_rows < 0) return set_error(SPMX_ERR_INVALID_VALUE, "round SpMV: rb_rows must be >= 0");
+  int optin = 0;
+  cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, h->device);
+  const long long avail = (long long)optin - round_static_smem();
+  // every nonempty row needs a slot and a row sum: at most avail / 8 rows
+  long long rcap = std::min<long long>((avail / 8) & ~3LL, 65532);
+  if (rb_rows > 0) rcap = std::min<long long>(rcap, std::max(4, (rb_rows + 3) & ~3));
+  if (rcap < 4) return set_error(SPMX_ERR_INVALID_VALUE, "round SpMV: no shared memory left for y");
+  // rows with many nonzeros in one round (hub rows, or rows whose nonzeros
+  // sit in neighbouring columns) need several slots each; when a row block
+  // needs more than fit, retry with row blocks half as tall (up to 5 times)
+  for (int attempt = 0;; ++attempt) {
+    bool overflow = false;
+    const int rc = round_build(h, rcap, avail, &overflow);
+    if (rc == SPMX_SUCCESS || !overflow || attempt == 5 || rcap <= 64) return rc;
+    rcap = std::max<long long>(64, (rcap / 2) & ~3LL);
+  }
 }
 
 template <bool GATED>

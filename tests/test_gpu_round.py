@@ -31,6 +31,14 @@ def _extra():
     yield "tall-thin", rand_csr(200000, 3, density=0.4, seed=42)
     from spmx import gen
     yield "zipf-64k", gen.zipf_rows(1 << 16, 1.5, 16, 5000, seed=43)
+    # power-law rows and columns (hub rows fill whole rounds) and a stencil
+    # (neighbouring columns: several slots per row): both need the retry with
+    # shorter row blocks
+    yield "chung-lu-64k", gen.chung_lu(1 << 16, 2.1, 16.0, seed=46)
+    g = gen.rmat(15, 16, seed=47)
+    g.val = np.random.default_rng(48).uniform(-1, 1, g.nnz).astype(np.float32)
+    yield "rmat-15", g
+    yield "laplacian-512", gen.laplacian(512)
 
 
 EXTRA = list(_extra())
