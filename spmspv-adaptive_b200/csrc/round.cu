@@ -87,6 +87,12 @@ round_spmv_kernel(int nslots, const int* __restrict__ rb_row, const int* __restr
   const int row0 = __ldg(rb_row + rb), rows = __ldg(rb_row + rb + 1) - row0;
   for (int r = threadIdx.x; r < nslots; r += blockDim.x) ys[r] = 0.f;
   const int k0 = __ldg(cta_round + blockIdx.x), k1 = __ldg(cta_round + blockIdx.x + 1);
+  // the row block's slot prefix is read by the epilogue: bring it into L2 now
+  if (threadIdx.x == 0 && rows > 0) {
+    const size_t a0 = ((size_t)(vbg + row0)) & ~(size_t)15;
+    const size_t a1 = ((size_t)(vbg + row0 + rows + 1) + 15) & ~(size_t)15;
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(a0), "r"((unsigned)(a1 - a0)) : "memory");
+  }
   // two register sets, used alternately: a round's stream words, values,
   // chunk bases and gathered x
   uint4 pa[CPW], pb[CPW];
@@ -147,11 +153,24 @@ round_spmv_kernel(int nslots, const int* __restrict__ rb_row, const int* __restr
   }
   // each row's slots, summed in slot order
   const int base0 = __ldg(vbg + row0);
-  for (int r = threadIdx.x; r < rows; r += blockDim.x) {
-    const int s0 = __ldg(vbg + row0 + r) - base0, s1 = __ldg(vbg + row0 + r + 1) - base0;
-    float acc = 0.f;
-    for (int s = s0; s < s1; ++s) acc += ys[s];
-    F[r] = acc;
+  constexpr int FU = 8;  // rows per thread per pass: their slot bounds are loaded together
+  for (int rb4 = 0; rb4 < rows; rb4 += FU * (int)blockDim.x) {
+    int lo[FU], hi[FU];
+#pragma unroll
+    for (int j = 0; j < FU; ++j) {
+      const int r = rb4 + j * (int)blockDim.x + (int)threadIdx.x;
+      lo[j] = r < rows ? __ldg(vbg + row0 + r) : 0;
+      hi[j] = r < rows ? __ldg(vbg + row0 + r + 1) : 0;
+    }
+#pragma unroll
+    for (int j = 0; j < FU; ++j) {
+      const int r = rb4 + j * (int)blockDim.x + (int)threadIdx.x;
+      if (r < rows) {
+        float acc = 0.f;
+        for (int s = lo[j] - base0; s < hi[j] - base0; ++s) acc += ys[s];
+        F[r] = acc;
+      }
+    }
   }
   // the cluster's row sums, added in rank order; each CTA stores a slice
   cg::cluster_group cl = cg::this_cluster();
@@ -159,11 +178,23 @@ round_spmv_kernel(int nslots, const int* __restrict__ rb_row, const int* __restr
   const int rank = (int)cl.block_rank();
   const int slice = (rows + kRoundCS - 1) / kRoundCS;
   const int r0 = rank * slice, r1 = min(rows, r0 + slice);
-  for (int r = r0 + (int)threadIdx.x; r < r1; r += blockDim.x) {
-    float acc = 0.f;
+  constexpr int CU = 4;  // rows per thread per pass: their peer reads are issued together
+  for (int rc = r0; rc < r1; rc += CU * (int)blockDim.x) {
+    float acc[CU];
 #pragma unroll
-    for (int q = 0; q < kRoundCS; ++q) acc += *cl.map_shared_rank(F + r, q);
-    y[row0 + r] = alpha * acc;
+    for (int j = 0; j < CU; ++j) {
+      const int r = rc + j * (int)blockDim.x + (int)threadIdx.x;
+      acc[j] = 0.f;
+      if (r < r1) {
+#pragma unroll
+        for (int q = 0; q < kRoundCS; ++q) acc[j] += *cl.map_shared_rank(F + r, q);
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < CU; ++j) {
+      const int r = rc + j * (int)blockDim.x + (int)threadIdx.x;
+      if (r < r1) y[row0 + r] = alpha * acc[j];
+    }
   }
   cl.sync();  // peers read this CTA's row sums until here
 }
