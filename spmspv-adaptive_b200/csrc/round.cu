@@ -55,8 +55,19 @@ constexpr int kRoundCPW = kRoundE / kRoundChunk / kRoundNW;  // chunks per warp 
 constexpr int kRoundDummy = 32;   // padding slots after the real ones (one per lane)
 static_assert(kRoundCPW >= 1, "round geometry");
 
+// the per-CTA round runs and row-block bounds of a launch of at most
+// kRoundParamCtas CTAs, passed by value so that a CTA reads them without a
+// memory round trip (use = 0: read them from the device arrays instead)
+constexpr int kRoundParamCtas = 296;
+struct RoundGeom {
+  int use;
+  int cta_round[kRoundParamCtas + 1];
+  int rb_row[kRoundParamCtas / kRoundCS + 1];
+};
+
 struct RoundTables {
   int nrb = 0, grid = 0, rmax = 0, nrounds = 0, nslots = 0;
+  RoundGeom geom = {};
   size_t smem = 0;
   int* rb_row = nullptr;          // nrb + 1 row block boundaries
   int* cta_round = nullptr;       // grid + 1: rounds of CTA c are [cta_round[c], cta_round[c + 1])
@@ -75,7 +86,8 @@ size_t round_smem(int nslots, int rmax) { return 4 * (size_t)(((nslots + 3) & ~3
 
 template <bool GATED>
 __global__ void __launch_bounds__(kRoundNW * 32, 1)
-round_spmv_kernel(int nslots, const int* __restrict__ rb_row, const int* __restrict__ cta_round,
+round_spmv_kernel(const __grid_constant__ RoundGeom geom, int nslots, const int* __restrict__ rb_row,
+                  const int* __restrict__ cta_round,
                   const uint4* __restrict__ packed, const float4* __restrict__ val,
                   const int* __restrict__ cbase, const int* __restrict__ vbg, const float* __restrict__ x,
                   const unsigned* __restrict__ xbits, float alpha, float* __restrict__ y) {
@@ -84,9 +96,11 @@ round_spmv_kernel(int nslots, const int* __restrict__ rb_row, const int* __restr
   float* F = ys + ((nslots + 3) & ~3);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int rb = blockIdx.x / kRoundCS;
-  const int row0 = __ldg(rb_row + rb), rows = __ldg(rb_row + rb + 1) - row0;
+  const int row0 = geom.use ? geom.rb_row[rb] : __ldg(rb_row + rb);
+  const int rows = (geom.use ? geom.rb_row[rb + 1] : __ldg(rb_row + rb + 1)) - row0;
+  const int k0 = geom.use ? geom.cta_round[blockIdx.x] : __ldg(cta_round + blockIdx.x);
+  const int k1 = geom.use ? geom.cta_round[blockIdx.x + 1] : __ldg(cta_round + blockIdx.x + 1);
   for (int r = threadIdx.x; r < nslots; r += blockDim.x) ys[r] = 0.f;
-  const int k0 = __ldg(cta_round + blockIdx.x), k1 = __ldg(cta_round + blockIdx.x + 1);
   // the row block's slot prefix is read by the epilogue: bring it into L2 now
   if (threadIdx.x == 0 && rows > 0) {
     const size_t a0 = ((size_t)(vbg + row0)) & ~(size_t)15;
@@ -575,6 +589,11 @@ static int round_build(spmx_handle_t h, long long rcap, long long avail, bool* o
   }
   round_set_smem<false>(t->smem);
   round_set_smem<true>(t->smem);
+  t->geom.use = t->grid <= kRoundParamCtas ? 1 : 0;
+  if (t->geom.use) {
+    std::copy(cta.begin(), cta.end(), t->geom.cta_round);
+    std::copy(rbr.begin(), rbr.end(), t->geom.rb_row);
+  }
   return SPMX_SUCCESS;
 }
 
@@ -617,7 +636,7 @@ static cudaError_t round_launch(spmx_handle_t h, RoundTables* t, float alpha, fl
   at[1].val.programmaticStreamSerializationAllowed = 1;
   cfg.attrs = at;
   cfg.numAttrs = 2;
-  return cudaLaunchKernelEx(&cfg, round_spmv_kernel<GATED>, t->nslots, (const int*)t->rb_row,
+  return cudaLaunchKernelEx(&cfg, round_spmv_kernel<GATED>, t->geom, t->nslots, (const int*)t->rb_row,
                             (const int*)t->cta_round, (const uint4*)t->packed, (const float4*)t->val,
                             (const int*)t->cbase, (const int*)t->vbg, (const float*)h->x_dense, bits, alpha, y);
 }
