@@ -15,9 +15,10 @@ host->device copy of x (pinned) and the device->host read of y: its nonzeros
 (keys and values, after the count comes back) for a sparse x, the dense y for
 the dense x.
 
---impl reference times the reference's CPU path (its serial routines,
-restated in the oracle and parallelised with OpenMP over all host threads)
-on the same sweep.
+--impl reference times the reference's CPU path on all host threads on the
+same sweep (the reference's own serialspmv over row slices for the dense x,
+the oracle's OpenMP restatement of SpmSpvCSCHost for a sparse x), on inputs
+built by the oracle, and the reference's own GPU kernels rebuilt for sm_100a.
 """
 import argparse
 import json
@@ -149,6 +150,7 @@ def allmax(v, world):
 
 
 def make_inputs():
+    """The benchmark's inputs from the product's generators (libspmx.so)."""
     from spmx import gen
     A = gen.zipf_1m(seed=2)
     xs = []
@@ -159,25 +161,81 @@ def make_inputs():
     return A, xs
 
 
+def make_inputs_oracle():
+    """The same inputs from the oracle's restatement of the generators (bit
+    for bit the same, checked by tests/test_gen.py): the CPU reference arm
+    loads nothing from the product library."""
+    import oracle.oracle as orc
+    A = orc.gen_zipf_1m(seed=2)
+    xs = []
+    for d in DENSITIES:
+        k = orc.density_nnz(A.n, d)
+        key, val = orc.gen_sparse_vector(A.n, k, "uniform", 1000 + k)
+        xs.append((d, key, val))
+    return A, xs
+
+
+def cpu_model():
+    """The host CPU's model name (lscpu's "Model name", from /proc/cpuinfo)."""
+    try:
+        with open("/proc/cpuinfo") as f:
+            for ln in f:
+                if ln.startswith("model name"):
+                    return ln.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+def ref_host_libs():
+    """The reference's own host routines compiled from its sources
+    (oracle/_ref): (libref_host.so with serialspmv, libref_csc.so with
+    SpmSpvCSCHost), or None where they were not built."""
+    import ctypes
+    so1 = os.path.join(ROOT, "oracle", "_ref", "libref_host.so")
+    so2 = os.path.join(ROOT, "oracle", "_ref", "libref_csc.so")
+    if not (os.path.exists(so1) and os.path.exists(so2)):
+        return None
+    h, c = ctypes.CDLL(so1), ctypes.CDLL(so2)
+    P = ctypes.c_void_p
+    h.ref_serialspmv.argtypes = [ctypes.c_int] * 3 + [P] * 5 + [ctypes.c_float]
+    h.ref_serialspmv.restype = None
+    c.ref_spmspv_csc_host.argtypes = [ctypes.c_int] * 3 + [P] * 3 + [ctypes.c_int] + [P] * 5
+    c.ref_spmspv_csc_host.restype = None
+    return h, c
+
+
+def row_slices(rowptr, parts):
+    """Row ranges with about nnz/parts nonzeros each."""
+    nnz = int(rowptr[-1])
+    cuts = np.searchsorted(rowptr, np.linspace(0, nnz, parts + 1)[1:-1]).tolist()
+    b = [0] + cuts + [len(rowptr) - 1]
+    return [(b[i], b[i + 1]) for i in range(parts) if b[i + 1] > b[i]]
+
+
 def ref_gpu_sweep(A, xs, colptr, row, cval, binl, reps=7):
     """The reference's own GPU kernels (oracle/_ref, rebuilt for sm_100a from
     its sources) on the same sweep: per density the fastest of the kernels
     that run here (CSC naive atomic SpMSpV for every density; Hola and naive
     CSR SpMV for the dense x), each result checked against the FP64 oracle.
     Left out: the merge-path and sort CSC SpMSpV, whose chained scan spins
-    without a bound on the previous block's sum, and CSR5, whose
-    preprocessing made an illegal memory access on this matrix."""
+    without a bound on the previous block's sum, and CSR5, whose descriptor
+    kernel writes one word past its descriptor array on this matrix (a row
+    starting at offset nnz, with nnz a multiple of 32 * sigma); the
+    comparator library does not contain that path."""
     import ctypes
     import oracle.oracle as orc
     so = os.path.join(ROOT, "oracle", "_ref", "libref_host.so")
     if not os.path.exists(so):
         return {"unavailable": "oracle/_ref/libref_host.so not built"}
     lib = ctypes.CDLL(so)
+    if lib.ref_gpu_count() < 1:
+        return {"unavailable": "no CUDA device visible to the reference's GPU kernels"}
     P = ctypes.c_void_p
     lib.ref_gpu_time.argtypes = [ctypes.c_int] * 4 + [P] * 7 + [ctypes.c_int, P, P, ctypes.c_int, P, P]
     lib.ref_gpu_time.restype = ctypes.c_int
     m, n, nnz = A.m, A.n, A.nnz
-    names = {0: "hola-spmv", 1: "csr5-spmv", 2: "naive-spmv", 3: "csc-naive-atomic"}
+    names = {0: "hola-spmv", 2: "naive-spmv", 3: "csc-naive-atomic"}
     per = []
     tot_ms, tot_bytes = 0.0, 0
     for (d, key, val), b in zip(xs, binl):
@@ -214,10 +272,20 @@ def ref_gpu_sweep(A, xs, colptr, row, cval, binl, reps=7):
 # reference arm: the reference's CPU routines on all host threads
 # ---------------------------------------------------------------------------
 def run_reference(args, world, rank):
+    """The reference arm: the reference's CPU path on all host threads, on
+    inputs built by the oracle (nothing of the product is loaded).  The dense
+    leg is the reference's own serialspmv (oracle/_ref, compiled from its
+    sources), run over nnz-balanced row slices on every host thread; the
+    sparse legs are the oracle's OpenMP restatement of SpmSpvCSCHost (x
+    entries across threads, atomic adds), because the reference's routine is
+    one serial loop into one dense y and cannot be split without changing it.
+    With --ref-gpu (the default) the line also carries the reference's own GPU
+    kernels rebuilt for sm_100a on the same sweep."""
     if rank != 0:
         return 0
+    from concurrent.futures import ThreadPoolExecutor
     import oracle.oracle as orc
-    A, xs = make_inputs()
+    A, xs = make_inputs_oracle()
     colptr, row, cval = A.to_csc()
     threads = orc.raw.cpu_threads()
     m, n, nnz = A.m, A.n, A.nnz
@@ -226,13 +294,27 @@ def run_reference(args, world, rank):
     binl = [int(orc.vec_features(colptr, key)[0]) for _, key, _ in xs]
     tot_bytes = sum(eff_bytes(m, n, nnz, len(k), b) for (_, k, _), b in zip(xs, binl))
     dense = [orc.sparse2dense_bits(n, k, v)[0] for _, k, v in xs]
+    libs = ref_host_libs()
+    pool = ThreadPoolExecutor(max_workers=threads)
+    slices = row_slices(A.rowptr, 4 * threads)  # 4 per thread: a finer split balances better
+    rp_addr = A.rowptr.ctypes.data
+
+    def dense_leg(xd):
+        if libs is None:
+            orc.raw.cpu_spmv_omp(m, P(A.rowptr), P(A.col), P(A.val), P(xd), P(y), 1.0)
+            return
+        host = libs[0]
+        # ctypes releases the GIL for the call: the slices run in parallel
+        list(pool.map(lambda r: host.ref_serialspmv(r[1] - r[0], n, nnz, rp_addr + 4 * r[0], P(A.col),
+                                                     P(A.val), P(xd), y.ctypes.data + 4 * r[0], 1.0),
+                      slices))
 
     def step():
         t = 0.0
         for (d, key, val), xd in zip(xs, dense):
             t0 = time.perf_counter()
             if d >= 1.0:
-                orc.raw.cpu_spmv_omp(m, P(A.rowptr), P(A.col), P(A.val), P(xd), P(y), 1.0)
+                dense_leg(xd)
             else:
                 orc.raw.cpu_spmspv_csc_omp(m, P(colptr), P(row), P(cval), len(key), P(key),
                                            P(val), P(y))
@@ -242,19 +324,23 @@ def run_reference(args, world, rank):
     for _ in range(args.warmup):
         step()
     ts = [step() for _ in range(args.steps)]
+    pool.shutdown()
     sec = sum(ts) / len(ts)
     gbs = tot_bytes / sec / 1e9
+    dense_what = ("the reference's own serialspmv (oracle/_ref) over %d nnz-balanced row slices on "
+                  "%d host threads" % (len(slices), threads)) if libs else "the oracle's serialspmv, OpenMP"
     line = {"metric": METRIC, "value": gbs, "unit": "GB/s", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": sec * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic", "impl": "reference",
             "config": {"workload": WORKLOAD, "parallelism": "replicas" if args.gpus > 1 else "single"},
-            "cpu_baseline": {"value": gbs, "unit": "GB/s", "cores": threads, "kind": "port",
-                             "sample": "the full 6-density sweep per step: SpmSpvCSCHost for "
-                                       "sparse x and serialspmv for dense x (oracle restatement, "
-                                       "OpenMP over all host threads)"},
+            "cpu_baseline": {"value": gbs, "unit": "GB/s", "cores": threads, "cpu": cpu_model(),
+                             "kind": "port",
+                             "sample": "the full 6-density sweep per step; dense x: " + dense_what +
+                                       "; sparse x: SpmSpvCSCHost restated (oracle), OpenMP over all "
+                                       "host threads"},
             "e2e": {"value": gbs, "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
-    if args.ref_gpu:
+    if not args.no_ref_gpu:
         line["ref_gpu_sm100a"] = ref_gpu_sweep(A, xs, colptr, row, cval, binl)
     print(json.dumps(line), flush=True)
     return 0
@@ -462,7 +548,7 @@ def run_ours(args, world, rank, local):
 
     line = None
     if rank == 0:
-        cpu = cpu_baseline(A, xs, binl) if not args.no_cpu else None
+        cpu = cpu_baseline(A, xs, binl) if not args.no_cpu and world == 1 else None
         sweep = [{"density": dd, "x_nnz": k, "bin_len": b, "kernel": abi.KERNEL_NAMES[c],
                   "ms": float(t), "eff_gbs": eb / (t * 1e-3) / 1e9}
                  for (dd, _, _, k), b, c, t, eb in zip(dx, binl, chosen, per, ebytes)]
@@ -919,29 +1005,48 @@ def run_hybrid(torch, dev, stream, args):
 
 
 def cpu_baseline(A, xs, binl):
-    """The reference's serial CPU routines (restated), one core, one sweep."""
+    """The reference's CPU path on one core over one sweep: its own
+    serialspmv (dense x) and SpmSpvCSCHost (sparse x), compiled from its
+    sources (oracle/_ref), or the oracle's restatements where those were not
+    built."""
     import oracle.oracle as orc
     colptr, row, cval = A.to_csc()
     m, n, nnz = A.m, A.n, A.nnz
     y = np.zeros(m, np.float32)
+    yk = np.zeros(m, np.int32)
     P = lambda a: a.ctypes.data  # noqa: E731
     dense = [orc.sparse2dense_bits(n, k, v)[0] for _, k, v in xs]
+    libs = ref_host_libs()
+    import ctypes
+    ynnz = ctypes.c_int()
     best = None
     for _ in range(3):
         t = 0.0
         for (d, key, val), xd in zip(xs, dense):
             t0 = time.perf_counter()
-            if d >= 1.0:
-                orc.raw.cpu_spmv_serial(m, P(A.rowptr), P(A.col), P(A.val), P(xd), P(y), 1.0)
+            if libs is None:
+                if d >= 1.0:
+                    orc.raw.cpu_spmv_serial(m, P(A.rowptr), P(A.col), P(A.val), P(xd), P(y), 1.0)
+                else:
+                    orc.raw.cpu_spmspv_csc_serial(m, P(colptr), P(row), P(cval), len(key), P(key),
+                                                  P(val), P(y))
+            elif d >= 1.0:
+                libs[0].ref_serialspmv(m, n, nnz, P(A.rowptr), P(A.col), P(A.val), P(xd), P(y), 1.0)
             else:
-                orc.raw.cpu_spmspv_csc_serial(m, P(colptr), P(row), P(cval), len(key), P(key),
-                                              P(val), P(y))
+                libs[1].ref_spmspv_csc_host(m, n, nnz, P(row), P(colptr), P(cval), len(key), P(key),
+                                            P(val), ctypes.byref(ynnz), P(yk), P(y))
             t += time.perf_counter() - t0
         best = t if best is None else min(best, t)
     tot = sum(eff_bytes(m, n, nnz, len(k), b) for (_, k, _), b in zip(xs, binl))
-    return {"value": tot / best / 1e9, "unit": "GB/s", "cores": 1, "kind": "port",
-            "sample": "one full 6-density sweep (best of 3): SpmSpvCSCHost for sparse x, "
-                      "serialspmv for dense x, oracle restatement, single thread",
+    if libs is None:
+        kind, what = "port", "the oracle's restatements of SpmSpvCSCHost / serialspmv"
+    else:
+        kind, what = "reference", ("the reference's own SpmSpvCSCHost / serialspmv compiled from its "
+                                   "sources (SpmSpvCSCHost reads x into an int, so with U(-1,1) values "
+                                   "its products are 0; it still does the same loads, adds and output "
+                                   "pass)")
+    return {"value": tot / best / 1e9, "unit": "GB/s", "cores": 1, "cpu": cpu_model(), "kind": kind,
+            "sample": "one full 6-density sweep (best of 3), single thread: " + what,
             "ms": best * 1e3}
 
 
@@ -1034,9 +1139,9 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-batched", action="store_true")
     ap.add_argument("--no-ingest", action="store_true")
-    ap.add_argument("--ref-gpu", action="store_true",
-                    help="with --impl reference: also time the reference's own GPU kernels, rebuilt "
-                         "for sm_100a, on the same sweep")
+    ap.add_argument("--no-ref-gpu", action="store_true",
+                    help="with --impl reference: leave out the reference's own GPU kernels, rebuilt "
+                         "for sm_100a, on the same sweep (timed by default)")
     ap.add_argument("--tune-cache", default=None,
                     help="autotuner cache file: a second run with the same file (e.g. under a profiler, "
                          "whose serialised timings would mislead the tuner) reuses the first run's choices")

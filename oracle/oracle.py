@@ -52,6 +52,10 @@ _sigs = {
     "oracle_free": (None, [_P]),
     "oracle_coo2hybrid": (_i, [_i, _i, _P, _P, _P]),
     "oracle_mtx_read": (_i, [ctypes.c_char_p, _P, _P, _P, _P, _P, _P]),
+    "oracle_spmspv_csc_host_faithful": (_i, [_i, _P, _P, _P, _i, _P, _P, _P, _P]),
+    "oracle_csr2csc": (_i, [_i, _i, _P, _P, _P, _P, _P, _P]),
+    "oracle_gen_zipf_rows": (_i, [_i, _d, _i, _i, ctypes.c_uint64, _P, _P, _P]),
+    "oracle_gen_sparse_vector": (_i, [_i, _i, _i, ctypes.c_uint64, _P, _P]),
 }
 for _n, (_r, _a) in _sigs.items():
     _fn = getattr(_lib, _n)
@@ -236,3 +240,73 @@ def coo2hybrid(n, rowptr, col):
     flags = np.zeros(max(len(col), 1), np.uint8)
     k = _lib.oracle_coo2hybrid(len(rowptr) - 1, n, _p(rowptr), _p(col), _p(flags))
     return k, flags[:len(col)].astype(bool)
+
+
+def spmspv_csc_host_faithful(m, colptr, row, val, x_key, x_val):
+    """SpmSpvCSCHost as written (x truncated to int, FP32, IS_FLOAT_ZERO
+    output filter): (y_key, y_val)."""
+    colptr, row, val = _a(colptr, np.int32), _a(row, np.int32), _a(val, np.float32)
+    x_key, x_val = _a(x_key, np.int32), _a(x_val, np.float32)
+    key = np.zeros(max(m, 1), np.int32)
+    v = np.zeros(max(m, 1), np.float32)
+    k = _lib.oracle_spmspv_csc_host_faithful(m, _p(colptr), _p(row), _p(val), len(x_key), _p(x_key),
+                                             _p(x_val), _p(key), _p(v))
+    return key[:k], v[:k]
+
+
+def csr2csc(m, n, rowptr, col, val=None):
+    """Stable CSR -> CSC transpose: (colptr, row, cval)."""
+    rowptr, col = _a(rowptr, np.int32), _a(col, np.int32)
+    val = None if val is None else _a(val, np.float32)
+    nnz = int(rowptr[-1])
+    colptr = np.zeros(n + 1, np.int32)
+    row = np.zeros(max(nnz, 1), np.int32)
+    cval = None if val is None else np.zeros(max(nnz, 1), np.float32)
+    if _lib.oracle_csr2csc(m, n, _p(rowptr), _p(col), _p(val), _p(colptr), _p(row), _p(cval)):
+        raise ValueError("column index out of range")
+    return colptr, row[:nnz], None if cval is None else cval[:nnz]
+
+
+class HostCsr:
+    """A host CSR (int32 row pointer / columns, float32 values)."""
+
+    def __init__(self, m, n, rowptr, col, val):
+        self.m, self.n = int(m), int(n)
+        self.rowptr, self.col, self.val = rowptr, col, val
+
+    @property
+    def nnz(self):
+        return int(self.rowptr[-1])
+
+    def to_csc(self):
+        return csr2csc(self.m, self.n, self.rowptr, self.col, self.val)
+
+
+def gen_zipf_rows(m, s=1.5, mean=16, maxlen=10000, seed=2):
+    """The benchmark's Zipf-row matrix (restated generator, see spmx_oracle.c)."""
+    rowptr = np.zeros(m + 1, np.int32)
+    col = np.zeros(max(mean * m, 1), np.int32)
+    val = np.zeros(max(mean * m, 1), np.float32)
+    if _lib.oracle_gen_zipf_rows(m, s, mean, maxlen, seed, _p(rowptr), _p(col), _p(val)):
+        raise ValueError("zipf arguments out of range")
+    return HostCsr(m, m, rowptr, col[:mean * m], val[:mean * m])
+
+
+def gen_zipf_1m(seed=2):
+    """1,048,576 x 1,048,576, Zipf(1.5) rows, mean 16, max 10,000."""
+    return gen_zipf_rows(1 << 20, 1.5, 16, 10000, seed)
+
+
+def gen_sparse_vector(n, k, dist="uniform", seed=7):
+    """k distinct sorted positions in [0, n), U(-1,1) or N(0,1) values."""
+    key = np.zeros(max(k, 1), np.int32)
+    val = np.zeros(max(k, 1), np.float32)
+    if _lib.oracle_gen_sparse_vector(n, k, 0 if dist == "uniform" else 1, seed, _p(key), _p(val)):
+        raise ValueError("k out of range")
+    return key[:k], val[:k]
+
+
+def density_nnz(n, d):
+    """x_nnz = ceil(d * n) for the density sweep."""
+    import math
+    return min(n, int(math.ceil(d * n)))

@@ -69,18 +69,23 @@ extern "C" void ref_coo2hybrid(int m, int n, int nnz, int* row, int* col, float*
 // GPU comparator (test infrastructure): the reference's own SpMV / SpMSpV
 // kernels, compiled for sm_100a from its sources, timed with CUDA events on
 // the default stream, with a 256 MiB memset before each call to flush L2.
-// Only kernels without waits between thread blocks run here: Hola SpMV
-// (holaspmv.h), CSR5 SpMV (csr5_spmv_cuda.h), the naive CSR SpMV
+// Only kernels without waits between thread blocks and without a known
+// out-of-bounds access run here: Hola SpMV (holaspmv.h), the naive CSR SpMV
 // (naivespmv.h) and the atomic naive CSC SpMSpV (CscBasedNoSortNaiveSpmspv,
 // csc_sort_spmspv.cuh:98-119).  The merge-path and sort CSC variants use a
 // chained scan whose blocks spin without a bound on the previous block's sum
-// (scan_kernel.cuh:99, :232), so they are not run.  The CSR5 path (which 1)
-// made an illegal memory access in its preprocessing on the 1M-row Zipf
-// matrix; callers leave it out.
-//   which: 0 Hola SpMV, 1 CSR5 SpMV, 2 naive SpMV, 3 CSC naive atomic SpMSpV
+// (scan_kernel.cuh:99, :232), so they are not run.  CSR5 is not built into
+// this comparator at all: its descriptor kernel
+// (generate_partition_descriptor_s1_kernel, format_conversion.h:147-163)
+// maps a row that starts at offset nnz (an empty last row) to tile
+// nnz / (omega * sigma), which is one past the last tile when nnz is a
+// multiple of omega * sigma, and its atomicOr then writes one word past the
+// descriptor array (spmspv.h:1464).
+//   which: 0 Hola SpMV, 2 naive SpMV, 3 CSC naive atomic SpMSpV; any other
+//   value returns -1 without touching the device.
 // All arrays are host arrays; the function makes its own device copies.
 // ms_out[reps] receives each call's time, y_out[m] the last result.
-// Returns 0, or -1 after a CUDA error.
+// Returns 0, or -1 after a CUDA error or for an unknown `which`.
 namespace {
 template <class T>
 T* dcopy(const T* h, size_t count) {
@@ -91,10 +96,21 @@ T* dcopy(const T* h, size_t count) {
 }
 }  // namespace
 
+// Number of CUDA devices this process can use (0 without a GPU or driver).
+extern "C" int ref_gpu_count() {
+  int c = 0;
+  if (cudaGetDeviceCount(&c) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  return c;
+}
+
 extern "C" int ref_gpu_time(int which, int m, int n, int nnz, const int* rowptr, const int* col,
                             const float* val, const int* colptr, const int* crow, const float* cval,
                             const float* x, int x_nnz, const int* xkey, const float* xval, int reps,
                             float* ms_out, float* y_out) {
+  if (which != 0 && which != 2 && which != 3) return -1;
   int* d_rp = dcopy(rowptr, (size_t)m + 1);
   int* d_col = dcopy(col, (size_t)nnz);
   float* d_val = dcopy(val, (size_t)nnz);
@@ -106,6 +122,15 @@ extern "C" int ref_gpu_time(int which, int m, int n, int nnz, const int* rowptr,
   float* d_xval = which == 3 ? dcopy(xval, (size_t)x_nnz) : nullptr;
   float* d_y = dcopy<float>(nullptr, (size_t)m);
   char* flush = dcopy<char>(nullptr, (size_t)256 << 20);
+  const bool csc = which == 3;
+  if (!d_rp || !d_col || !d_val || !d_x || !d_y || !flush ||
+      (csc && (!d_cp || !d_crow || !d_cval || !d_xkey || !d_xval))) {
+    cudaFree(d_rp); cudaFree(d_col); cudaFree(d_val); cudaFree(d_cp); cudaFree(d_crow);
+    cudaFree(d_cval); cudaFree(d_x); cudaFree(d_xkey); cudaFree(d_xval); cudaFree(d_y);
+    cudaFree(flush);
+    cudaGetLastError();
+    return -1;
+  }
   SpmspvHandle<int, unsigned int, float> A(m, n, nnz);
   if (which == 3) {
     A.InputCSC(nnz, d_crow, d_cp, d_cval);
@@ -113,19 +138,12 @@ extern "C" int ref_gpu_time(int which, int m, int n, int nnz, const int* rowptr,
     A.allocPreBuffer();
   } else {
     A.InputCSR(nnz, d_rp, d_col, d_val);
-    if (which == 1) {
-      A.setX(d_x);
-      A.setSigma(ANONYMOUSLIB_AUTO_TUNED_SIGMA);  // as the reference's drivers do
-      A.CSR5Preprocess();
-    } else {
-      A.set_x(d_x);
-      if (which == 0) A.holaPreprocess();
-    }
+    A.set_x(d_x);
+    if (which == 0) A.holaPreprocess();
   }
   auto call = [&]() {
     int ynnz = 0;
     if (which == 0) A.holaspmv(1.0f, d_y);
-    else if (which == 1) A.csr5spmv(1.0f, d_y);
     else if (which == 2) A.naivespmv(1.0f, d_y);
     else A.CscBasedNoSortNaiveSpmspv(1.0f, &ynnz, d_y);
   };
@@ -144,7 +162,6 @@ extern "C" int ref_gpu_time(int which, int m, int n, int nnz, const int* rowptr,
   if (y_out) cudaMemcpy(y_out, d_y, sizeof(float) * (size_t)m, cudaMemcpyDeviceToHost);
   const cudaError_t err = cudaDeviceSynchronize();
   if (which == 0) A.holaPostprocess();
-  if (which == 1) A.CSR5Postprocess();
   if (which == 3) A.deallocPreBuffer();
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);

@@ -8,7 +8,8 @@
  * Each function restates a CPU routine of hpc-research-2020/spmspv-adaptive
  * (paths relative to hice-spmspv/hice/la/):
  *   - serialspmv                 test/test_application.cu:107-116
- *   - SpmSpvCSCHost              test/test_sort_spmspv.cu:330-375
+ *   - SpmSpvCSCHost              test/test_sort_spmspv.cu:330-375 (FP64 and
+ *                                faithful forms)
  *   - computeMatFeture_serial    include/spmspv/csc-spmspv/spmspv.h:2275-2335
  *   - extractMatFeature (stdRow) include/spmspv/csc-spmspv/spmspv.h:423-447
  *   - computeVecFeture_serial    include/spmspv/csc-spmspv/spmspv.h:2338-2361
@@ -27,9 +28,13 @@
  * compiled from its sources (oracle/build_ref.sh -> oracle/_ref) where that
  * builds, as recorded by tests/test_oracle_pin.py.
  *
+ * It also holds a CSR -> CSC transpose and a restatement of the benchmark's
+ * synthetic input generators (end of file), so the CPU legs of the benchmark
+ * need nothing from the product library.
+ *
  * Deliberate departures from the reference, each noted at its function:
  *   - SpmSpvCSCHost reads x_val into an int (test_sort_spmspv.cu:340); the
- *     oracle keeps the value.
+ *     FP64 oracle keeps the value (the faithful form truncates).
  *   - accumulation is FP64 unless the function is marked "faithful".
  */
 #include <math.h>
@@ -117,6 +122,54 @@ EXPORT int oracle_sparse_output_flt_eps(int m, const double* y, int* key, float*
   for (int r = 0; r < m; r++)
     if (!(fabs(y[r]) < FLT_EPSILON)) { key[k] = r; v[k] = (float)y[r]; k++; }
   return k;
+}
+
+/* SpmSpvCSCHost, faithful (test_sort_spmspv.cu:330-375): each x value is
+ * read into an int (`int col_index, x_val;`, :340), i.e. truncated toward
+ * zero; y is a dense FP32 vector accumulated as y[row] += val * x in x order,
+ * then column order; alpha is not applied (the routine takes none); the
+ * output lists, in row order, the entries that are not IS_FLOAT_ZERO
+ * (fabs(y) < FLT_EPSILON; the float overload of abs, as the reference build
+ * resolves it).  y_key / y_val need room for m entries.  Returns y_nnz. */
+EXPORT int oracle_spmspv_csc_host_faithful(int m, const int* colptr, const int* row,
+                                           const float* val, int x_nnz, const int* x_key,
+                                           const float* x_val, int* y_key, float* y_val) {
+  float* y = (float*)calloc((size_t)(m > 0 ? m : 1), sizeof(float));
+  for (int i = 0; i < x_nnz; i++) {
+    const int c = x_key[i];
+    const int xv = (int)x_val[i];
+    for (int j = colptr[c]; j < colptr[c + 1]; j++) y[row[j]] += val[j] * (float)xv;
+  }
+  int k = 0;
+  for (int r = 0; r < m; r++)
+    if (!(fabsf(y[r]) < FLT_EPSILON)) { y_key[k] = r; y_val[k] = y[r]; k++; }
+  free(y);
+  return k;
+}
+
+/* Stable CSR -> CSC transpose (rows ascending within each column), the
+ * layout the reference's ToCSC produces (cusparse csr2csc, spmspv.h:384-419).
+ * colptr[n+1], row[nnz], cval[nnz] (cval may be NULL).  Returns 0, or -1 for
+ * a column index out of range. */
+EXPORT int oracle_csr2csc(int m, int n, const int* rowptr, const int* col, const float* val,
+                          int* colptr, int* row, float* cval) {
+  const int nnz = rowptr[m];
+  memset(colptr, 0, sizeof(int) * (size_t)(n + 1));
+  for (int k = 0; k < nnz; k++) {
+    if ((unsigned)col[k] >= (unsigned)n) return -1;
+    colptr[col[k] + 1]++;
+  }
+  for (int c = 0; c < n; c++) colptr[c + 1] += colptr[c];
+  int* cur = (int*)malloc(sizeof(int) * (size_t)(n > 0 ? n : 1));
+  memcpy(cur, colptr, sizeof(int) * (size_t)n);
+  for (int r = 0; r < m; r++)
+    for (int k = rowptr[r]; k < rowptr[r + 1]; k++) {
+      const int p = cur[col[k]]++;
+      row[p] = r;
+      if (val && cval) cval[p] = val[k];
+    }
+  free(cur);
+  return 0;
 }
 
 /* ---- vector format conversions --------------------------------------------- */
@@ -560,4 +613,145 @@ EXPORT int oracle_coo2hybrid(int m, int n, const int* rowptr, const int* col, un
   free(cr);
   free(cc);
   return csr;
+}
+
+/* ---- synthetic inputs of the benchmark --------------------------------------
+ * A second, independent statement of the benchmark's input generators, so
+ * that the CPU reference arm of the benchmark builds its inputs without the
+ * product library.  The scheme (stated here in full; the product's
+ * generators follow the same one and a CPU test checks the outputs equal):
+ *   rng(seed, stream, ctr) = mix(mix(seed*0x632be59bd9b4e019 + stream) ^
+ *                                (ctr*0xd1b54a32d192ed03)), mix = splitmix64's
+ *   finaliser; u01 = (rng >> 11) / 2^53; normal = Box-Muller on two u01.
+ *   Streams: 2 Zipf length, 3 Zipf rounding, 4 Zipf total fix, 5 Zipf
+ *   column, 6 Zipf value, 10 vector position, 11 vector value. */
+static uint64_t gen_mix(uint64_t z) {
+  z += 0x9e3779b97f4a7c15ULL;
+  z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ULL;
+  z = (z ^ (z >> 27)) * 0x94d049bb133111ebULL;
+  return z ^ (z >> 31);
+}
+static uint64_t gen_rng(uint64_t seed, uint64_t stream, uint64_t ctr) {
+  return gen_mix(gen_mix(seed * 0x632be59bd9b4e019ULL + stream) ^ (ctr * 0xd1b54a32d192ed03ULL));
+}
+static double gen_u01(uint64_t seed, uint64_t stream, uint64_t ctr) {
+  return (double)(gen_rng(seed, stream, ctr) >> 11) * (1.0 / 9007199254740992.0);
+}
+static double gen_normal(uint64_t seed, uint64_t stream, uint64_t ctr) {
+  double u1 = gen_u01(seed, stream, 2 * ctr), u2 = gen_u01(seed, stream, 2 * ctr + 1);
+  if (u1 < 1e-300) u1 = 1e-300;
+  return sqrt(-2.0 * log(u1)) * cos(6.283185307179586 * u2);
+}
+static int gen_cmp_int(const void* a, const void* b) {
+  const int x = *(const int*)a, y = *(const int*)b;
+  return (x > y) - (x < y);
+}
+static int gen_unique(int* c, int len) {
+  int w = 0;
+  for (int k = 0; k < len; k++)
+    if (w == 0 || c[k] != c[w - 1]) c[w++] = c[k];
+  return w;
+}
+
+/* m x m matrix whose row lengths are Zipf(s) on [1, maxlen], scaled by
+ * mean / E[L] with stochastic rounding and clamped to [0, maxlen], the total
+ * then fixed to exactly mean * m by +-1 on random rows; per row distinct
+ * uniform columns (draw, sort, deduplicate, redraw the shortfall) and values
+ * U(-1, 1).  rowptr[m+1], col / val [mean*m] are the caller's.  Returns 0, or
+ * -1 for arguments out of range. */
+EXPORT int oracle_gen_zipf_rows(int m, double s, int mean, int maxlen, uint64_t seed, int* rowptr,
+                                int* col, float* val) {
+  if (m < 1 || mean < 0 || maxlen < 1 || maxlen > m) return -1;
+  const long long target = (long long)mean * m;
+  if (target > 2147483647LL || target > (long long)maxlen * m) return -1;
+  double* cdf = (double*)malloc(sizeof(double) * (size_t)maxlen);
+  double z = 0, ez = 0;
+  for (int k = 1; k <= maxlen; k++) {
+    const double p = pow((double)k, -s);
+    z += p;
+    ez += k * p;
+    cdf[k - 1] = z;
+  }
+  for (int k = 0; k < maxlen; k++) cdf[k] /= z;
+  ez /= z;
+  const double f = ez > 0 ? (double)mean / ez : 0.0;
+  int* len = (int*)malloc(sizeof(int) * (size_t)m);
+#pragma omp parallel for schedule(static)
+  for (int i = 0; i < m; i++) {
+    const double r = gen_u01(seed, 2, (uint64_t)i);
+    int lo = 0, hi = maxlen; /* first index with cdf >= r */
+    while (lo < hi) {
+      const int mid = lo + (hi - lo) / 2;
+      if (cdf[mid] < r) lo = mid + 1; else hi = mid;
+    }
+    const double scaled = (lo + 1) * f;
+    int L = (int)floor(scaled);
+    if (gen_u01(seed, 3, (uint64_t)i) < scaled - L) ++L;
+    len[i] = L < 0 ? 0 : (L > maxlen ? maxlen : L);
+  }
+  long long tot = 0;
+  for (int i = 0; i < m; i++) tot += len[i];
+  uint64_t ctr = 0;
+  while (tot != target) {
+    const int i = (int)(gen_rng(seed, 4, ctr++) % (uint64_t)m);
+    if (tot < target && len[i] < maxlen) { ++len[i]; ++tot; }
+    else if (tot > target && len[i] > 0) { --len[i]; --tot; }
+  }
+  rowptr[0] = 0;
+  for (int i = 0; i < m; i++) rowptr[i + 1] = rowptr[i] + len[i];
+#pragma omp parallel for schedule(dynamic, 256)
+  for (int i = 0; i < m; i++) {
+    const int L = len[i];
+    int* c = col + rowptr[i];
+    int have = 0;
+    uint64_t t = 0;
+    while (have < L) {
+      for (int k = have; k < L; k++)
+        c[k] = (int)(gen_rng(seed, 5, ((uint64_t)i << 24) + t++) % (uint64_t)m);
+      qsort(c, (size_t)L, sizeof(int), gen_cmp_int);
+      have = gen_unique(c, L);
+    }
+    for (int k = 0; k < L; k++)
+      val[rowptr[i] + k] = (float)(2.0 * gen_u01(seed, 6, (uint64_t)rowptr[i] + k) - 1.0);
+  }
+  free(len);
+  free(cdf);
+  return 0;
+}
+
+/* k distinct positions in [0, n), sorted, with U(-1,1) (dist 0) or N(0,1)
+ * values: a partial Fisher-Yates over [0, n) when 3k >= n, else draws in
+ * order keeping first occurrences.  Returns 0, or -1 for k outside [0, n]. */
+EXPORT int oracle_gen_sparse_vector(int n, int k, int dist, uint64_t seed, int* key, float* val) {
+  if (n < 0 || k < 0 || k > n) return -1;
+  if (k == 0) return 0;
+  if ((long long)k * 3 >= n) {
+    int* p = (int*)malloc(sizeof(int) * (size_t)n);
+    for (int i = 0; i < n; i++) p[i] = i;
+    for (int i = 0; i < k; i++) {
+      const int j = i + (int)(gen_rng(seed, 10, (uint64_t)i) % (uint64_t)(n - i));
+      const int t = p[i];
+      p[i] = p[j];
+      p[j] = t;
+    }
+    memcpy(key, p, sizeof(int) * (size_t)k);
+    free(p);
+  } else {
+    unsigned char* seen = (unsigned char*)calloc((size_t)n / 8 + 1, 1);
+    uint64_t t = 0;
+    int have = 0;
+    while (have < k) {
+      const int c = (int)(gen_rng(seed, 10, t++) % (uint64_t)n);
+      if (!(seen[c >> 3] & (1u << (c & 7)))) {
+        seen[c >> 3] |= (unsigned char)(1u << (c & 7));
+        key[have++] = c;
+      }
+    }
+    free(seen);
+  }
+  qsort(key, (size_t)k, sizeof(int), gen_cmp_int);
+  for (int i = 0; i < k; i++)
+    val[i] = dist == 0 ? (float)(2.0 * gen_u01(seed, 11, (uint64_t)i) - 1.0)
+                       : (float)gen_normal(seed, 11, (uint64_t)i);
+  return 0;
 }

@@ -68,3 +68,20 @@ def test_sparse_vector(n, k):
     assert (np.diff(key) > 0).all() if k > 1 else True
     if k:
         assert key.min() >= 0 and key.max() < n and (np.abs(val) <= 1).all()
+
+
+def test_oracle_generators_equal_product_generators():
+    """The oracle's restatement of the benchmark's generators (used by the
+    CPU reference arm, which loads nothing from the product) produces the
+    same bits as the product's generators."""
+    import oracle.oracle as orc
+    for m, seed in ((20000, 2), (4096, 9)):
+        A = gen.zipf_rows(m, 1.5, 16, min(10000, m), seed=seed)
+        B = orc.gen_zipf_rows(m, 1.5, 16, min(10000, m), seed=seed)
+        assert np.array_equal(A.rowptr, B.rowptr) and np.array_equal(A.col, B.col)
+        assert np.array_equal(A.val.view(np.uint32), B.val.view(np.uint32))
+        assert all(np.array_equal(x, y) for x, y in zip(A.to_csc(), B.to_csc()))
+    for n, k, dist in ((10**6, 11, "uniform"), (10**6, 105, "normal"), (3000, 1000, "uniform"),
+                       (3000, 2999, "normal"), (3000, 3000, "uniform"), (50, 0, "uniform")):
+        a, b = gen.sparse_vector(n, k, dist=dist, seed=k + 1), orc.gen_sparse_vector(n, k, dist, k + 1)
+        assert np.array_equal(a[0], b[0]) and np.array_equal(a[1].view(np.uint32), b[1].view(np.uint32))

@@ -1,14 +1,15 @@
 """Pin the oracle against the reference's own serial routines, compiled from
-its sources by oracle/build_ref.sh into oracle/_ref/libref_host.so (built by
-__graft_entry__.build() wherever the reference tree is present).
+its sources by oracle/build_ref.sh into oracle/_ref/libref_host.so and
+oracle/_ref/libref_csc.so (built by __graft_entry__.build() wherever the
+reference tree is present).
 
   serialspmv (test/test_application.cu:107-116)       == oracle_serialspmv_f32, bit for bit
   computeMatFeture_serial (spmspv.h:2275-2335)        == oracle_mat_features_faithful, bit for bit
   extractMatFeature (spmspv.h:423-447)                == oracle_std_row_intmean_faithful, bit for bit
-SpmSpvCSCHost (test/test_sort_spmspv.cu:330-375) lives in a driver that no
-longer compiles against the reference's own handle API, so it is not pinned
-here; the oracle checks its CSC restatement against serialspmv instead
-(tests/test_oracle.py).
+  SpmSpvCSCHost (test/test_sort_spmspv.cu:330-375)    == oracle_spmspv_csc_host_faithful, bit for bit
+SpmSpvCSCHost reads x into an int; on integer-valued x that changes nothing,
+and there the FP64 CSC oracle the GPU tests use agrees with it within FP32
+accumulation error.
 """
 import ctypes
 import os
@@ -21,6 +22,7 @@ import oracle.oracle as orc
 
 SO = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "oracle", "_ref",
                   "libref_host.so")
+SO_CSC = os.path.join(os.path.dirname(SO), "libref_csc.so")
 
 
 @pytest.fixture(scope="module")
@@ -115,3 +117,76 @@ def test_coo2hybrid_split_matches_reference(ref, idx):
     o = np.lexsort((r0[~flags], A.col[~flags]))
     assert np.array_equal(row[kk:], r0[~flags][o]) and np.array_equal(col[kk:], A.col[~flags][o])
     assert np.array_equal(val[kk:].view(np.uint32), A.val[~flags][o].view(np.uint32))
+
+
+@pytest.fixture(scope="module")
+def ref_csc():
+    if not os.path.exists(SO_CSC):
+        pytest.skip("oracle/_ref/libref_csc.so not built (no reference tree on this machine)")
+    lib = ctypes.CDLL(SO_CSC)
+    P = ctypes.c_void_p
+    lib.ref_spmspv_csc_host.argtypes = [ctypes.c_int] * 3 + [P] * 3 + [ctypes.c_int] + [P] * 5
+    lib.ref_spmspv_csc_host.restype = None
+    return lib
+
+
+def _ref_csc_call(lib, A, csc, key, xv):
+    colptr, row, cval = (np.ascontiguousarray(a) for a in csc)
+    key, xv = np.ascontiguousarray(key, np.int32), np.ascontiguousarray(xv, np.float32)
+    yn = ctypes.c_int()
+    yk = np.zeros(max(A.m, 1), np.int32)
+    yv = np.zeros(max(A.m, 1), np.float32)
+    lib.ref_spmspv_csc_host(A.m, A.n, A.nnz, row.ctypes.data, colptr.ctypes.data, cval.ctypes.data,
+                            len(key), key.ctypes.data, xv.ctypes.data, ctypes.byref(yn),
+                            yk.ctypes.data, yv.ctypes.data)
+    return yk[:yn.value], yv[:yn.value]
+
+
+@pytest.mark.parametrize("idx", range(4))
+@pytest.mark.parametrize("xkind", ["integer", "uniform", "mixed"])
+def test_spmspv_csc_host_bit_exact(ref_csc, idx, xkind):
+    """The reference's SpmSpvCSCHost against the oracle's faithful form, bit
+    for bit: integer-valued x (the int read keeps it), U(-1,1) x (the int read
+    makes every product 0 and the output empty) and values in (-4, 4) (the
+    read truncates toward zero)."""
+    A = list(_mats())[idx]
+    csc = A.to_csc()
+    rng = np.random.default_rng(100 + idx)
+    k = max(1, A.n // 7)
+    key = np.sort(rng.choice(A.n, k, replace=False)).astype(np.int32)
+    if xkind == "integer":
+        xv = rng.integers(-3, 4, k).astype(np.float32)
+    elif xkind == "uniform":
+        xv = rng.uniform(-1, 1, k).astype(np.float32)
+    else:
+        xv = rng.uniform(-4, 4, k).astype(np.float32)
+    rk, rv = _ref_csc_call(ref_csc, A, csc, key, xv)
+    ok, ov = orc.spmspv_csc_host_faithful(A.m, *csc, key, xv)
+    assert np.array_equal(rk, ok)
+    assert np.array_equal(rv.view(np.uint32), ov.view(np.uint32))
+    if xkind == "uniform":
+        assert len(rk) == 0
+    if xkind == "integer":
+        # the FP64 oracle of the GPU tests agrees with the reference's output
+        y64, mag, _ = orc.spmspv_csc_f64(A.m, *csc, key, xv)
+        dense = np.zeros(A.m, np.float32)
+        dense[rk] = rv
+        _, good = orc.within_tol(dense, y64, mag, 1e-4)
+        # entries the reference drops as IS_FLOAT_ZERO are within FLT_EPSILON of 0
+        assert (good | (np.abs(y64) < 2 * np.finfo(np.float32).eps)).all()
+
+
+def test_spmspv_csc_host_edge_cases(ref_csc):
+    """Empty x, a column without nonzeros and an exactly cancelling row."""
+    from spmx.gen import Csr
+    # column 1 is empty; row 0 gets 0.5*2 + (-1)*1 = 0 exactly
+    A = Csr(3, 3, np.array([0, 2, 3, 4], np.int32), np.array([0, 2, 0, 2], np.int32),
+            np.array([0.5, -1.0, 0.25, 3.0], np.float32))
+    csc = A.to_csc()
+    for key, xv in ((np.zeros(0, np.int32), np.zeros(0, np.float32)),
+                    (np.array([1], np.int32), np.array([2.0], np.float32)),
+                    (np.array([0, 1, 2], np.int32), np.array([2.0, 5.0, 1.0], np.float32))):
+        rk, rv = _ref_csc_call(ref_csc, A, csc, key, xv)
+        ok, ov = orc.spmspv_csc_host_faithful(A.m, *csc, key, xv)
+        assert np.array_equal(rk, ok) and np.array_equal(rv.view(np.uint32), ov.view(np.uint32))
+    assert list(rk) == [1, 2]  # row 0 cancelled to exactly 0 and is dropped
