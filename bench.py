@@ -447,14 +447,16 @@ def run_ours(args, world, rank, local):
     # oracle with the parity tests' magnitude-scaled bound, plus the raw
     # relative and normwise errors ---
     correctness = []
+    ref64 = []
+    import oracle.oracle as orc
     if rank == 0:
-        import oracle.oracle as orc
         colptr_h, row_h, cval_h = A.to_csc()
         for (dd, kd, vd, k), (_, key, val) in zip(dx, xs):
             h.set_sparse_x(kd, vd, k)
             h.run_adaptive(1.0, y)
             yh = y.cpu().numpy().astype(np.float64)
             y64, mag, _ = orc.spmspv_csc_f64(m, colptr_h, row_h, cval_h, key, val)
+            ref64.append((y64, mag))
             nz = y64 != 0
             rel = float(np.max(np.abs(yh[nz] - y64[nz]) / np.abs(y64[nz]))) if nz.any() else 0.0
             top = float(np.max(np.abs(y64))) if len(y64) else 0.0
@@ -465,44 +467,51 @@ def run_ours(args, world, rank, local):
 
     # --- e2e through the public API with host buffers.  Per call: the
     # pinned host->device copy of x, the adaptive call, and the read-back of
-    # y: for a sparse x the nonzeros of y (dense2sparse_outer, which returns
-    # the count to the host, then a copy of that many keys and values), for
-    # the dense x the dense y. ---
+    # y: for a sparse x the nonzeros of y, compacted straight into pinned host
+    # memory with their count (spmx_dense2sparse_to_host, no host round trip
+    # inside the call), for the dense x the dense y.  One stream
+    # synchronisation per call, at its end. ---
     pin_k = [torch.from_numpy(np.ascontiguousarray(k)).pin_memory() for _, k, _ in xs]
     pin_v = [torch.from_numpy(np.ascontiguousarray(v)).pin_memory() for _, _, v in xs]
     kbuf = torch.empty(n, dtype=torch.int32, device=dev)
     vbuf = torch.empty(n, dtype=torch.float32, device=dev)
-    ykey = torch.empty(m, dtype=torch.int32, device=dev)
-    yval = torch.empty(m, dtype=torch.float32, device=dev)
     yhost = torch.empty(m, dtype=torch.float32).pin_memory()
     ykey_h = torch.empty(m, dtype=torch.int32).pin_memory()
     yval_h = torch.empty(m, dtype=torch.float32).pin_memory()
+    ycnt_h = torch.zeros(1, dtype=torch.int32).pin_memory()
     h2d = sum(8 * len(k) for _, k, _ in xs)
     d2h_calls = []
+    e2e_ok = []
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
 
-    def e2e_step():
+    def e2e_step(check=False):
         tot = 0.0
         d2h_calls.clear()
         for i in range(len(xs)):
             k = len(xs[i][1])
+            sparse_out = xs[i][0] < 1.0
             flush.fill_(2.0)
             e0.record(stream)
             kbuf[:k].copy_(pin_k[i], non_blocking=True)
             vbuf[:k].copy_(pin_v[i], non_blocking=True)
             h.set_sparse_x(kbuf, vbuf, k)
             h.run_adaptive(1.0, y)
-            if xs[i][0] < 1.0:
-                ynz = h.dense2sparse_outer(m, y, ykey, yval)  # count read back to the host
-                ykey_h[:ynz].copy_(ykey[:ynz], non_blocking=True)
-                yval_h[:ynz].copy_(yval[:ynz], non_blocking=True)
-                d2h_calls.append(4 + 8 * ynz)
+            if sparse_out:
+                h.dense2sparse_to_host(m, y, ykey_h, yval_h, ycnt_h)
             else:
                 yhost.copy_(y, non_blocking=True)
-                d2h_calls.append(4 * m)
             e1.record(stream)
             stream.synchronize()
             tot += e0.elapsed_time(e1)
+            ynz = int(ycnt_h[0]) if sparse_out else m
+            d2h_calls.append(4 + 8 * ynz if sparse_out else 4 * m)
+            if check and ref64:
+                got = np.zeros(m, np.float64)
+                if sparse_out:
+                    got[ykey_h[:ynz].numpy()] = yval_h[:ynz].numpy()
+                else:
+                    got[:] = yhost.numpy()
+                e2e_ok.append(bool(orc.within_tol(got, ref64[i][0], ref64[i][1], 1e-5)[0]))
         return tot
 
     for _ in range(max(args.warmup, 3)):
@@ -512,6 +521,7 @@ def run_ours(args, world, rank, local):
     e2e_ms = allmax(e2e_ms, world)
     d2h = sum(d2h_calls)
     e2e_val = world * total_bytes / (e2e_ms * 1e-3) / 1e9
+    e2e_step(check=True)  # untimed: the host-side results against the FP64 oracle
 
     # --- the selector against exhaustive timing of all eight kernels (rank 0,
     # after the last collective) ---
@@ -568,7 +578,8 @@ def run_ours(args, world, rank, local):
                          "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
                          "bytes_per_launch": sb, "ms_per_launch": k_ms},
             "e2e": {"value": e2e_val, "unit": "GB/s", "h2d_bytes_per_step": h2d,
-                    "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms},
+                    "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms,
+                    "host_results_within_1e-5": bool(e2e_ok) and all(e2e_ok)},
             "gpu_launches": int(launches // max(args.steps, 1)),
             "clocks": clk.summary(),
             "sweep": sweep,
@@ -663,6 +674,13 @@ def run_bfs_batched(torch, dev, stream, args):
         tp.append(s.elapsed_time(e))
     h.check_device_error()
     exact = bool(torch.equal(lv_b, lv_p))
+    # full-size parity: sampled sources of the batch against the oracle's
+    # queue BFS on the host (bit for bit)
+    import oracle.oracle as orc
+    sampled = (0, 21, 42, 63)
+    lvh = lv_b.view(64, n)
+    oracle_ok = all(np.array_equal(lvh[i].cpu().numpy(), orc.bfs_queue(n, g.rowptr, g.col, srcs[i])[0])
+                    for i in sampled)
     degd = torch.from_numpy(deg.astype(np.int64)).to(dev)
     reached = (lv_p.view(64, n) >= 0).to(torch.int64)
     edges = int((reached * degd).sum().item()) // 2
@@ -671,7 +689,8 @@ def run_bfs_batched(torch, dev, stream, args):
     return {"graph": "rmat scale 22, edge factor 16, seed 3, 64 sources (seed 3)",
             "batched_ms": mb, "plain64_ms": mp, "edges": edges,
             "batched_gteps": edges / (mb * 1e-3) / 1e9, "plain64_gteps": edges / (mp * 1e-3) / 1e9,
-            "speedup": mp / mb, "bit_exact_vs_plain": exact}
+            "speedup": mp / mb, "bit_exact_vs_plain": exact,
+            "bit_exact_vs_oracle": {"sources": [int(srcs[i]) for i in sampled], "ok": bool(oracle_ok)}}
 
 
 def run_batched_spmspv(torch, dev, stream, args):
@@ -744,6 +763,30 @@ def run_batched_spmspv(torch, dev, stream, args):
         y64, mag, _ = orc.spmspv_csc_f64(m, colptr_h, row_h, cval_h, xkey[a:b], xval[a:b])
         Yh = Y[:, v].cpu().numpy()
         ok = ok and orc.within_tol(Yh, y64, mag, 1e-5)[0]
+    # backward parity at full size: dxval of the sampled vectors against FP64
+    # A^T dy over the whole matrix, dvals on 4,096 sampled nonzeros against
+    # FP64 sums over the batch's entries in their column
+    bwd_ok = True
+    for v in (0, nvec // 2, int(np.argmax(sizes))):
+        a, b = xptr[v], xptr[v + 1]
+        dx64, adx = orc.spmv_t_f64(n, A.rowptr, A.col, A.val, dY[:, v].cpu().numpy())
+        kk = xkey[a:b]
+        bwd_ok = bwd_ok and orc.within_tol(dxval[a:b].cpu().numpy(), dx64[kk], adx[kk], 1e-5)[0]
+    ks = np.sort(rng.choice(A.nnz, 4096, replace=False))
+    rows_k = np.searchsorted(A.rowptr, ks, side="right") - 1
+    cols_k = A.col[ks]
+    order = np.argsort(xkey, kind="stable")
+    skey = xkey[order]
+    svec = np.repeat(np.arange(nvec), sizes)[order]
+    sval = xval[order].astype(np.float64)
+    dyr = dY[torch.from_numpy(rows_k).to(dev)].cpu().numpy().astype(np.float64)  # 4,096 x nvec
+    lo, hi = np.searchsorted(skey, cols_k, "left"), np.searchsorted(skey, cols_k, "right")
+    dv64, dvmag = np.zeros(len(ks)), np.zeros(len(ks))
+    for i in range(len(ks)):
+        terms = sval[lo[i]:hi[i]] * dyr[i, svec[lo[i]:hi[i]]]
+        dv64[i], dvmag[i] = terms.sum(), np.abs(terms).sum()
+    got_dv = dvals[torch.from_numpy(ks).to(dev)].cpu().numpy()
+    bwd_ok = bool(bwd_ok and orc.within_tol(got_dv, dv64, dvmag, 1e-5)[0])
     bins = int(np.sum(colptr_h[xkey + 1] - colptr_h[xkey]))
     # 256 sequential single-vector calls: the forward through the adaptive
     # single-vector engine (selector + CSC SpMSpV into a dense y), the backward
@@ -782,6 +825,7 @@ def run_batched_spmspv(torch, dev, stream, args):
             "nnz": int(A.nnz), "nvec": nvec, "x_nnz_total": xn, "products": bins,
             "graph_fwd_bwd_ms": mb, "plain256_fwd_bwd_ms": mp, "speedup": mp / mb,
             "eff_gbs": (fwd_b + bwd_b) / (mb * 1e-3) / 1e9, "forward_within_1e-5": bool(ok),
+            "backward_within_1e-5": bwd_ok,
             "note": "single calls: adaptive single-vector SpMSpV forward + one-vector backward "
                     "without dvals (less work than the batch, which also computes dvals)"}
 

@@ -171,6 +171,16 @@ int spmx_dense2bitarray(spmx_handle_t h);
 /* dense2sparse_outer — H:1953-1998 (no cudaMalloc per call here) */
 int spmx_dense2sparse_outer(spmx_handle_t h, int m, const float* d_dense,
                             int* ynnz, int* d_key, float* d_val);
+/* dense2sparse_outer — H:1953-1998, with the result written straight into
+ * host memory: the nonzeros of d_dense[m] (in index order) go to h_key /
+ * h_val and their count to *h_count, all three page-locked host buffers
+ * mapped into the device's address space (cudaHostAlloc / cudaMallocHost on
+ * a unified-addressing system; anything else is rejected).  No host
+ * synchronisation: the values are there once the handle's stream has
+ * reached this call (synchronise it, or wait on an event, before reading).
+ * h_key / h_val need room for m entries. */
+int spmx_dense2sparse_to_host(spmx_handle_t h, int m, const float* d_dense, int* h_key,
+                              float* h_val, int* h_count);
 /* sparse2dense_outer — H:1931-1950 */
 int spmx_sparse2dense_outer(spmx_handle_t h, int ynnz, const int* d_key,
                             const float* d_val, int m, float* d_dense);
@@ -329,6 +339,14 @@ int spmx_spmspv_csc_noalloc(int m, int n, int nnz, const int* d_csc_row,
                             const int* d_csc_col, const float* d_csc_val,
                             int x_nnz, const int* d_x_key, const float* d_x_val,
                             float alpha, float* d_y, void* stream);
+/* No counterpart in the reference.  Reads the device error word of the last
+ * spmx_spmspv_csc_noalloc call on the current device: synchronises `stream`,
+ * copies 4 bytes out of the fixed scratch array (nothing is allocated) and
+ * returns SPMX_ERR_OOB for an x key outside [0, n) or a row index outside
+ * [0, m) that the kernels skipped, SPMX_ERR_TIMEOUT for a bounded wait that
+ * gave up, else SPMX_SUCCESS.  Call it after the SpMSpV call, on the same
+ * stream, before the next one (each call clears the word). */
+int spmx_spmspv_csc_noalloc_check(void* stream);
 
 /* ======================= features / selector ============================== */
 /* computeBinlenVer2 — H:2703-2723 (sum of the column lengths of x's keys) */

@@ -131,7 +131,7 @@ bucket_reduce_kernel(int m, int rshift, int nb, const int* __restrict__ boff,
   unsigned total;
   (void)block_exclusive_sum<NT>(cnt, s_wtmp, &total);
   if (tid < 32) {
-    const unsigned p = lb_warp_lookback(st, bkt, total, err);
+    const unsigned p = lb_warp_lookback(st, bkt, nb, total, err);
     if (tid == 0) { s_prefix = p; s_total = total; }
   }
   __syncthreads();
@@ -198,7 +198,7 @@ int launch_bucket_spmspv(const CscArgs& a, const CscScratch& s, const BucketScra
   bucket_scatter_kernel<NT, VT><<<grid, NT, hist_bytes, st>>>(a, s, variant, rshift, nb, bs.cursor,
                                                              bs.prow, bs.pval, bs.cap);
   if (nb > ls.status_len) return -1;
-  LookbackState lbs{ls.status, ls.ticket, ++ls.epoch};
+  LookbackState lbs{ls.status, ls.ticket};
   const int R = 1 << rshift;
   note_launch();
   bucket_reduce_kernel<256><<<nb, 256, 4 * (R + R / 32), st>>>(

@@ -182,11 +182,18 @@ __device__ __forceinline__ void st_volatile_u64(unsigned long long* p,
 // launch order through an atomic ticket, so every predecessor of a tile is
 // already resident and the look-back always terminates; the wait is still
 // bounded and reports kDevErrTimeout instead of hanging.
+//
+// The epoch lives in device memory (words[1]), not in the launch parameters:
+// every tile reads it when its look-back starts, and the launch's last tile to
+// publish its prefix (counted in words[2]) advances it for the next launch.
+// All tiles of a launch have read the epoch before that last publish, and the
+// next launch on the stream starts after this one ends, so each launch sees a
+// fresh epoch even when it is a replay of a captured CUDA graph (whose launch
+// parameters never change).  words[0..2] start at zero.
 // ---------------------------------------------------------------------------
 struct LookbackState {
   unsigned long long* status;  // one word per tile
-  unsigned* ticket;            // tile ticket, reset by the last tile
-  unsigned epoch;              // 30-bit launch epoch (host increments)
+  unsigned* words;             // [0] tile ticket, [1] epoch, [2] tiles published
 };
 
 __device__ __forceinline__ unsigned long long lb_pack(unsigned epoch,
@@ -200,10 +207,10 @@ __device__ __forceinline__ unsigned long long lb_pack(unsigned epoch,
 __device__ __forceinline__ int lb_acquire_tile(const LookbackState& st,
                                                int ntiles, int* smem_word) {
   if (threadIdx.x == 0) {
-    unsigned t = atomicAdd(st.ticket, 1u);
+    unsigned t = atomicAdd(st.words, 1u);
     // The last tile handed out resets the ticket for the next launch: every
     // other tile already holds its id, and the grid has exactly ntiles CTAs.
-    if ((int)t == ntiles - 1) atomicExch(st.ticket, 0u);
+    if ((int)t == ntiles - 1) atomicExch(st.words, 0u);
     *smem_word = (int)t;
   }
   __syncthreads();
@@ -212,19 +219,34 @@ __device__ __forceinline__ int lb_acquire_tile(const LookbackState& st,
   return t;
 }
 
-// Called by warp 0 only.  Publishes the tile aggregate, looks back over the
-// predecessors and publishes the inclusive prefix.  Returns the exclusive
-// prefix of the tile (valid in all lanes of warp 0).
+// lane 0: count this tile's publish; the launch's last one advances the epoch
+__device__ __forceinline__ void lb_published(const LookbackState& st, int ntiles) {
+  if (atomicAdd(st.words + 2, 1u) == (unsigned)ntiles - 1u) {
+    atomicExch(st.words + 2, 0u);
+    atomicAdd(st.words + 1, 1u);
+  }
+}
+
+// Called by warp 0 of every tile (all ntiles of them).  Publishes the tile
+// aggregate, looks back over the predecessors and publishes the inclusive
+// prefix.  Returns the exclusive prefix of the tile (valid in all lanes of
+// warp 0).
 __device__ __forceinline__ unsigned lb_warp_lookback(const LookbackState& st,
-                                                     int tile,
+                                                     int tile, int ntiles,
                                                      unsigned aggregate,
                                                      int* err) {
   const unsigned lane = lane_id();
+  unsigned epoch = 0;
+  if (lane == 0) epoch = *reinterpret_cast<volatile unsigned*>(st.words + 1);
+  epoch = __shfl_sync(0xffffffffu, epoch, 0) & 0x3fffffffu;
   if (tile == 0) {
-    if (lane == 0) st_volatile_u64(&st.status[0], lb_pack(st.epoch, 2u, aggregate));
+    if (lane == 0) {
+      st_volatile_u64(&st.status[0], lb_pack(epoch, 2u, aggregate));
+      lb_published(st, ntiles);
+    }
     return 0u;
   }
-  if (lane == 0) st_volatile_u64(&st.status[tile], lb_pack(st.epoch, 1u, aggregate));
+  if (lane == 0) st_volatile_u64(&st.status[tile], lb_pack(epoch, 1u, aggregate));
   unsigned exclusive = 0;
   int j = tile - 1;
   bool timed_out = false;
@@ -236,7 +258,7 @@ __device__ __forceinline__ unsigned lb_warp_lookback(const LookbackState& st,
       if (idx >= 0) {
         unsigned long long w = ld_volatile_u64(&st.status[idx]);
         unsigned ep = (unsigned)(w >> 34);
-        state = (ep == (st.epoch & 0x3fffffffu)) ? (unsigned)((w >> 32) & 3u) : 0u;
+        state = (ep == epoch) ? (unsigned)((w >> 32) & 3u) : 0u;
         value = (unsigned)w;
       }
       if (!__any_sync(0xffffffffu, state == 0u)) break;
@@ -255,8 +277,10 @@ __device__ __forceinline__ unsigned lb_warp_lookback(const LookbackState& st,
     if (pmask) break;
     j -= 32;
   }
-  if (lane == 0)
-    st_volatile_u64(&st.status[tile], lb_pack(st.epoch, 2u, exclusive + aggregate));
+  if (lane == 0) {
+    st_volatile_u64(&st.status[tile], lb_pack(epoch, 2u, exclusive + aggregate));
+    lb_published(st, ntiles);
+  }
   return exclusive;
 }
 

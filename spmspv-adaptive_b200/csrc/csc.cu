@@ -62,7 +62,7 @@ csc_scan_kernel(CscArgs a, CscScratch s, LookbackState st, int ntiles, int K) {
   unsigned total;
   const unsigned ex = block_exclusive_sum<NT>(sum, s_wtmp, &total);
   if (tid < 32) {
-    const unsigned p = lb_warp_lookback(st, tile, total, a.err);
+    const unsigned p = lb_warp_lookback(st, tile, ntiles, total, a.err);
     if (tid == 0) s_prefix = p;
   }
   __syncthreads();
@@ -187,7 +187,7 @@ int launch_csc_scan(const CscArgs& a, const CscScratch& s, ScanScratch& ls,
   const int ntiles = (a.x_nnz + NT * VT - 1) / (NT * VT);
   if (ntiles <= 0) return 0;
   if (ntiles > ls.status_len) return -1;
-  LookbackState lbs{ls.status, ls.ticket, ++ls.epoch};
+  LookbackState lbs{ls.status, ls.ticket};
   note_launch();
   csc_scan_kernel<NT, VT><<<ntiles, NT, 0, st>>>(a, s, lbs, ntiles, block_items);
   return 0;

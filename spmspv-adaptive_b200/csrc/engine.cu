@@ -534,6 +534,36 @@ extern "C" int spmx_dense2sparse_outer(spmx_handle_t h, int m, const float* dens
   return dense_to_sparse(h, m, dense, key, val, kCntYnnz, ynnz);
 }
 
+// a page-locked host buffer the device can address (UVA-mapped)
+static int host_mapped(const void* p, const char* what) {
+  cudaPointerAttributes at{};
+  if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
+    cudaGetLastError();
+    return set_error(SPMX_ERR_INVALID_VALUE, std::string(what) + " is not a pointer CUDA knows");
+  }
+  if (at.type != cudaMemoryTypeHost || at.devicePointer != p)
+    return set_error(SPMX_ERR_INVALID_VALUE,
+                     std::string(what) + " must be page-locked host memory mapped into the device's "
+                                         "address space (cudaHostAlloc / cudaMallocHost)");
+  return SPMX_SUCCESS;
+}
+
+extern "C" int spmx_dense2sparse_to_host(spmx_handle_t h, int m, const float* dense, int* h_key,
+                                         float* h_val, int* h_count) {
+  SPMX_CHECK_HANDLE(h);
+  if (m < 0 || !h_count || (m > 0 && (!dense || !h_key || !h_val)))
+    return set_error(SPMX_ERR_INVALID_VALUE, "bad dense2sparse_to_host arguments");
+  SPMX_TRY(host_mapped(h_count, "h_count"));
+  if (m > 0) {
+    SPMX_TRY(host_mapped(h_key, "h_key"));
+    SPMX_TRY(host_mapped(h_val, "h_val"));
+  }
+  SPMX_TRY(ensure_scan_tiles(h, ((long long)m + 2047) / 2048));
+  if (launch_compact_nonzero(m, dense, h_key, h_val, h_count, h->ls, h->d_err, h->stream))
+    return set_error(SPMX_ERR_INVALID_VALUE, "compaction capacity");
+  return launch_ok("dense2sparse_to_host");
+}
+
 extern "C" int spmx_sparse2dense_outer(spmx_handle_t h, int ynnz, const int* key,
                                        const float* val, int m, float* dense) {
   SPMX_CHECK_HANDLE(h);

@@ -54,8 +54,7 @@ int launch_spmv_backward_sparse(int m, int n, const int* rowptr, const int* col,
 struct ScanScratch {
   unsigned long long* status;  // tile status words
   int status_len;              // capacity in tiles
-  unsigned* ticket;            // one ticket word
-  unsigned epoch;              // bumped by the caller per launch
+  unsigned* ticket;            // 4 words, zeroed once: ticket, epoch, publish count
 };
 
 // indices into the handle's device counter block

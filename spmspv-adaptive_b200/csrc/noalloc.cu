@@ -18,15 +18,20 @@
 //
 // Host code cannot use the array's name as a device address (in host code it
 // names a host-side stand-in), so the first call on each device looks up the
-// real address with cudaGetSymbolAddress while that device is current and
-// caches it; make that first call before any stream capture.  Every call on a
-// device shares the one array and leaves its contents behind: what must start
-// at zero (the tile ticket, the error word) is cleared at the start of every
-// call, and the look-back status words carry a per-call epoch.  Calls whose
-// work overlaps on the GPU (different streams, or host threads racing) would
-// corrupt each other's scratch: serialise them, e.g. on one stream.
+// real address with cudaGetSymbolAddress while that device is current, sizes
+// the launch grid from the device's SM count and caches both; make that first
+// call before any stream capture.  Every call on a device shares the one array
+// and leaves its contents behind: what must start at zero (the look-back
+// status words, the tile ticket and epoch, the error word) is cleared by a
+// small memset at the start of every call.  Calls whose work overlaps on the
+// GPU (different streams, or host threads racing) would corrupt each other's
+// scratch: serialise them, e.g. on one stream.
+//
+// Bad input (an x key outside [0, n), a row index outside [0, m)) and a
+// bounded wait that gave up are recorded in an error word in the same array,
+// never as a fault.  spmx_spmspv_csc_noalloc_check reads that word after a
+// call (it synchronises the stream and copies 4 bytes; it allocates nothing).
 #include <algorithm>
-#include <atomic>
 #include <mutex>
 #include <string>
 
@@ -49,20 +54,31 @@ constexpr size_t kOffBytes = align256(4 * (size_t)(kNoAllocMaxX + 1));
 constexpr size_t kColstartBytes = align256(4 * (size_t)kNoAllocMaxX);
 constexpr size_t kBstartBytes = align256(4 * (size_t)kNoAllocMaxBlocks);
 constexpr size_t kStatusBytes = align256(8 * (size_t)kNoAllocMaxTiles);
-constexpr size_t kWordsBytes = 256;  // ticket (4 words) + counts (16) + err
-constexpr size_t kNoAllocScratchBytes =
-    kOffBytes + kColstartBytes + 2 * kBstartBytes + kStatusBytes + kWordsBytes;
+constexpr size_t kWordsBytes = 256;  // ticket words (4) + counts (16) + err
+constexpr size_t kStatusOffset = kOffBytes + kColstartBytes + 2 * kBstartBytes;
+constexpr size_t kWordsOffset = kStatusOffset + kStatusBytes;
+constexpr size_t kErrOffset = kWordsOffset + 16 + 4 * (size_t)spmx::kCntTotal;
+constexpr size_t kNoAllocScratchBytes = kWordsOffset + kWordsBytes;
+static_assert(kErrOffset + 4 <= kNoAllocScratchBytes, "error word inside the scratch array");
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
 
 constexpr int kMaxDevices = 64;
 std::mutex g_setup_mu;
 unsigned char* g_base[kMaxDevices] = {nullptr};
-std::atomic<unsigned> g_epoch[kMaxDevices];
+int g_grid[kMaxDevices] = {0};
 
-// device address of the scratch array on the current device (set-up on the
-// first call per device)
-int scratch_base(int dev, unsigned char** base) {
+}  // namespace
+
+namespace spmx {
+int csc_lb_blocks_per_sm();
+}
+
+namespace {
+
+// device address of the scratch array and the load-balanced kernel's grid on
+// the current device (set-up on the first call per device)
+int scratch_base(int dev, unsigned char** base, int* grid) {
   std::lock_guard<std::mutex> lock(g_setup_mu);
   if (!g_base[dev]) {
     void* p = nullptr;
@@ -72,17 +88,20 @@ int scratch_base(int dev, unsigned char** base) {
       return spmx::set_error(SPMX_ERR_CUDA, std::string("cudaGetSymbolAddress(noalloc scratch): ") +
                                                 cudaGetErrorString(e));
     }
+    int sms = 0;
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) {
+      cudaGetLastError();
+      sms = 1;
+    }
+    g_grid[dev] = std::max(1, sms) * std::max(1, spmx::csc_lb_blocks_per_sm());
     g_base[dev] = static_cast<unsigned char*>(p);
   }
   *base = g_base[dev];
+  *grid = g_grid[dev];
   return SPMX_SUCCESS;
 }
 
 }  // namespace
-
-namespace spmx {
-int csc_lb_blocks_per_sm();
-}
 
 using namespace spmx;
 
@@ -116,7 +135,8 @@ extern "C" int spmx_spmspv_csc_noalloc(int m, int n, int nnz, const int* d_csc_r
     return set_error(SPMX_ERR_NO_DEVICE, "noalloc SpMSpV: no usable current device");
   }
   unsigned char* base = nullptr;
-  const int rc = scratch_base(dev, &base);
+  int grid = 1;
+  const int rc = scratch_base(dev, &base, &grid);
   if (rc) return rc;
 
   unsigned char* p = base;
@@ -132,27 +152,38 @@ extern "C" int spmx_spmspv_csc_noalloc(int m, int n, int nnz, const int* d_csc_r
   s.tl_cap = kNoAllocMaxBlocks;
   s.mg_cap = kNoAllocMaxBlocks;
   ScanScratch ls{};
-  ls.status = reinterpret_cast<unsigned long long*>(p);
+  ls.status = reinterpret_cast<unsigned long long*>(base + kStatusOffset);
   ls.status_len = kNoAllocMaxTiles;
-  p += kStatusBytes;
-  ls.ticket = reinterpret_cast<unsigned*>(p);
-  int* counts = reinterpret_cast<int*>(p + 16);
-  int* err = reinterpret_cast<int*>(p + 16 + 4 * kCntTotal);
-  // a fresh epoch per call: status words of earlier calls read as not ready
-  ls.epoch = g_epoch[dev].fetch_add(1u) + 1u;
-  if (cudaMemsetAsync(p, 0, kWordsBytes, st) != cudaSuccess)
+  ls.ticket = reinterpret_cast<unsigned*>(base + kWordsOffset);
+  int* counts = reinterpret_cast<int*>(base + kWordsOffset + 16);
+  int* err = reinterpret_cast<int*>(base + kErrOffset);
+  // status words, ticket / epoch / publish words, counts and the error word
+  // start at zero in every call (one contiguous region of a few KB)
+  if (cudaMemsetAsync(base + kStatusOffset, 0, kStatusBytes + kWordsBytes, st) != cudaSuccess)
     return set_error(SPMX_ERR_CUDA, "noalloc SpMSpV: scratch reset failed");
 
   const CscArgs a{m, n, d_csc_col, d_csc_row, d_csc_val, x_nnz, d_x_key, d_x_val,
                   (double)alpha, err, counts};
   if (launch_csc_scan(a, s, ls, kNoAllocBlockItems, st))
     return set_error(SPMX_ERR_INVALID_VALUE, "noalloc SpMSpV: scan capacity");
-  int sms = 0;
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  const int grid = std::max(1, sms) * std::max(1, csc_lb_blocks_per_sm());
   launch_csc_lb(a, s, 1, d_y, nullptr, nullptr, grid, st);
   const cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess)
     return set_error(SPMX_ERR_CUDA, std::string("noalloc SpMSpV launch: ") + cudaGetErrorString(e));
+  return SPMX_SUCCESS;
+}
+
+extern "C" int spmx_spmspv_csc_noalloc_check(void* stream) {
+  cudaStream_t st = (cudaStream_t)stream;
+  int e = 0;
+  if (cudaMemcpyFromSymbolAsync(&e, g_noalloc_scratch, sizeof(int), kErrOffset,
+                                cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+      cudaStreamSynchronize(st) != cudaSuccess) {
+    const cudaError_t ce = cudaGetLastError();
+    return set_error(SPMX_ERR_CUDA, std::string("noalloc SpMSpV check: ") + cudaGetErrorString(ce));
+  }
+  if (e & kDevErrTimeout) return set_error(SPMX_ERR_TIMEOUT, "noalloc SpMSpV: a bounded device wait timed out");
+  if (e & kDevErrOob) return set_error(SPMX_ERR_OOB, "noalloc SpMSpV: an index was out of range (bad input)");
+  if (e & kDevErrCapacity) return set_error(SPMX_ERR_OOB, "noalloc SpMSpV: an internal capacity was exceeded");
   return SPMX_SUCCESS;
 }

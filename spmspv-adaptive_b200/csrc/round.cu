@@ -266,6 +266,44 @@ __global__ void round_bounds_kernel(int nnz, const unsigned* __restrict__ skey, 
   out[t] = lo;
 }
 
+// out[t] = first sorted position with key >= (rb << cbits) | (seg << 16),
+// t = rb * nseg + seg in [0, nrb * nseg]: where each 2^16-column segment of
+// each row block starts (t = nrb * nseg gives the end of the last block)
+__global__ void round_seg_bounds_kernel(int nnz, const unsigned* __restrict__ skey, int nrb, int nseg,
+                                        int cbits, int* __restrict__ out) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t > (long long)nrb * nseg) return;
+  const unsigned rb = (unsigned)(t / nseg), seg = (unsigned)(t % nseg);
+  const unsigned want = (rb << cbits) | (seg << 16);
+  int lo = 0, hi = nnz;
+  while (lo < hi) {
+    const int mid = (int)(((long long)lo + hi) >> 1);
+    if (__ldg(skey + mid) < want) lo = mid + 1;
+    else hi = mid;
+  }
+  out[t] = lo;
+}
+
+// stream position of every sorted nonzero within its CTA's half when each
+// 2^16-column segment starts a new 128-entry chunk: half h (real entries
+// [half_lo[h], half_lo[h + 1])) places segment j at padded offset
+// pad_off[h * nseg + j]; its first real entry is seg_real[h * nseg + j]
+__global__ void round_ppos_kernel(int nvalid, const unsigned* __restrict__ skey, unsigned cmask, int nhalf,
+                                  const int* __restrict__ half_lo, int nseg, const int* __restrict__ seg_real,
+                                  const int* __restrict__ pad_off, int* __restrict__ ppos) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nvalid) return;
+  int lo = 0, hi = nhalf;  // the last half with half_lo <= i
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) >> 1;
+    if (__ldg(half_lo + mid) <= i) lo = mid;
+    else hi = mid;
+  }
+  const int j = (int)((__ldg(skey + i) & cmask) >> 16);
+  const long long hj = (long long)lo * nseg + j;
+  ppos[i] = __ldg(pad_off + hj) + (i - __ldg(seg_real + hj));
+}
+
 // one CTA per round: the second sort's keys (round << 16 | local row, stable
 // over the round's column order) and the column-order positions
 __global__ void round_key2_kernel(const int* __restrict__ rstart, const int* __restrict__ rlen,
@@ -311,37 +349,47 @@ __device__ __forceinline__ int round_vperm(int p) {
 }
 
 // one CTA per round: stream words (slot << 16 | column offset from the
-// chunk's first column), values and chunk bases; a chunk spanning 2^16
-// columns or more sets flags bit 1
+// chunk's first column), values and chunk bases.  Every position starts as
+// padding (a lane's own dummy slot, the chunk's base column, value 0); real
+// entry t of the round then goes to position t, or, with ppos, to its padded
+// position ppos[i] - rpad0[q] (chunks then never cross a 2^16-column segment).
+// A chunk's real entries are contiguous from its first position, which holds
+// its base column.  An offset of 2^16 columns or more sets flags bit 1.
 __global__ void __launch_bounds__(256)
-round_layout_kernel(const int* __restrict__ rstart, const int* __restrict__ rlen, const int* __restrict__ rrb,
-                    const int* __restrict__ rb_row, const int* __restrict__ vbg, const unsigned* __restrict__ skey,
-                    const unsigned* __restrict__ slrow, const unsigned* __restrict__ sval, unsigned cmask,
-                    const int* __restrict__ occ, int dummy, unsigned* __restrict__ packed, float* __restrict__ val,
-                    int* __restrict__ cbase, int* __restrict__ flags) {
+round_layout_kernel(const int* __restrict__ rstart, const int* __restrict__ rlen, const int* __restrict__ rpad0,
+                    const int* __restrict__ rrb, const int* __restrict__ rb_row, const int* __restrict__ vbg,
+                    const unsigned* __restrict__ skey, const unsigned* __restrict__ slrow,
+                    const unsigned* __restrict__ sval, unsigned cmask, const int* __restrict__ occ,
+                    const int* __restrict__ ppos, int dummy, unsigned* __restrict__ packed,
+                    float* __restrict__ val, int* __restrict__ cbase, int* __restrict__ flags) {
   constexpr int E = kRoundE;
   const int q = blockIdx.x;
   const int s = __ldg(rstart + q), len = __ldg(rlen + q);
+  const int p0 = ppos ? __ldg(rpad0 + q) : 0;
   const int row0 = __ldg(rb_row + __ldg(rrb + q));
   const int vb0 = __ldg(vbg + row0);
   const size_t o = (size_t)q * E;
   for (int p = threadIdx.x; p < E; p += blockDim.x) {
-    const int first = p & ~(kRoundChunk - 1);  // the chunk's first position
-    const unsigned cb = first < len ? (__ldg(skey + s + first) & cmask) : 0u;
-    const int sp = round_vperm(p);
-    if (p == first) cbase[o / kRoundChunk + p / kRoundChunk] = (int)cb;
-    if (p < len) {
-      const int i = s + p;
-      const unsigned c = __ldg(skey + i) & cmask;
-      const int slot = __ldg(vbg + row0 + (int)__ldg(slrow + i)) - vb0 + __ldg(occ + i);
-      if (c - cb >= 65536u) atomicOr(flags, 2);
-      packed[o + sp] = ((unsigned)slot << 16) | ((c - cb) & 0xffffu);
-      val[o + sp] = __uint_as_float(__ldg(sval + i));
-    } else {
-      // padding: a lane's own dummy slot, the chunk's base column, value 0
-      packed[o + sp] = (unsigned)(dummy + (p & 31)) << 16;
-      val[o + sp] = 0.f;
+    packed[o + round_vperm(p)] = (unsigned)(dummy + (p & 31)) << 16;
+    val[o + round_vperm(p)] = 0.f;
+    if ((p & (kRoundChunk - 1)) == 0) cbase[o / kRoundChunk + p / kRoundChunk] = 0;
+  }
+  __syncthreads();
+  for (int t = threadIdx.x; t < len; t += blockDim.x) {
+    const int i = s + t;
+    const int pp = ppos ? __ldg(ppos + i) - p0 : t;
+    if ((unsigned)pp >= (unsigned)E) {
+      atomicOr(flags, 4);
+      continue;
     }
+    const int first = pp & ~(kRoundChunk - 1);
+    const unsigned cb = __ldg(skey + i - (pp - first)) & cmask;
+    const unsigned c = __ldg(skey + i) & cmask;
+    const int slot = __ldg(vbg + row0 + (int)__ldg(slrow + i)) - vb0 + __ldg(occ + i);
+    if (c - cb >= 65536u) atomicOr(flags, 2);
+    packed[o + round_vperm(pp)] = ((unsigned)slot << 16) | ((c - cb) & 0xffffu);
+    val[o + round_vperm(pp)] = __uint_as_float(__ldg(sval + i));
+    if (pp == first) cbase[o / kRoundChunk + pp / kRoundChunk] = (int)cb;
   }
 }
 
@@ -393,8 +441,12 @@ extern "C" int spmx_round_postprocess(spmx_handle_t h) {
 }
 
 // builds the round format with row blocks of at most rcap rows; *overflow is
-// set when a row block needs more accumulator slots than shared memory holds
-static int round_build(spmx_handle_t h, long long rcap, long long avail, bool* overflow) {
+// set when a row block needs more accumulator slots than shared memory holds,
+// *span when 128 consecutive nonzeros of a row block span 2^16 columns or more
+// (then a build with pad = true starts a new chunk at every 2^16-column
+// segment, which bounds every chunk's span)
+static int round_build(spmx_handle_t h, long long rcap, long long avail, bool pad, bool* overflow,
+                       bool* span) {
   constexpr int E = kRoundE;
   spmx_round_postprocess(h);
   const int m = h->m, n = h->n, nnz = h->nnz;
@@ -482,11 +534,31 @@ static int round_build(spmx_handle_t h, long long rcap, long long avail, bool* o
         rc = set_error(SPMX_ERR_CUDA, "round SpMV: block bounds");
     }
   }
+  // with pad: where each 2^16-column segment of each row block starts
+  const int nseg = pad ? (int)(((long long)std::max(n, 1) + 65535) / 65536) : 1;
+  std::vector<int> segb;
+  int* d_segb = nullptr;
+  if (!rc && pad && nnz > 0) {
+    const long long nt = (long long)nrb * nseg + 1;
+    segb.assign((size_t)nt, 0);
+    rc = dalloc((void**)&d_segb, 4 * (size_t)nt, "round segment bounds");
+    if (!rc) {
+      note_launch();
+      round_seg_bounds_kernel<<<(unsigned)((nt + 255) / 256), 256, 0, st>>>(nnz, skey, nrb, nseg, cbits, d_segb);
+      if (cudaMemcpyAsync(segb.data(), d_segb, 4 * (size_t)nt, cudaMemcpyDeviceToHost, st) != cudaSuccess)
+        rc = set_error(SPMX_ERR_CUDA, "round SpMV: segment bounds");
+    }
+  }
   cudaError_t se = cudaStreamSynchronize(st);
   if (!rc && se != cudaSuccess) rc = set_error(SPMX_ERR_CUDA, std::string("round SpMV: ") + cudaGetErrorString(se));
   // rounds (host): each row block's sorted nonzeros split in two halves of
   // whole rounds, one per CTA of the cluster, each cut into rounds of E
-  std::vector<int> rstart, rlen, rrb, cta((size_t)t->grid + 1, 0);
+  // stream positions.  With pad, a half's stream places every segment at a
+  // multiple of the chunk length (a segment's last chunk is padded), and the
+  // rounds are cut on that padded stream; a round then holds the real entries
+  // whose padded positions fall in it, a contiguous run of the sorted order.
+  std::vector<int> rstart, rlen, rpad0, rrb, cta((size_t)t->grid + 1, 0);
+  std::vector<int> half_lo, seg_real, pad_off;  // per half (pad only)
   if (!rc) {
     for (int k = 0; k < nrb; ++k) {
       const int s = bounds[k], e = bounds[k + 1];
@@ -496,19 +568,53 @@ static int round_build(spmx_handle_t h, long long rcap, long long avail, bool* o
       const int part[3] = {s, mid, e};
       for (int c = 0; c < kRoundCS; ++c) {
         cta[(size_t)k * kRoundCS + c] = (int)rstart.size();
-        for (int p = part[c]; p < part[c + 1]; p += E) {
-          rstart.push_back(p);
-          rlen.push_back(std::min(E, part[c + 1] - p));
+        const int lo = part[c], hi = part[c + 1];
+        if (!pad) {
+          for (int p = lo; p < hi; p += E) {
+            rstart.push_back(p);
+            rlen.push_back(std::min(E, hi - p));
+            rpad0.push_back(0);
+            rrb.push_back(k);
+          }
+          continue;
+        }
+        half_lo.push_back(lo);
+        std::vector<long long> off((size_t)nseg + 1, 0);
+        std::vector<int> st0((size_t)nseg, lo), cnts((size_t)nseg, 0);
+        for (int j = 0; j < nseg; ++j) {
+          const int a = std::max(lo, segb[(size_t)k * nseg + j]);
+          const int b = std::min(hi, segb[(size_t)k * nseg + j + 1]);
+          st0[j] = a;
+          cnts[j] = std::max(0, b - a);
+          off[j + 1] = off[j] + ((cnts[j] + kRoundChunk - 1) / kRoundChunk) * kRoundChunk;
+          seg_real.push_back(a);
+          pad_off.push_back((int)off[j]);
+        }
+        const long long L = off[nseg];
+        // the real index at padded position P (a chunk start, or L)
+        auto real_at = [&](long long P) -> int {
+          if (P >= L) return hi;
+          const int j = (int)(std::upper_bound(off.begin(), off.end(), P) - off.begin()) - 1;
+          return st0[j] + (int)std::min<long long>(P - off[j], cnts[j]);
+        };
+        for (long long P = 0; P < L; P += E) {
+          const int a = real_at(P), b = real_at(std::min(L, P + E));
+          rstart.push_back(a);
+          rlen.push_back(b - a);
+          rpad0.push_back((int)P);
           rrb.push_back(k);
         }
       }
     }
     cta[(size_t)t->grid] = (int)rstart.size();
     if (rstart.size() >= 65536) rc = set_error(SPMX_ERR_INVALID_VALUE, "round SpMV: too many rounds");
+    if (pad && (long long)half_lo.size() * nseg > (1LL << 26))
+      rc = set_error(SPMX_ERR_INVALID_VALUE, "round SpMV: too many column segments");
   }
   const int nrounds = (int)rstart.size();
   t->nrounds = nrounds;
   int *d_rstart = nullptr, *d_rlen = nullptr, *d_rrb = nullptr, *occ = nullptr, *d_bslots = nullptr;
+  int *d_rpad0 = nullptr, *d_half_lo = nullptr, *d_seg_real = nullptr, *d_pad_off = nullptr, *ppos = nullptr;
   const size_t qn = (size_t)std::max(nrounds, 1);
   rc = rc ? rc : dalloc((void**)&t->cta_round, 4 * cta.size(), "round CTA runs");
   rc = rc ? rc : dalloc((void**)&t->packed, 4 * qn * E, "round stream words");
@@ -519,6 +625,14 @@ static int round_build(spmx_handle_t h, long long rcap, long long avail, bool* o
   rc = rc ? rc : dalloc((void**)&d_rrb, 4 * qn, "round blocks");
   rc = rc ? rc : dalloc((void**)&occ, b4, "round occurrences");
   rc = rc ? rc : dalloc((void**)&d_bslots, 4 * ((size_t)nrb + 1), "round block slots");
+  if (pad) {
+    const size_t hs = std::max<size_t>(half_lo.size(), 1), ss = std::max<size_t>(seg_real.size(), 1);
+    rc = rc ? rc : dalloc((void**)&d_rpad0, 4 * qn, "round padded starts");
+    rc = rc ? rc : dalloc((void**)&d_half_lo, 4 * hs, "round half starts");
+    rc = rc ? rc : dalloc((void**)&d_seg_real, 4 * ss, "round segment starts");
+    rc = rc ? rc : dalloc((void**)&d_pad_off, 4 * ss, "round segment offsets");
+    rc = rc ? rc : dalloc((void**)&ppos, b4, "round padded positions");
+  }
   const unsigned cmask = (unsigned)((1ULL << cbits) - 1);
   int nslots_real = 0;
   if (!rc) {
@@ -528,6 +642,15 @@ static int round_build(spmx_handle_t h, long long rcap, long long avail, bool* o
       cudaMemcpyAsync(d_rlen, rlen.data(), 4 * (size_t)nrounds, cudaMemcpyHostToDevice, st);
       cudaMemcpyAsync(d_rrb, rrb.data(), 4 * (size_t)nrounds, cudaMemcpyHostToDevice, st);
       const int nvalid = bounds[nrb];
+      if (pad && nvalid > 0) {
+        cudaMemcpyAsync(d_rpad0, rpad0.data(), 4 * (size_t)nrounds, cudaMemcpyHostToDevice, st);
+        cudaMemcpyAsync(d_half_lo, half_lo.data(), 4 * half_lo.size(), cudaMemcpyHostToDevice, st);
+        cudaMemcpyAsync(d_seg_real, seg_real.data(), 4 * seg_real.size(), cudaMemcpyHostToDevice, st);
+        cudaMemcpyAsync(d_pad_off, pad_off.data(), 4 * pad_off.size(), cudaMemcpyHostToDevice, st);
+        note_launch();
+        round_ppos_kernel<<<(nvalid + 255) / 256, 256, 0, st>>>(nvalid, skey, cmask, (int)half_lo.size(), d_half_lo,
+                                                                nseg, d_seg_real, d_pad_off, ppos);
+      }
       unsigned* pos_in = a1 == slrow ? a0 : a1;
       unsigned* pos_alt = k1 == skey ? k0 : k1;
       note_launch();
@@ -567,8 +690,9 @@ static int round_build(spmx_handle_t h, long long rcap, long long avail, bool* o
     }
     if (!rc && nrounds > 0) {
       note_launch();
-      round_layout_kernel<<<nrounds, 256, 0, st>>>(d_rstart, d_rlen, d_rrb, t->rb_row, t->vbg, skey, slrow, sval,
-                                                  cmask, occ, nslots_real, t->packed, t->val, t->cbase, flags);
+      round_layout_kernel<<<nrounds, 256, 0, st>>>(d_rstart, d_rlen, d_rpad0, d_rrb, t->rb_row, t->vbg, skey,
+                                                  slrow, sval, cmask, occ, pad ? ppos : nullptr, nslots_real,
+                                                  t->packed, t->val, t->cbase, flags);
     }
     int hflags[4] = {0, 0, 0, 0};
     if (cudaMemcpyAsync(hflags, flags, sizeof(hflags), cudaMemcpyDeviceToHost, st) != cudaSuccess)
@@ -576,13 +700,17 @@ static int round_build(spmx_handle_t h, long long rcap, long long avail, bool* o
     se = cudaStreamSynchronize(st);
     if (!rc && se != cudaSuccess) rc = set_error(SPMX_ERR_CUDA, std::string("round SpMV: ") + cudaGetErrorString(se));
     if (!rc && (hflags[0] & 1)) rc = set_error(SPMX_ERR_INVALID_VALUE, "round SpMV: column index out of range");
-    if (!rc && (hflags[0] & 2))
+    if (!rc && (hflags[0] & 4)) rc = set_error(SPMX_ERR_INVALID_VALUE, "round SpMV: internal layout error");
+    if (!rc && (hflags[0] & 2)) {
+      *span = true;
       rc = set_error(SPMX_ERR_INVALID_VALUE,
-                     "round SpMV: 128 consecutive nonzeros of a row block span 2^16 columns (matrix too sparse)");
+                     "round SpMV: 128 consecutive nonzeros of a row block span 2^16 columns");
+    }
   }
   dfree(k0); dfree(k1); dfree(a0); dfree(a1); dfree(v0); dfree(v1); dfree(q0); dfree(q1);
   dfree(hist); dfree(hoff); dfree(flags); dfree(d_bounds); dfree(spr);
   dfree(d_rstart); dfree(d_rlen); dfree(d_rrb); dfree(occ); dfree(d_bslots);
+  dfree(d_segb); dfree(d_rpad0); dfree(d_half_lo); dfree(d_seg_real); dfree(d_pad_off); dfree(ppos);
   if (rc) {
     spmx_round_postprocess(h);
     return rc;
@@ -612,10 +740,19 @@ extern "C" int spmx_round_preprocess(spmx_handle_t h, int rb_rows) {
   // rows with many nonzeros in one round (hub rows, or rows whose nonzeros
   // sit in neighbouring columns) need several slots each; when a row block
   // needs more than fit, retry with row blocks half as tall (up to 5 times)
+  // A matrix whose 128 consecutive nonzeros (in a row block's column order)
+  // can span 2^16 columns or more is rebuilt with every 2^16-column segment
+  // starting a new chunk.
+  bool pad = false;
   for (int attempt = 0;; ++attempt) {
-    bool overflow = false;
-    const int rc = round_build(h, rcap, avail, &overflow);
-    if (rc == SPMX_SUCCESS || !overflow || attempt == 5 || rcap <= 64) return rc;
+    bool overflow = false, span = false;
+    const int rc = round_build(h, rcap, avail, pad, &overflow, &span);
+    if (rc == SPMX_SUCCESS) return rc;
+    if (span && !pad) {
+      pad = true;
+      continue;
+    }
+    if (!overflow || attempt >= 6 || rcap <= 64) return rc;
     rcap = std::max<long long>(64, (rcap / 2) & ~3LL);
   }
 }

@@ -123,7 +123,7 @@ scan_exclusive_kernel(const int* __restrict__ in, int* __restrict__ out, int n,
   unsigned total;
   const unsigned ex = block_exclusive_sum<NT>(sum, s_wtmp, &total);
   if (tid < 32) {
-    const unsigned p = lb_warp_lookback(st, tile, total, err);
+    const unsigned p = lb_warp_lookback(st, tile, ntiles, total, err);
     if (tid == 0) s_prefix = p;
   }
   __syncthreads();
@@ -145,7 +145,7 @@ int launch_scan_exclusive(const int* in, int* out, int n, int* total_out,
   if (n <= 0) return 0;
   const int ntiles = (n + NT * VT - 1) / (NT * VT);
   if (ntiles > ls.status_len) return -1;
-  LookbackState lbs{ls.status, ls.ticket, ++ls.epoch};
+  LookbackState lbs{ls.status, ls.ticket};
   note_launch();
   scan_exclusive_kernel<NT, VT><<<ntiles, NT, 0, st>>>(in, out, n, lbs, ntiles,
                                                       total_out, err);
@@ -231,7 +231,7 @@ rbk_heads_kernel(const unsigned* __restrict__ keys, int n, int* __restrict__ slo
   const unsigned ex = block_exclusive_sum<NT>(c, s_wtmp, &total);
   if (tid < VT * NW) s_cnt[tid] = ex;
   if (tid < 32) {
-    const unsigned p = lb_warp_lookback(st, tile, total, err);
+    const unsigned p = lb_warp_lookback(st, tile, ntiles, total, err);
     if (tid == 0) { s_prefix = p; s_total = total; }
   }
   __syncthreads();
@@ -278,7 +278,7 @@ int reduce_by_key_sorted(const unsigned* keys, const float* vals, int n,
   if (n <= 0) { cudaMemsetAsync(d_count, 0, sizeof(int), st); return 0; }
   const int ntiles = (n + NT * VT - 1) / (NT * VT);
   if (ntiles > ls.status_len) return -1;
-  LookbackState lbs{ls.status, ls.ticket, ++ls.epoch};
+  LookbackState lbs{ls.status, ls.ticket};
   note_launch(2);
   rbk_heads_kernel<NT, VT><<<ntiles, NT, 0, st>>>(keys, n, slot_scratch, out_key, out_val,
                                                  d_count, lbs, ntiles, err);

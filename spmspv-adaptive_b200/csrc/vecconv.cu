@@ -88,7 +88,7 @@ compact_nonzero_kernel(int len, const float* __restrict__ dense,
   const unsigned ex = block_exclusive_sum<NT>(c, s_wtmp, &total);
   if (tid < VT * NW) s_cnt[tid] = ex;
   if (tid < 32) {
-    const unsigned p = lb_warp_lookback(st, tile, total, err);
+    const unsigned p = lb_warp_lookback(st, tile, ntiles, total, err);
     if (tid == 0) { s_prefix = p; s_total = total; }
   }
   __syncthreads();
@@ -148,7 +148,7 @@ int launch_compact_nonzero(int len, const float* dense, int* key, float* val,
   if (len <= 0) { cudaMemsetAsync(d_count, 0, sizeof(int), st); return 0; }
   const int ntiles = (len + NT * VT - 1) / (NT * VT);
   if (ntiles > ls.status_len) return -1;
-  LookbackState lbs{ls.status, ls.ticket, ++ls.epoch};
+  LookbackState lbs{ls.status, ls.ticket};
   note_launch();
   compact_nonzero_kernel<NT, VT><<<ntiles, NT, 0, st>>>(len, dense, key, val, d_count,
                                                        lbs, ntiles, err);

@@ -83,6 +83,7 @@ _SIGS = {
     "spmx_bitarray2sparse": (c_int, [P, PI]),
     "spmx_dense2bitarray": (c_int, [P]),
     "spmx_dense2sparse_outer": (c_int, [P, c_int, P, PI, P, P]),
+    "spmx_dense2sparse_to_host": (c_int, [P, c_int, P, P, P, P]),
     "spmx_sparse2dense_outer": (c_int, [P, c_int, P, P, c_int, P]),
     "spmx_alloc_pre_buffer": (c_int, [P]),
     "spmx_dealloc_pre_buffer": (c_int, [P]),
@@ -125,6 +126,7 @@ _SIGS = {
     "spmx_csc_twolayer_sort": (c_int, [P, c_int, c_float, PI, P, P, P]),
     "spmx_csc_bucket": (c_int, [P, c_float, PI, P, P, P, c_int]),
     "spmx_spmspv_csc_noalloc": (c_int, [c_int, c_int, c_int, P, P, P, c_int, P, P, c_float, P, P]),
+    "spmx_spmspv_csc_noalloc_check": (c_int, [P]),
     "spmx_compute_binlen": (c_int, [P, PLL]),
     "spmx_compute_gm": (c_int, [P, PD]),
     "spmx_mat_features": (c_int, [P, PD]),

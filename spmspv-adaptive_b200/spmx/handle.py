@@ -203,6 +203,19 @@ class SpmspvHandle:
                                           _i32(d_key), _f32(d_val)), "dense2sparse_outer")
         return n.value
 
+    def dense2sparse_to_host(self, m, d_dense, h_key, h_val, h_count):
+        """Nonzeros of d_dense[:m] into pinned host tensors h_key / h_val and
+        their count into h_count[0] (pinned int32), without synchronising:
+        read them after the stream has passed this call."""
+        for t, dt in ((h_key, torch.int32), (h_val, torch.float32), (h_count, torch.int32)):
+            if t.is_cuda or not t.is_pinned():
+                raise ValueError("h_key, h_val and h_count must be pinned host tensors")
+            if t.dtype != dt:
+                raise TypeError("h_key / h_count must be int32 and h_val float32")
+        check(lib.spmx_dense2sparse_to_host(self._h, int(m), _f32(d_dense), h_key.data_ptr(),
+                                            h_val.data_ptr(), h_count.data_ptr()),
+              "dense2sparse_to_host")
+
     def sparse2dense_outer(self, ynnz, d_key, d_val, m, d_dense):
         check(lib.spmx_sparse2dense_outer(self._h, int(ynnz), _i32(d_key), _f32(d_val), int(m),
                                           _f32(d_dense)), "sparse2dense_outer")

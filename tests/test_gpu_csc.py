@@ -188,6 +188,21 @@ def test_vector_conversions(torch_cuda):
     back = torch.empty(70000, device="cuda")
     h.sparse2dense_outer(cnt, dk, dv, 70000, back)
     assert np.array_equal(back.cpu().numpy(), d)
+    # the same compaction written straight into pinned host memory, twice in a
+    # row on the handle's stream (no synchronisation inside the call)
+    hk = torch.full((70000,), -1, dtype=torch.int32).pin_memory()
+    hv = torch.zeros(70000).pin_memory()
+    hc = torch.full((1,), -1, dtype=torch.int32).pin_memory()
+    for dd in (d, np.where(np.arange(70000) % 3 == 0, d, 0).astype(np.float32)):
+        dd_d = dev(dd, torch)
+        h.dense2sparse_to_host(70000, dd_d, hk, hv, hc)
+        torch.cuda.synchronize()
+        ek, ev = orc.dense2sparse(dd)
+        c = int(hc[0])
+        assert c == len(ek)
+        assert np.array_equal(hk[:c].numpy(), ek) and np.array_equal(hv[:c].numpy(), ev)
+    with pytest.raises(ValueError):
+        h.dense2sparse_to_host(70000, dd_d, dk.cpu(), hv, hc)  # not pinned
 
 
 def test_features(torch_cuda):

@@ -166,3 +166,38 @@ def test_graph_round_spmv_chain(torch_cuda):
         assert orc.within_tol(y0.cpu().numpy(), y64, mag, RTOL)[0]
         assert orc.within_tol(y1.cpu().numpy(), z64, zmag, RTOL)[0]
     del g
+
+
+def test_graph_replay_after_keys_change(torch_cuda):
+    """A captured load-balanced CSC SpMSpV (look-back scan + merge-path pass)
+    replayed after x's keys and values change in place: every replay scans
+    with a fresh look-back epoch (kept in device memory), so no tile can take
+    a prefix left by the previous replay.  x spans many scan tiles."""
+    torch = torch_cuda
+    A = rand_csr(30000, 40000, density=0.0008, seed=23)
+    h = make_handle(A, torch, hola=False)
+    rng = np.random.default_rng(5)
+    k = 20000
+    keys = [np.sort(rng.choice(A.n, k, replace=False)).astype(np.int32) for _ in range(3)]
+    vals = [rng.uniform(-1, 1, k).astype(np.float32) for _ in range(3)]
+    kd, vd = dev(keys[0], torch), dev(vals[0], torch)
+    y = torch.empty(A.m, device="cuda")
+
+    def work():
+        h.set_sparse_x(kd, vd, k)
+        h.spmspv_csc(1, 0, 1.0, y, sync=False)  # merge-path, atomic
+
+    g, s = _capture(torch, h, work)
+    colptr, row, cval = A.to_csc()
+    for rep in range(6):
+        i = rep % 3
+        with torch.cuda.stream(s):
+            kd.copy_(torch.from_numpy(keys[i]))
+            vd.copy_(torch.from_numpy(vals[i]))
+            y.fill_(9.0)
+        g.replay()
+        s.synchronize()
+        h.check_device_error()
+        y64, mag, _ = orc.spmspv_csc_f64(A.m, colptr, row, cval, keys[i], vals[i])
+        assert orc.within_tol(y.cpu().numpy(), y64, mag, RTOL)[0], f"replay {rep}"
+    del g

@@ -7,9 +7,10 @@ whole rounds, all rows empty), hub rows with thousands of accumulators, row
 blocks capped small enough that
 the grid runs in several waves, a tall thin matrix, the 1M-row Zipf matrix;
 alpha values; the gated form through the dispatcher; determinism (bitwise
-equal results of repeated calls); and the preprocessing's refusals (a column
-out of range, 128-nonzero chunks spanning too many columns), after which the handle still
-serves the other back-ends."""
+equal results of repeated calls); matrices whose 128 consecutive nonzeros of a
+row block span 2^16 columns or more (the build pads every 2^16-column segment
+to a chunk boundary); and the preprocessing's refusal of a column out of
+range, after which the handle still serves the other back-ends."""
 import numpy as np
 import pytest
 
@@ -39,6 +40,12 @@ def _extra():
     g.val = np.random.default_rng(48).uniform(-1, 1, g.nnz).astype(np.float32)
     yield "rmat-15", g
     yield "laplacian-512", gen.laplacian(512)
+    # chunks spanning 2^16 columns or more: 24,000 nonzeros over 16M columns,
+    # and an R-MAT graph with 131,072 columns (two segments)
+    yield "span-16M", rand_csr(4, 1 << 24, lens=[6000, 6000, 6000, 6000], seed=45)
+    g = gen.rmat(17, 16, seed=49)
+    g.val = np.random.default_rng(50).uniform(-1, 1, g.nnz).astype(np.float32)
+    yield "rmat-17", g
 
 
 EXTRA = list(_extra())
@@ -127,17 +134,14 @@ def test_round_refusals_keep_handle_usable(torch_cuda):
         h.roundPreprocess()
     with pytest.raises(SpmxError):
         h.round_info()  # nothing kept
-    # 128 consecutive nonzeros spanning 2^16 columns: 24,000 nonzeros over 16M columns
-    B = rand_csr(4, 1 << 24, lens=[6000, 6000, 6000, 6000], seed=45)
-    hb = make_handle(B, torch, csc=False, hola=False)
-    with pytest.raises(SpmxError):
-        hb.roundPreprocess()
     # the other back-ends still serve the handle
-    x = np.random.default_rng(3).uniform(-1, 1, B.n).astype(np.float32)
-    hb.set_x(dev(x, torch))
-    hb.holaPreprocess()
-    y = torch.empty(B.m, device="cuda")
-    hb.holaspmv(1.0, y)
-    hb.check_device_error()
-    y64, mag = orc.spmv_f64(B.rowptr, B.col, B.val, x)
+    x = np.random.default_rng(3).uniform(-1, 1, A.n).astype(np.float32)
+    h.set_x(dev(x, torch))
+    h.holaPreprocess()
+    y = torch.empty(A.m, device="cuda")
+    h.holaspmv(1.0, y)
+    with pytest.raises(SpmxError):
+        h.check_device_error()  # Hola skips the bad column and reports it
+    ok = bad < A.n
+    y64, mag = orc.spmv_f64(A.rowptr, np.where(ok, bad, 0), np.where(ok, A.val, 0), x)
     assert orc.within_tol(y.cpu().numpy(), y64, mag, RTOL)[0]
