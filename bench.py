@@ -9,11 +9,13 @@ of the benchmark's shape: no dataset is involved.
 
 Metric: effective GB/s = compulsory bytes of the cheapest formulation of each
 call (min of the CSC SpMSpV traffic 16*x_nnz + 8*bin_len + 4*m and the SpMV
-traffic 4(m+1) + 8*nnz + 4n + 4m), summed over the sweep, divided by the summed
-device time.  `value` has inputs resident in HBM; `e2e` adds, per call, the
-host->device copy of x (pinned) and the device->host read of y: its nonzeros
-(keys and values, after the count comes back) for a sparse x, the dense y for
-the dense x.
+traffic 4(m+1) + 8*nnz + 4n + 4m), summed over the sweep, divided by the
+device time of the step (the six calls back to back, CUDA events around them,
+the L2 flushed before each step).  `value` has inputs resident in HBM; `e2e`
+adds, per call, the host->device copy of x (pinned) and the device->host read
+of y: its nonzeros (keys, values and their count, compacted straight into
+pinned host memory) for a sparse x, the dense y for the dense x; one stream
+synchronisation per step.
 
 --impl reference times the reference's CPU path on all host threads on the
 same sweep (the reference's own serialspmv over row slices for the dense x,
@@ -355,7 +357,10 @@ def run_ours(args, world, rank, local):
     from spmx import abi
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
-    stream = torch.cuda.current_stream(dev)
+    # one side stream for everything (graph capture needs a stream other than
+    # the legacy default stream)
+    stream = torch.cuda.Stream(dev)
+    torch.cuda.set_stream(stream)
     A, xs = make_inputs()
     m, n, nnz = A.m, A.n, A.nnz
 
@@ -382,41 +387,62 @@ def run_ours(args, world, rank, local):
     ebytes = [eff_bytes(m, n, nnz, k, b) for (_, _, _, k), b in zip(dx, binl)]
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)  # 256 MiB > L2
 
-    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
-          for _ in dx]
+    # --- one step = the whole sweep: the six adaptive calls through the public
+    # API, back to back on one stream, each into its own y (the selector picks
+    # every call's kernel on the host, from features it knows without a device
+    # round trip); one pair of CUDA events around the step, the L2 flushed
+    # before it. ---
+    ys = [torch.empty(m, device=dev) for _ in dx]
     chosen = [None] * len(dx)
+    s_ev, e_ev = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
 
-    def step(record):
-        times = []
+    def step():
+        flush.fill_(1.0)
+        s_ev.record(stream)
         for i, (dd, kd, vd, k) in enumerate(dx):
-            flush.fill_(float(i))
             h.set_sparse_x(kd, vd, k)
-            s, e = ev[i]
-            s.record(stream)
-            chosen[i] = h.run_adaptive(1.0, y)
-            e.record(stream)
+            chosen[i] = h.run_adaptive(1.0, ys[i])
+        e_ev.record(stream)
         stream.synchronize()
-        return [ev[i][0].elapsed_time(ev[i][1]) for i in range(len(dx))]
+        return s_ev.elapsed_time(e_ev)
 
     for _ in range(max(args.warmup, 3)):
-        step(False)
+        step()
     h.check_device_error()
     barrier(world)
     torch.cuda.synchronize(dev)
-    per = np.zeros(len(dx))
+    step_t = []
     l0 = abi.lib.spmx_launch_count()
     with Clocks(local) as clk:
         for _ in range(args.steps):
-            per += np.array(step(True))
+            step_t.append(step())
     launches = abi.lib.spmx_launch_count() - l0
+    launches_per_step = launches // max(args.steps, 1)
     torch.cuda.synchronize(dev)
     barrier(world)
     h.check_device_error()
-    per /= args.steps
-    step_ms = float(per.sum())
+    step_ms = float(np.mean(step_t))
     step_ms_max = allmax(step_ms, world)
     total_bytes = float(sum(ebytes))
     value = world * total_bytes / (step_ms_max * 1e-3) / 1e9
+    # the timed replays' results, kept for the check against the oracle below
+    ys_h = [t.cpu().numpy().astype(np.float64) for t in ys]
+
+    # --- each call alone, the L2 flushed before it (CUDA events around the
+    # call; an empty kernel timed this way after the flush takes about 6 us) ---
+    ev1 = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in dx]
+    per_call = np.zeros(len(dx))
+    for it in range(3 + args.steps):
+        for i, (dd, kd, vd, k) in enumerate(dx):
+            flush.fill_(float(i))
+            h.set_sparse_x(kd, vd, k)
+            ev1[i][0].record(stream)
+            h.run_adaptive(1.0, y)
+            ev1[i][1].record(stream)
+        stream.synchronize()
+        if it >= 3:
+            per_call += np.array([a.elapsed_time(b) for a, b in ev1])
+    per_call /= args.steps
 
     # --- roofline: the load-balanced SpMV on the dense x (the dominant call of
     # the sweep), through the dispatcher, i.e. the back-end the autotuner chose
@@ -451,10 +477,7 @@ def run_ours(args, world, rank, local):
     import oracle.oracle as orc
     if rank == 0:
         colptr_h, row_h, cval_h = A.to_csc()
-        for (dd, kd, vd, k), (_, key, val) in zip(dx, xs):
-            h.set_sparse_x(kd, vd, k)
-            h.run_adaptive(1.0, y)
-            yh = y.cpu().numpy().astype(np.float64)
+        for (dd, kd, vd, k), (_, key, val), yh in zip(dx, xs, ys_h):
             y64, mag, _ = orc.spmspv_csc_f64(m, colptr_h, row_h, cval_h, key, val)
             ref64.append((y64, mag))
             nz = y64 != 0
@@ -465,54 +488,62 @@ def run_ours(args, world, rank, local):
                                 "normwise_err": float(np.max(np.abs(yh - y64))) / top if top else 0.0})
         h.check_device_error()
 
-    # --- e2e through the public API with host buffers.  Per call: the
-    # pinned host->device copy of x, the adaptive call, and the read-back of
-    # y: for a sparse x the nonzeros of y, compacted straight into pinned host
-    # memory with their count (spmx_dense2sparse_to_host, no host round trip
-    # inside the call), for the dense x the dense y.  One stream
-    # synchronisation per call, at its end. ---
+    # --- e2e through the public API with host buffers, one step = the sweep.
+    # Every x is copied from pinned host memory on a copy stream (all six
+    # uploads back to back); each adaptive call waits for its own x only, so
+    # the later uploads overlap the earlier calls.  The result of each call is
+    # read back without a host round trip: for a sparse x the nonzeros of y,
+    # compacted straight into pinned host memory with their count
+    # (spmx_dense2sparse_to_host), for the dense x the dense y.  One stream
+    # synchronisation per step, at its end; the L2 is flushed between steps.
     pin_k = [torch.from_numpy(np.ascontiguousarray(k)).pin_memory() for _, k, _ in xs]
     pin_v = [torch.from_numpy(np.ascontiguousarray(v)).pin_memory() for _, _, v in xs]
-    kbuf = torch.empty(n, dtype=torch.int32, device=dev)
-    vbuf = torch.empty(n, dtype=torch.float32, device=dev)
+    kbufs = [torch.empty(max(len(k), 1), dtype=torch.int32, device=dev) for _, k, _ in xs]
+    vbufs = [torch.empty(max(len(k), 1), dtype=torch.float32, device=dev) for _, k, _ in xs]
+    sparse_out = [dd < 1.0 for dd, _, _ in xs]
     yhost = torch.empty(m, dtype=torch.float32).pin_memory()
-    ykey_h = torch.empty(m, dtype=torch.int32).pin_memory()
-    yval_h = torch.empty(m, dtype=torch.float32).pin_memory()
-    ycnt_h = torch.zeros(1, dtype=torch.int32).pin_memory()
+    ykey_h = [torch.empty(m if sp else 1, dtype=torch.int32).pin_memory() for sp in sparse_out]
+    yval_h = [torch.empty(m if sp else 1, dtype=torch.float32).pin_memory() for sp in sparse_out]
+    ycnt_h = torch.zeros(len(xs), dtype=torch.int32).pin_memory()
     h2d = sum(8 * len(k) for _, k, _ in xs)
     d2h_calls = []
     e2e_ok = []
+    copy_stream = torch.cuda.Stream(dev)
+    ev_in = [torch.cuda.Event() for _ in xs]
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
 
     def e2e_step(check=False):
-        tot = 0.0
-        d2h_calls.clear()
+        flush.fill_(2.0)
+        e0.record(stream)
+        copy_stream.wait_event(e0)
+        with torch.cuda.stream(copy_stream):
+            for i in range(len(xs)):
+                k = len(xs[i][1])
+                kbufs[i][:k].copy_(pin_k[i], non_blocking=True)
+                vbufs[i][:k].copy_(pin_v[i], non_blocking=True)
+                ev_in[i].record(copy_stream)
         for i in range(len(xs)):
-            k = len(xs[i][1])
-            sparse_out = xs[i][0] < 1.0
-            flush.fill_(2.0)
-            e0.record(stream)
-            kbuf[:k].copy_(pin_k[i], non_blocking=True)
-            vbuf[:k].copy_(pin_v[i], non_blocking=True)
-            h.set_sparse_x(kbuf, vbuf, k)
+            stream.wait_event(ev_in[i])
+            h.set_sparse_x(kbufs[i], vbufs[i], len(xs[i][1]))
             h.run_adaptive(1.0, y)
-            if sparse_out:
-                h.dense2sparse_to_host(m, y, ykey_h, yval_h, ycnt_h)
+            if sparse_out[i]:
+                h.dense2sparse_to_host(m, y, ykey_h[i], yval_h[i], ycnt_h[i:i + 1])
             else:
                 yhost.copy_(y, non_blocking=True)
-            e1.record(stream)
-            stream.synchronize()
-            tot += e0.elapsed_time(e1)
-            ynz = int(ycnt_h[0]) if sparse_out else m
-            d2h_calls.append(4 + 8 * ynz if sparse_out else 4 * m)
+        e1.record(stream)
+        stream.synchronize()
+        d2h_calls.clear()
+        for i in range(len(xs)):
+            ynz = int(ycnt_h[i]) if sparse_out[i] else m
+            d2h_calls.append(4 + 8 * ynz if sparse_out[i] else 4 * m)
             if check and ref64:
                 got = np.zeros(m, np.float64)
-                if sparse_out:
-                    got[ykey_h[:ynz].numpy()] = yval_h[:ynz].numpy()
+                if sparse_out[i]:
+                    got[ykey_h[i][:ynz].numpy()] = yval_h[i][:ynz].numpy()
                 else:
                     got[:] = yhost.numpy()
                 e2e_ok.append(bool(orc.within_tol(got, ref64[i][0], ref64[i][1], 1e-5)[0]))
-        return tot
+        return e0.elapsed_time(e1)
 
     for _ in range(max(args.warmup, 3)):
         e2e_step()
@@ -555,19 +586,22 @@ def run_ours(args, world, rank, local):
     adjoint = run_adjoint(torch, dev, stream, args) if rank == 0 and not args.no_batched else None
     ingest = run_ingest(torch, dev, stream, args) if rank == 0 and not args.no_ingest else None
     hybrid = run_hybrid(torch, dev, stream, args) if rank == 0 and not args.no_batched else None
+    powerlaw = run_powerlaw(torch, dev, stream, args) if rank == 0 and not args.no_batched else None
 
     line = None
     if rank == 0:
         cpu = cpu_baseline(A, xs, binl) if not args.no_cpu and world == 1 else None
         sweep = [{"density": dd, "x_nnz": k, "bin_len": b, "kernel": abi.KERNEL_NAMES[c],
-                  "ms": float(t), "eff_gbs": eb / (t * 1e-3) / 1e9}
-                 for (dd, _, _, k), b, c, t, eb in zip(dx, binl, chosen, per, ebytes)]
+                  "ms_alone_flushed": float(t1), "eff_gbs_alone_flushed": eb / (t1 * 1e-3) / 1e9}
+                 for (dd, _, _, k), b, c, t1, eb in zip(dx, binl, chosen, per_call, ebytes)]
         line = {
             "metric": METRIC, "value": value, "unit": "GB/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": step_ms_max,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic",
-            "config": {"workload": WORKLOAD, "l2": "flushed (256 MiB write) before every timed call",
+            "config": {"workload": WORKLOAD,
+                       "step": "the six adaptive calls of the sweep, back to back through the public API",
+                       "l2": "flushed (256 MiB write) before every timed step",
                        "row_lengths": {"mean": float(np.mean(np.diff(A.rowptr))),
                                        "max": int(np.max(np.diff(A.rowptr))),
                                        "std": float(np.std(np.diff(A.rowptr)))},
@@ -580,7 +614,8 @@ def run_ours(args, world, rank, local):
             "e2e": {"value": e2e_val, "unit": "GB/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms,
                     "host_results_within_1e-5": bool(e2e_ok) and all(e2e_ok)},
-            "gpu_launches": int(launches // max(args.steps, 1)),
+            "gpu_launches": int(launches),
+            "gpu_launches_per_step": int(launches_per_step),
             "clocks": clk.summary(),
             "sweep": sweep,
             "correctness": correctness,
@@ -592,6 +627,7 @@ def run_ours(args, world, rank, local):
             "adjoint": adjoint,
             "ingest": ingest,
             "hybrid_candidate": hybrid,
+            "powerlaw_spmv": powerlaw,
         }
         print(json.dumps(line), flush=True)
     h.Destroy()
@@ -893,6 +929,52 @@ def run_adjoint(torch, dev, stream, args):
             "forward_gbs": fb / (f_ms * 1e-3) / 1e9, "backward_gbs": bb / (b_ms * 1e-3) / 1e9}
 
 
+def run_powerlaw(torch, dev, stream, args):
+    """SpMV on power-law matrices through the autotuned dispatcher: the
+    Chung-Lu graph of the batched benchmark at 1,048,576 vertices (exponent
+    2.1, average degree 32, N(0,1) values, seed 5) and R-MAT scale 20 (edge
+    factor 16, seed 1, U(-1,1) values).  L2 flushed before every timed call;
+    the roofline is the SpMV's compulsory bytes over the measured HBM peak;
+    the result is checked against the FP64 oracle."""
+    import spmx
+    from spmx import gen
+    import oracle.oracle as orc
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    peak, peak_kind = peaks()
+    out = []
+    g = gen.rmat(20, 16, seed=1)
+    g.val = np.random.default_rng(7).uniform(-1, 1, g.nnz).astype(np.float32)
+    for name, A in (("chung-lu-1M", gen.chung_lu(1 << 20, 2.1, 32.0, seed=5)), ("rmat-20", g)):
+        t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)  # noqa: E731
+        h = spmx.SpmspvHandle(A.m, A.n, A.nnz, stream=stream)
+        h.InputCSR(A.nnz, t(A.rowptr), t(A.col), t(A.val))
+        h.holaPreprocess()
+        backend = SPMV_BACKENDS.get(h.autotune(), "?")
+        x_h = np.random.default_rng(3).uniform(-1, 1, A.n).astype(np.float32)
+        h.set_x(t(x_h))
+        y = torch.empty(A.m, device=dev)
+        ts = []
+        for it in range(3 + max(args.steps, 5)):
+            flush.fill_(float(it))
+            e0.record(stream)
+            h.spmv(1.0, y)
+            e1.record(stream)
+            stream.synchronize()
+            if it >= 3:
+                ts.append(e0.elapsed_time(e1))
+        h.check_device_error()
+        y64, mag = orc.spmv_f64(A.rowptr, A.col, A.val, x_h)
+        ok = bool(orc.within_tol(y.cpu().numpy(), y64, mag, 1e-5)[0])
+        ms = statistics.median(ts)
+        b = spmv_bytes(A.m, A.n, A.nnz)
+        h.Destroy()
+        out.append({"matrix": name, "nnz": A.nnz, "backend": backend, "ms": ms,
+                    "gbs": b / (ms * 1e-3) / 1e9, "frac": b / (ms * 1e-3) / 1e9 / peak,
+                    "peak_kind": peak_kind, "within_1e-5": ok})
+    return out
+
+
 def _ref_host_lib():
     """The reference's host routines compiled from its sources (oracle/_ref),
     or None where they were not built."""
@@ -1094,7 +1176,7 @@ def cpu_baseline(A, xs, binl):
             "ms": best * 1e3}
 
 
-ONLY = ("hybrid", "ingest", "batched-spmspv", "adjoint", "hola-spmv", "csr5-spmv", "naive-spmv", "tiled-spmv", "round-spmv", "hola-spmspv", "csc-lb-atomic",
+ONLY = ("powerlaw", "hybrid", "ingest", "batched-spmspv", "adjoint", "hola-spmv", "csr5-spmv", "naive-spmv", "tiled-spmv", "round-spmv", "hola-spmspv", "csc-lb-atomic",
         "csc-naive-atomic", "csc-bucket", "csc-lb-sort", "bfs-rmat14", "bfs-batched")
 
 
@@ -1122,6 +1204,9 @@ def run_only(args):
         return 0
     if args.only == "hybrid":
         print(json.dumps(run_hybrid(torch, dev, stream, args)))
+        return 0
+    if args.only == "powerlaw":
+        print(json.dumps(run_powerlaw(torch, dev, stream, args)))
         return 0
     A, xs = make_inputs()
     d = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)  # noqa: E731

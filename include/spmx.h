@@ -228,15 +228,26 @@ int spmx_tiledspmspv(spmx_handle_t h, float alpha, float* d_y);
  * row block needs more accumulators than shared memory holds, the
  * preprocessing retries with row blocks half as tall (up to 5 times).  Fails
  * with SPMX_ERR_INVALID_VALUE (the other back-ends still apply) when a column
- * index is out of range, when 128 consecutive nonzeros of a row block span
- * 2^16 columns or more (a very sparse row block), when the accumulators
- * still do not fit, or when row blocks x columns need a sort key of more
- * than 32 bits. */
+ * index is out of range, when the accumulators still do not fit, or when
+ * row blocks x columns need a sort key of more than 32 bits.  When 128
+ * consecutive nonzeros of a row block (a very sparse row block) span 2^16
+ * columns or more, the format is rebuilt with every 2^16-column segment
+ * starting a new 128-entry chunk. */
 int spmx_round_preprocess(spmx_handle_t h, int rb_rows);
+/* No reference counterpart.  The round format with `parts` CTAs per row
+ * block: 2 (what spmx_round_preprocess builds: one 2-CTA cluster per row
+ * block) or 4 (two clusters per row block, each row block twice as tall, the
+ * row sums folded into each row's first accumulator slot; the two clusters'
+ * sums meet in a small device buffer and the second to finish a row slice
+ * stores y, so every row is still added in a fixed order).  Taller row blocks
+ * put more nonzeros on each column range of x, so fewer x cache lines are
+ * gathered per nonzero. */
+int spmx_round_preprocess_parts(spmx_handle_t h, int rb_rows, int parts);
 int spmx_round_postprocess(spmx_handle_t h);
-/* geometry chosen by spmx_round_preprocess: info[0..7] = row blocks, CTAs
- * per cluster, rounds, nonzeros per round, accumulator slots per CTA, shared
- * y rows, shared bytes, grid */
+/* geometry chosen by spmx_round_preprocess(_parts): info[0..7] = row blocks,
+ * CTAs per row block (2 or 4; clusters are always 2 CTAs), rounds, nonzeros
+ * per round, accumulator slots per CTA, rows per row block (at most), shared
+ * bytes, grid */
 int spmx_round_info(spmx_handle_t h, int* info);
 int spmx_roundspmv(spmx_handle_t h, float alpha, float* d_y);
 int spmx_roundspmspv(spmx_handle_t h, float alpha, float* d_y);

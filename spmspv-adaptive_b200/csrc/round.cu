@@ -67,6 +67,10 @@ struct RoundGeom {
 
 struct RoundTables {
   int nrb = 0, grid = 0, rmax = 0, nrounds = 0, nslots = 0;
+  int parts = kRoundCS;           // CTAs per row block: one cluster, or two (then psum / pcnt)
+  bool inplace = false;           // row sums folded into each row's first slot
+  float* psum = nullptr;          // parts > 2: each cluster's row sums, [parts / 2][m]
+  unsigned* pcnt = nullptr;       // parts > 2: arrivals per (row block, row slice)
   RoundGeom geom = {};
   size_t smem = 0;
   int* rb_row = nullptr;          // nrb + 1 row block boundaries
@@ -81,21 +85,28 @@ static RoundTables* rtab(spmx_handle_t h) { return reinterpret_cast<RoundTables*
 
 namespace {
 
-// shared memory: nslots accumulators (rounded to 4), then rmax row sums
-size_t round_smem(int nslots, int rmax) { return 4 * (size_t)(((nslots + 3) & ~3) + rmax); }
+// shared memory: nslots accumulators (rounded to 4), then (unless the row
+// sums are folded into the slots) rmax row sums
+size_t round_smem(int nslots, int rmax, bool inplace) {
+  return 4 * (size_t)(((nslots + 3) & ~3) + (inplace ? 0 : rmax));
+}
 
-template <bool GATED>
+// parts CTAs per row block, in clusters of 2; with parts = 4 each cluster
+// adds its two CTAs' row sums and the two clusters meet in psum: the second
+// to arrive at a row slice writes y (no waiting, a fixed order of addition).
+template <bool GATED, bool INPLACE>
 __global__ void __launch_bounds__(kRoundNW * 32, 1)
-round_spmv_kernel(const __grid_constant__ RoundGeom geom, int nslots, const int* __restrict__ rb_row,
+round_spmv_kernel(const __grid_constant__ RoundGeom geom, int nslots, int parts, const int* __restrict__ rb_row,
                   const int* __restrict__ cta_round,
                   const uint4* __restrict__ packed, const float4* __restrict__ val,
                   const int* __restrict__ cbase, const int* __restrict__ vbg, const float* __restrict__ x,
-                  const unsigned* __restrict__ xbits, float alpha, float* __restrict__ y) {
+                  const unsigned* __restrict__ xbits, float alpha, float* __restrict__ y, int m,
+                  float* __restrict__ psum, unsigned* __restrict__ pcnt) {
   constexpr int E = kRoundE, CPW = kRoundCPW;
   extern __shared__ __align__(16) float ys[];
   float* F = ys + ((nslots + 3) & ~3);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int rb = blockIdx.x / kRoundCS;
+  const int rb = blockIdx.x / parts;
   const int row0 = geom.use ? geom.rb_row[rb] : __ldg(rb_row + rb);
   const int rows = (geom.use ? geom.rb_row[rb + 1] : __ldg(rb_row + rb + 1)) - row0;
   const int k0 = geom.use ? geom.cta_round[blockIdx.x] : __ldg(cta_round + blockIdx.x);
@@ -165,7 +176,8 @@ round_spmv_kernel(const __grid_constant__ RoundGeom geom, int nslots, const int*
     step(k, pa, va, ba, xa, pb, bb, xb);
     if (k + 1 < k1) step(k + 1, pb, vb, bb, xb, pa, ba, xa);
   }
-  // each row's slots, summed in slot order
+  // each row's slots, summed in slot order, into F[r] or (INPLACE) into the
+  // row's first slot; a row without slots has the sum 0
   const int base0 = __ldg(vbg + row0);
   constexpr int FU = 8;  // rows per thread per pass: their slot bounds are loaded together
   for (int rb4 = 0; rb4 < rows; rb4 += FU * (int)blockDim.x) {
@@ -182,32 +194,70 @@ round_spmv_kernel(const __grid_constant__ RoundGeom geom, int nslots, const int*
       if (r < rows) {
         float acc = 0.f;
         for (int s = lo[j] - base0; s < hi[j] - base0; ++s) acc += ys[s];
-        F[r] = acc;
+        if (!INPLACE) F[r] = acc;
+        else if (hi[j] > lo[j]) ys[lo[j] - base0] = acc;  // rows own disjoint slots
       }
     }
   }
-  // the cluster's row sums, added in rank order; each CTA stores a slice
+  // the cluster's row sums, added in rank order; each CTA takes a slice
   cg::cluster_group cl = cg::this_cluster();
   cl.sync();
   const int rank = (int)cl.block_rank();
   const int slice = (rows + kRoundCS - 1) / kRoundCS;
   const int r0 = rank * slice, r1 = min(rows, r0 + slice);
+  const int nclu = parts / kRoundCS;  // clusters per row block
+  float* mine = nclu > 1 ? psum + (size_t)((blockIdx.x % parts) / kRoundCS) * m + row0 : nullptr;
   constexpr int CU = 4;  // rows per thread per pass: their peer reads are issued together
   for (int rc = r0; rc < r1; rc += CU * (int)blockDim.x) {
     float acc[CU];
+    int at[CU];  // where the row's sum lives: F[r], or its first slot (-1: no slots)
 #pragma unroll
     for (int j = 0; j < CU; ++j) {
       const int r = rc + j * (int)blockDim.x + (int)threadIdx.x;
-      acc[j] = 0.f;
-      if (r < r1) {
-#pragma unroll
-        for (int q = 0; q < kRoundCS; ++q) acc[j] += *cl.map_shared_rank(F + r, q);
+      at[j] = r;
+      if (INPLACE && r < r1) {
+        const int lo = __ldg(vbg + row0 + r);
+        at[j] = __ldg(vbg + row0 + r + 1) > lo ? lo - base0 : -1;
       }
     }
 #pragma unroll
     for (int j = 0; j < CU; ++j) {
       const int r = rc + j * (int)blockDim.x + (int)threadIdx.x;
-      if (r < r1) y[row0 + r] = alpha * acc[j];
+      acc[j] = 0.f;
+      if (r < r1 && at[j] >= 0) {
+        float* src = INPLACE ? ys + at[j] : F + r;
+#pragma unroll
+        for (int q = 0; q < kRoundCS; ++q) acc[j] += *cl.map_shared_rank(src, q);
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < CU; ++j) {
+      const int r = rc + j * (int)blockDim.x + (int)threadIdx.x;
+      if (r < r1) {
+        if (nclu == 1) y[row0 + r] = alpha * acc[j];
+        else mine[r] = acc[j];
+      }
+    }
+  }
+  if (nclu > 1) {
+    // the last cluster to finish this row slice adds the clusters' sums in
+    // cluster order and stores y; its ticket is reset for the next launch
+    __shared__ int s_last;
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      unsigned* t = pcnt + (size_t)rb * kRoundCS + rank;
+      s_last = atomicAdd(t, 1u) == (unsigned)(nclu - 1);
+      if (s_last) atomicExch(t, 0u);
+    }
+    __syncthreads();
+    if (s_last) {
+      __threadfence();
+      for (int r = r0 + (int)threadIdx.x; r < r1; r += blockDim.x) {
+        float acc = 0.f;
+        for (int c = 0; c < nclu; ++c) acc += __ldcg(psum + (size_t)c * m + row0 + r);
+        y[row0 + r] = alpha * acc;
+      }
     }
   }
   cl.sync();  // peers read this CTA's row sums until here
@@ -406,14 +456,14 @@ int bits_for(long long v) {  // bits to hold values in [0, v)
   return b;
 }
 
-template <bool GATED>
+template <bool GATED, bool INPLACE>
 static void round_set_smem(size_t smem) {
-  cudaFuncSetAttribute(round_spmv_kernel<GATED>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  cudaFuncSetAttribute(round_spmv_kernel<GATED, INPLACE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
 }
 
 static long long round_static_smem() {
   cudaFuncAttributes a = {};
-  if (cudaFuncGetAttributes(&a, round_spmv_kernel<true>) != cudaSuccess) {
+  if (cudaFuncGetAttributes(&a, round_spmv_kernel<true, false>) != cudaSuccess) {
     cudaGetLastError();
     return 1024;
   }
@@ -435,6 +485,8 @@ extern "C" int spmx_round_postprocess(spmx_handle_t h) {
   dfree(t->val);
   dfree(t->cbase);
   dfree(t->vbg);
+  dfree(t->psum);
+  dfree(t->pcnt);
   delete t;
   h->round = nullptr;
   return SPMX_SUCCESS;
@@ -445,8 +497,8 @@ extern "C" int spmx_round_postprocess(spmx_handle_t h) {
 // *span when 128 consecutive nonzeros of a row block span 2^16 columns or more
 // (then a build with pad = true starts a new chunk at every 2^16-column
 // segment, which bounds every chunk's span)
-static int round_build(spmx_handle_t h, long long rcap, long long avail, bool pad, bool* overflow,
-                       bool* span) {
+static int round_build(spmx_handle_t h, long long rcap, long long avail, int parts, bool inplace, bool pad,
+                       bool* overflow, bool* span) {
   constexpr int E = kRoundE;
   spmx_round_postprocess(h);
   const int m = h->m, n = h->n, nnz = h->nnz;
@@ -459,7 +511,7 @@ static int round_build(spmx_handle_t h, long long rcap, long long avail, bool pa
   // row blocks: one wave of 2-CTA clusters when the rows fit, about equal
   // nonzero counts, boundaries on multiples of 4, at most rcap rows each
   const long long need = std::max<long long>(1, (m + rcap - 1) / rcap);
-  int nrb = (int)std::max<long long>(need, std::min<long long>(h->num_sms / kRoundCS, std::max(1, m / 4)));
+  int nrb = (int)std::max<long long>(need, std::min<long long>(h->num_sms / parts, std::max(1, m / 4)));
   nrb = std::max(1, nrb);
   const int cbits = bits_for((long long)std::max(n, 1));
   const int bbits = bits_for((long long)nrb + 1);
@@ -485,8 +537,10 @@ static int round_build(spmx_handle_t h, long long rcap, long long avail, bool pa
   RoundTables* t = new RoundTables();
   h->round = t;
   t->nrb = nrb;
-  t->grid = nrb * kRoundCS;
+  t->grid = nrb * parts;
   t->rmax = rmax;
+  t->parts = parts;
+  t->inplace = inplace;
 
   const size_t b4 = 4 * (size_t)std::max(nnz, 1);
   unsigned *k0 = nullptr, *k1 = nullptr, *a0 = nullptr, *a1 = nullptr, *v0 = nullptr, *v1 = nullptr;
@@ -564,10 +618,15 @@ static int round_build(spmx_handle_t h, long long rcap, long long avail, bool pa
       const int s = bounds[k], e = bounds[k + 1];
       const long long cnt = e - s;
       const long long nr = (cnt + E - 1) / E;
-      const int mid = s + (int)std::min<long long>(cnt, ((nr + 1) / 2) * E);
-      const int part[3] = {s, mid, e};
-      for (int c = 0; c < kRoundCS; ++c) {
-        cta[(size_t)k * kRoundCS + c] = (int)rstart.size();
+      // part q takes nr / parts whole rounds, the first nr % parts one more
+      std::vector<int> part((size_t)parts + 1, e);
+      long long acc_r = 0;
+      for (int q = 0; q <= parts; ++q) {
+        part[q] = s + (int)std::min<long long>(cnt, acc_r * E);
+        if (q < parts) acc_r += nr / parts + (q < nr % parts ? 1 : 0);
+      }
+      for (int c = 0; c < parts; ++c) {
+        cta[(size_t)k * parts + c] = (int)rstart.size();
         const int lo = part[c], hi = part[c + 1];
         if (!pad) {
           for (int p = lo; p < hi; p += E) {
@@ -681,7 +740,7 @@ static int round_build(spmx_handle_t h, long long rcap, long long avail, bool pa
     if (!rc) {
       for (int k = 0; k < nrb; ++k) nslots_real = std::max(nslots_real, bslots[k]);
       t->nslots = nslots_real + kRoundDummy;
-      t->smem = round_smem(t->nslots, rmax);
+      t->smem = round_smem(t->nslots, rmax, inplace);
       if (t->nslots >= 65536 || (long long)t->smem > avail) {
         *overflow = true;
         rc = set_error(SPMX_ERR_INVALID_VALUE,
@@ -711,12 +770,24 @@ static int round_build(spmx_handle_t h, long long rcap, long long avail, bool pa
   dfree(hist); dfree(hoff); dfree(flags); dfree(d_bounds); dfree(spr);
   dfree(d_rstart); dfree(d_rlen); dfree(d_rrb); dfree(occ); dfree(d_bslots);
   dfree(d_segb); dfree(d_rpad0); dfree(d_half_lo); dfree(d_seg_real); dfree(d_pad_off); dfree(ppos);
+  if (!rc && parts > kRoundCS) {
+    rc = dalloc((void**)&t->psum, 4 * (size_t)(parts / kRoundCS) * (size_t)std::max(m, 1), "round cluster sums");
+    rc = rc ? rc : dalloc((void**)&t->pcnt, 4 * (size_t)nrb * kRoundCS, "round cluster tickets");
+    if (!rc && cudaMemsetAsync(t->pcnt, 0, 4 * (size_t)nrb * kRoundCS, st) != cudaSuccess)
+      rc = set_error(SPMX_ERR_CUDA, "round SpMV: ticket reset");
+    if (!rc && cudaStreamSynchronize(st) != cudaSuccess) rc = set_error(SPMX_ERR_CUDA, "round SpMV: ticket reset");
+  }
   if (rc) {
     spmx_round_postprocess(h);
     return rc;
   }
-  round_set_smem<false>(t->smem);
-  round_set_smem<true>(t->smem);
+  if (inplace) {
+    round_set_smem<false, true>(t->smem);
+    round_set_smem<true, true>(t->smem);
+  } else {
+    round_set_smem<false, false>(t->smem);
+    round_set_smem<true, false>(t->smem);
+  }
   t->geom.use = t->grid <= kRoundParamCtas ? 1 : 0;
   if (t->geom.use) {
     std::copy(cta.begin(), cta.end(), t->geom.cta_round);
@@ -725,39 +796,48 @@ static int round_build(spmx_handle_t h, long long rcap, long long avail, bool pa
   return SPMX_SUCCESS;
 }
 
-extern "C" int spmx_round_preprocess(spmx_handle_t h, int rb_rows) {
+// parts = 2: one 2-CTA cluster per row block, row sums in their own shared
+// array (rows <= avail / 8), row blocks halved while the slots overflow;
+// parts = 4: two clusters per row block over twice as many rows, the row sums
+// folded into the slots (rows <= avail / 4), row blocks shrunk by 15% while
+// the slots overflow.  Either way a matrix whose 128 consecutive nonzeros
+// (in a row block's column order) span 2^16 columns or more is rebuilt with
+// every 2^16-column segment starting a new chunk.
+static int round_preprocess(spmx_handle_t h, int rb_rows, int parts) {
   if (!h) return set_error(SPMX_ERR_INVALID_VALUE, "NULL handle");
   if (!h->has_csr || (!h->val && h->nnz > 0))
     return set_error(SPMX_ERR_NOT_READY, "round SpMV needs the CSR input with values");
   if (rb_rows < 0) return set_error(SPMX_ERR_INVALID_VALUE, "round SpMV: rb_rows must be >= 0");
+  if (parts != 2 && parts != 4) return set_error(SPMX_ERR_INVALID_VALUE, "round SpMV: parts must be 2 or 4");
   int optin = 0;
   cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, h->device);
   const long long avail = (long long)optin - round_static_smem();
-  // every nonempty row needs a slot and a row sum: at most avail / 8 rows
-  long long rcap = std::min<long long>((avail / 8) & ~3LL, 65532);
+  const bool inplace = parts > 2;
+  // every nonempty row needs a slot (and, unless folded, a row sum)
+  long long rcap = std::min<long long>((avail / (inplace ? 4 : 8)) & ~3LL, 65532);
   if (rb_rows > 0) rcap = std::min<long long>(rcap, std::max(4, (rb_rows + 3) & ~3));
   if (rcap < 4) return set_error(SPMX_ERR_INVALID_VALUE, "round SpMV: no shared memory left for y");
-  // rows with many nonzeros in one round (hub rows, or rows whose nonzeros
-  // sit in neighbouring columns) need several slots each; when a row block
-  // needs more than fit, retry with row blocks half as tall (up to 5 times)
-  // A matrix whose 128 consecutive nonzeros (in a row block's column order)
-  // can span 2^16 columns or more is rebuilt with every 2^16-column segment
-  // starting a new chunk.
   bool pad = false;
   for (int attempt = 0;; ++attempt) {
     bool overflow = false, span = false;
-    const int rc = round_build(h, rcap, avail, pad, &overflow, &span);
+    const int rc = round_build(h, rcap, avail, parts, inplace, pad, &overflow, &span);
     if (rc == SPMX_SUCCESS) return rc;
     if (span && !pad) {
       pad = true;
       continue;
     }
-    if (!overflow || attempt >= 6 || rcap <= 64) return rc;
-    rcap = std::max<long long>(64, (rcap / 2) & ~3LL);
+    if (!overflow || attempt >= (inplace ? 12 : 6) || rcap <= 64) return rc;
+    rcap = std::max<long long>(64, (inplace ? rcap * 85 / 100 : rcap / 2) & ~3LL);
   }
 }
 
-template <bool GATED>
+extern "C" int spmx_round_preprocess(spmx_handle_t h, int rb_rows) { return round_preprocess(h, rb_rows, 2); }
+
+extern "C" int spmx_round_preprocess_parts(spmx_handle_t h, int rb_rows, int parts) {
+  return round_preprocess(h, rb_rows, parts);
+}
+
+template <bool GATED, bool INPLACE>
 static cudaError_t round_launch(spmx_handle_t h, RoundTables* t, float alpha, float* y, const unsigned* bits) {
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(t->grid);
@@ -773,9 +853,10 @@ static cudaError_t round_launch(spmx_handle_t h, RoundTables* t, float alpha, fl
   at[1].val.programmaticStreamSerializationAllowed = 1;
   cfg.attrs = at;
   cfg.numAttrs = 2;
-  return cudaLaunchKernelEx(&cfg, round_spmv_kernel<GATED>, t->geom, t->nslots, (const int*)t->rb_row,
-                            (const int*)t->cta_round, (const uint4*)t->packed, (const float4*)t->val,
-                            (const int*)t->cbase, (const int*)t->vbg, (const float*)h->x_dense, bits, alpha, y);
+  return cudaLaunchKernelEx(&cfg, round_spmv_kernel<GATED, INPLACE>, t->geom, t->nslots, t->parts,
+                            (const int*)t->rb_row, (const int*)t->cta_round, (const uint4*)t->packed,
+                            (const float4*)t->val, (const int*)t->cbase, (const int*)t->vbg,
+                            (const float*)h->x_dense, bits, alpha, y, h->m, t->psum, t->pcnt);
 }
 
 int round_spmv_impl(spmx_handle_t h, float alpha, float* y, bool gated) {
@@ -786,8 +867,11 @@ int round_spmv_impl(spmx_handle_t h, float alpha, float* y, bool gated) {
   if (!y && h->m > 0) return set_error(SPMX_ERR_INVALID_VALUE, "y is NULL");
   if (h->m == 0) return SPMX_SUCCESS;
   note_launch();
-  const cudaError_t e = gated ? round_launch<true>(h, t, alpha, y, (const unsigned*)h->bitvec)
-                              : round_launch<false>(h, t, alpha, y, nullptr);
+  const unsigned* bits = (const unsigned*)h->bitvec;
+  const cudaError_t e = t->inplace ? (gated ? round_launch<true, true>(h, t, alpha, y, bits)
+                                            : round_launch<false, true>(h, t, alpha, y, nullptr))
+                                   : (gated ? round_launch<true, false>(h, t, alpha, y, bits)
+                                            : round_launch<false, false>(h, t, alpha, y, nullptr));
   if (e != cudaSuccess) return set_error(SPMX_ERR_CUDA, std::string("round spmv: ") + cudaGetErrorString(e));
   return SPMX_SUCCESS;
 }
@@ -797,7 +881,7 @@ extern "C" int spmx_round_info(spmx_handle_t h, int* info) {
   RoundTables* t = rtab(h);
   if (!t) return set_error(SPMX_ERR_NOT_READY, "call spmx_round_preprocess first");
   info[0] = t->nrb;
-  info[1] = kRoundCS;
+  info[1] = t->parts;
   info[2] = t->nrounds;
   info[3] = kRoundE;
   info[4] = t->nslots;

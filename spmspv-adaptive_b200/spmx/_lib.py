@@ -102,6 +102,7 @@ _SIGS = {
     "spmx_tiledspmv": (c_int, [P, c_float, P]),
     "spmx_tiledspmspv": (c_int, [P, c_float, P]),
     "spmx_round_preprocess": (c_int, [P, c_int]),
+    "spmx_round_preprocess_parts": (c_int, [P, c_int, c_int]),
     "spmx_round_postprocess": (c_int, [P]),
     "spmx_round_info": (c_int, [P, P]),
     "spmx_roundspmv": (c_int, [P, c_float, P]),

@@ -263,19 +263,24 @@ class SpmspvHandle:
     def tiledspmspv(self, alpha, y):
         check(lib.spmx_tiledspmspv(self._h, float(alpha), _f32(y)), "tiledspmspv")
 
-    def roundPreprocess(self, rb_rows=0):
-        check(lib.spmx_round_preprocess(self._h, int(rb_rows)), "roundPreprocess")
+    def roundPreprocess(self, rb_rows=0, parts=2):
+        """Round format with `parts` CTAs per row block (2, or 4: two clusters
+        over row blocks twice as tall)."""
+        if parts == 2:
+            check(lib.spmx_round_preprocess(self._h, int(rb_rows)), "roundPreprocess")
+        else:
+            check(lib.spmx_round_preprocess_parts(self._h, int(rb_rows), int(parts)), "roundPreprocess")
 
     def roundPostprocess(self):
         check(lib.spmx_round_postprocess(self._h), "roundPostprocess")
 
     def round_info(self):
-        """Geometry of the round format: row blocks, CTAs per cluster, rounds,
+        """Geometry of the round format: row blocks, CTAs per row block, rounds,
         nonzeros per round, accumulator slots per CTA, shared y rows, shared
         bytes, grid."""
         info = (ctypes.c_int * 8)()
         check(lib.spmx_round_info(self._h, info), "round_info")
-        names = ("row_blocks", "cluster", "rounds", "round", "slots", "rmax", "smem", "grid")
+        names = ("row_blocks", "parts", "rounds", "round", "slots", "rmax", "smem", "grid")
         return dict(zip(names, list(info)))
 
     def roundspmv(self, alpha, y):

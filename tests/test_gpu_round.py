@@ -68,13 +68,14 @@ def _check_spmv(torch, h, A, alpha, x):
 
 @pytest.mark.parametrize("name,A", ALL, ids=[c[0] for c in ALL])
 @pytest.mark.parametrize("rb", [0, 64])
-def test_round_spmv(torch_cuda, name, A, rb):
+@pytest.mark.parametrize("parts", [2, 4])
+def test_round_spmv(torch_cuda, name, A, rb, parts):
     torch = torch_cuda
     h = make_handle(A, torch, csc=False, hola=False)
-    h.roundPreprocess(rb)
+    h.roundPreprocess(rb, parts)
     info = h.round_info()
-    assert info["cluster"] == 2 and info["round"] == 4096
-    assert info["grid"] == 2 * info["row_blocks"]
+    assert info["parts"] == parts and info["round"] == 4096
+    assert info["grid"] == parts * info["row_blocks"]
     assert info["rounds"] >= (A.nnz + 4095) // 4096
     # every row with a nonzero has an accumulator; the 32 padding slots follow
     assert info["slots"] >= 32 + min(A.m, np.count_nonzero(np.diff(A.rowptr))) // max(1, info["row_blocks"])
@@ -107,14 +108,15 @@ def test_round_spmv(torch_cuda, name, A, rb):
     h.roundPostprocess()
 
 
-def test_round_zipf_full_size(torch_cuda):
+@pytest.mark.parametrize("parts", [2, 4])
+def test_round_zipf_full_size(torch_cuda, parts):
     torch = torch_cuda
     from spmx import gen
     A = gen.zipf_1m()
     h = make_handle(A, torch, csc=False, hola=False)
-    h.roundPreprocess()
+    h.roundPreprocess(0, parts)
     info = h.round_info()
-    assert info["row_blocks"] == 74 and info["grid"] == 148
+    assert info["row_blocks"] == 148 // parts and info["grid"] == 148
     x = np.random.default_rng(2).uniform(-1, 1, A.n).astype(np.float32)
     h.set_x(dev(x, torch))
     _check_spmv(torch, h, A, 1.0, x)
