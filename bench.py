@@ -443,6 +443,19 @@ def run_ours(args, world, rank, local):
         if it >= 3:
             per_call += np.array([a.elapsed_time(b) for a, b in ev1])
     per_call /= args.steps
+    # the same timing around a kernel that writes one float: what an event
+    # pair around any single launch costs after the flush
+    tiny = torch.zeros(1, device=dev)
+    floor_t = []
+    for it in range(3 + args.steps):
+        flush.fill_(float(it))
+        ev1[0][0].record(stream)
+        tiny.fill_(float(it))
+        ev1[0][1].record(stream)
+        stream.synchronize()
+        if it >= 3:
+            floor_t.append(ev1[0][0].elapsed_time(ev1[0][1]))
+    floor_ms = statistics.median(floor_t)
 
     # --- roofline: the load-balanced SpMV on the dense x (the dominant call of
     # the sweep), through the dispatcher, i.e. the back-end the autotuner chose
@@ -618,6 +631,7 @@ def run_ours(args, world, rank, local):
             "gpu_launches_per_step": int(launches_per_step),
             "clocks": clk.summary(),
             "sweep": sweep,
+            "one_kernel_floor_ms": floor_ms,
             "correctness": correctness,
             "selector_vs_exhaustive": exhaustive,
             "cpu_baseline": cpu,
@@ -769,6 +783,10 @@ def run_batched_spmspv(torch, dev, stream, args):
     dvals = torch.empty(A.nnz, device=dev)
     s = torch.cuda.Stream(device=dev)
     h.set_stream(s)
+    # the backward reuses the forward's inversion of the batch and accumulates
+    # dxval in the dvals pass (atomic adds: dxval not bitwise reproducible)
+    from spmx import abi
+    h.set_batch_options(abi.BATCH_REUSE_INVERSION | abi.BATCH_FUSED_DXVAL)
     with torch.cuda.stream(s):
         h.spmspv_batched(xp, xk, xv, 1.0, Y, x_total=tot)
         h.spmspv_batched_backward(xp, xk, xv, 1.0, dY, dxval, dvals, x_total=tot)
@@ -824,6 +842,7 @@ def run_batched_spmspv(torch, dev, stream, args):
     got_dv = dvals[torch.from_numpy(ks).to(dev)].cpu().numpy()
     bwd_ok = bool(bwd_ok and orc.within_tol(got_dv, dv64, dvmag, 1e-5)[0])
     bins = int(np.sum(colptr_h[xkey + 1] - colptr_h[xkey]))
+    h.set_batch_options(0)
     # 256 sequential single-vector calls: the forward through the adaptive
     # single-vector engine (selector + CSC SpMSpV into a dense y), the backward
     # through the batched entry point with one vector and without dvals (its
@@ -862,6 +881,8 @@ def run_batched_spmspv(torch, dev, stream, args):
             "graph_fwd_bwd_ms": mb, "plain256_fwd_bwd_ms": mp, "speedup": mp / mb,
             "eff_gbs": (fwd_b + bwd_b) / (mb * 1e-3) / 1e9, "forward_within_1e-5": bool(ok),
             "backward_within_1e-5": bwd_ok,
+            "options": "backward reuses the forward's inversion; dxval accumulated in the dvals pass "
+                       "(atomic adds, not bitwise reproducible)",
             "note": "single calls: adaptive single-vector SpMSpV forward + one-vector backward "
                     "without dvals (less work than the batch, which also computes dvals)"}
 

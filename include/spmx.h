@@ -453,10 +453,26 @@ int spmx_spmspv_batched(spmx_handle_t h, int nvec, int x_total, const int* d_xpt
  *   dxval[e] = alpha * sum_i A[i][xkey[e]] * dY[i * nvec + v(e)]   (needs the CSC)
  *   dvals[k] = alpha * sum over the batch's entries e in column col_k of
  *              xval[e] * dY[row_k * nvec + v(e)]                    (CSR order)
- * Both are written in full, deterministically.  Either output may be NULL. */
+ * Both are written in full, deterministically (dxval not bitwise so with
+ * SPMX_BATCH_FUSED_DXVAL, below).  Either output may be NULL. */
 int spmx_spmspv_batched_backward(spmx_handle_t h, int nvec, int x_total, const int* d_xptr,
                                  const int* d_xkey, const float* d_xval, float alpha,
                                  const float* d_dY, float* d_dxval, float* d_dvals);
+/* No reference counterpart.  Options of the batched entry points (flags,
+ * default 0):
+ *   SPMX_BATCH_REUSE_INVERSION: a backward call on the same batch (the same
+ *     xptr / xkey pointers, nvec and x_total) as the handle's last forward
+ *     call reuses that call's inversion of the batch instead of sorting it
+ *     again.  The caller promises that xptr and xkey were not changed in
+ *     between.
+ *   SPMX_BATCH_FUSED_DXVAL: when a backward call asks for both dxval and
+ *     dvals, dxval is accumulated during the dvals pass (which holds dY's rows
+ *     in shared memory) with atomic adds, instead of a separate pass over the
+ *     CSC that reads dY one element at a time.  dxval is then not bitwise
+ *     reproducible (the order of its additions varies); dvals still is. */
+#define SPMX_BATCH_REUSE_INVERSION 1
+#define SPMX_BATCH_FUSED_DXVAL 2
+int spmx_set_batch_options(spmx_handle_t h, int flags);
 
 /* ======================= device counters ================================== */
 /* device pointers to the handle's counters: [0] y_nnz of the last SpMSpV,

@@ -109,12 +109,15 @@ batch_forward_kernel(int m, int n, int nvec, const int* __restrict__ rowptr, con
 }
 
 // dvals[k] = alpha * sum over column col_k's pairs of xval[e] * dY[i][v(e)],
-// one warp per row with dY's row in shared memory
+// one warp per row with dY's row in shared memory.  With dxval (fused form,
+// dxval zeroed before) every pair also adds alpha * a[k] * dY[i][v(e)] into
+// dxval[e] with an atomic add.
 __global__ void __launch_bounds__(kBatchWarps * 32)
 batch_dvals_kernel(int m, int n, int nvec, const int* __restrict__ rowptr, const int* __restrict__ col,
                    const int* __restrict__ invptr, const unsigned* __restrict__ inv_ent,
                    const unsigned* __restrict__ inv_vec, const float* __restrict__ xval, float alpha,
-                   const float* __restrict__ dY, float* __restrict__ dvals, int* err) {
+                   const float* __restrict__ dY, float* __restrict__ dvals, const float* __restrict__ val,
+                   float* __restrict__ dxval, int* err) {
   extern __shared__ float s_dy[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   float* g = s_dy + warp * nvec;
@@ -130,8 +133,13 @@ batch_dvals_kernel(int m, int n, int nvec, const int* __restrict__ rowptr, const
       float s = 0.f;
       if ((unsigned)j < (unsigned)n) {
         const int p1 = __ldg(invptr + j + 1);
-        for (int p = __ldg(invptr + j); p < p1; ++p)
-          s += __ldg(xval + __ldg(inv_ent + p)) * g[__ldg(inv_vec + p)];
+        const float a = dxval ? alpha * __ldg(val + k) : 0.f;
+        for (int p = __ldg(invptr + j); p < p1; ++p) {
+          const unsigned e = __ldg(inv_ent + p);
+          const float gv = g[__ldg(inv_vec + p)];
+          s += __ldg(xval + e) * gv;
+          if (dxval) atomicAdd(dxval + e, a * gv);
+        }
       } else {
         flag_error(err, kDevErrOob);
       }
@@ -177,8 +185,11 @@ batch_dxval_kernel(int m, int n, int nvec, int total, const int* __restrict__ xp
 using namespace spmx;
 
 // scratch for the inverted batch of x_total entries (grown, never shrunk)
+static void batch_forget_inversion(spmx_handle_t h);
+
 static int ensure_batch_scratch(spmx_handle_t h, int total) {
   if (h->batch_cap >= total && h->batch_invptr_n == h->n && h->batch_invptr) return SPMX_SUCCESS;
+  batch_forget_inversion(h);
   cudaStreamSynchronize(h->stream);
   const int cap = std::max(total, 1);
   for (auto& p : h->batch_buf) {
@@ -202,9 +213,24 @@ static int ensure_batch_scratch(spmx_handle_t h, int total) {
   return SPMX_SUCCESS;
 }
 
-// invert the batch: per column, the (entry, vector) pairs in entry order
+static void batch_forget_inversion(spmx_handle_t h) {
+  h->inv_xptr = h->inv_xkey = nullptr;
+  h->inv_nvec = h->inv_total = -1;
+  h->inv_ent = h->inv_vec = nullptr;
+}
+
+// invert the batch: per column, the (entry, vector) pairs in entry order.
+// A forward call records which batch the inversion belongs to; a backward
+// call with SPMX_BATCH_REUSE_INVERSION set reuses it for the same batch.
 static int batch_invert(spmx_handle_t h, int nvec, int total, const int* xptr, const int* xkey,
-                        const unsigned** inv_ent, const unsigned** inv_vec) {
+                        bool forward, const unsigned** inv_ent, const unsigned** inv_vec) {
+  if (!forward && (h->batch_opts & SPMX_BATCH_REUSE_INVERSION) && h->inv_ent && h->inv_xptr == xptr &&
+      h->inv_xkey == xkey && h->inv_nvec == nvec && h->inv_total == total && h->batch_invptr_n == h->n) {
+    *inv_ent = h->inv_ent;
+    *inv_vec = h->inv_vec;
+    return SPMX_SUCCESS;
+  }
+  batch_forget_inversion(h);
   SPMX_TRY(ensure_batch_scratch(h, total));
   cudaStream_t st = h->stream;
   unsigned** b = reinterpret_cast<unsigned**>(h->batch_buf);
@@ -223,6 +249,14 @@ static int batch_invert(spmx_handle_t h, int nvec, int total, const int* xptr, c
   *inv_vec = rb.result_in_alt ? b[5] : b[4];
   note_launch();
   batch_bounds_kernel<<<(h->n + 1 + 255) / 256, 256, 0, st>>>(total, skey, h->n, h->batch_invptr);
+  if (forward) {
+    h->inv_xptr = xptr;
+    h->inv_xkey = xkey;
+    h->inv_nvec = nvec;
+    h->inv_total = total;
+    h->inv_ent = *inv_ent;
+    h->inv_vec = *inv_vec;
+  }
   return SPMX_SUCCESS;
 }
 
@@ -254,7 +288,7 @@ extern "C" int spmx_spmspv_batched(spmx_handle_t h, int nvec, int x_total, const
   if (!d_Y && h->m > 0) return set_error(SPMX_ERR_INVALID_VALUE, "Y is NULL");
   if (x_total > 0 && (!d_xkey || !d_xval)) return set_error(SPMX_ERR_INVALID_VALUE, "NULL batch arrays");
   const unsigned *ie = nullptr, *iv = nullptr;
-  SPMX_TRY(batch_invert(h, nvec, x_total, d_xptr, d_xkey, &ie, &iv));
+  SPMX_TRY(batch_invert(h, nvec, x_total, d_xptr, d_xkey, true, &ie, &iv));
   if (h->m == 0) return SPMX_SUCCESS;
   const size_t smem = 4 * (size_t)kBatchWarps * nvec;
   if (smem > 48 * 1024)
@@ -274,18 +308,21 @@ extern "C" int spmx_spmspv_batched_backward(spmx_handle_t h, int nvec, int x_tot
   if (!d_dY && h->m > 0) return set_error(SPMX_ERR_INVALID_VALUE, "dY is NULL");
   if (x_total > 0 && (!d_xkey || !d_xval)) return set_error(SPMX_ERR_INVALID_VALUE, "NULL batch arrays");
   cudaStream_t st = h->stream;
+  // fused form: dxval accumulated by the dvals pass
+  const bool fused = (h->batch_opts & SPMX_BATCH_FUSED_DXVAL) && d_dxval && d_dvals && h->nnz > 0 && x_total > 0;
+  if (fused) SPMX_CUDA(cudaMemsetAsync(d_dxval, 0, 4 * (size_t)x_total, st));
   if (d_dvals && h->nnz > 0) {
     const unsigned *ie = nullptr, *iv = nullptr;
-    SPMX_TRY(batch_invert(h, nvec, x_total, d_xptr, d_xkey, &ie, &iv));
+    SPMX_TRY(batch_invert(h, nvec, x_total, d_xptr, d_xkey, false, &ie, &iv));
     const size_t smem = 4 * (size_t)kBatchWarps * nvec;
     if (smem > 48 * 1024)
       cudaFuncSetAttribute(batch_dvals_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     note_launch();
     batch_dvals_kernel<<<batch_rows_grid(h, (const void*)batch_dvals_kernel, smem), kBatchWarps * 32, smem,
                          st>>>(h->m, h->n, nvec, h->rowptr, h->col, h->batch_invptr, ie, iv, d_xval, alpha,
-                               d_dY, d_dvals, h->d_err);
+                               d_dY, d_dvals, h->val, fused ? d_dxval : nullptr, h->d_err);
   }
-  if (d_dxval && x_total > 0) {
+  if (d_dxval && x_total > 0 && !fused) {
     if (!h->has_csc || !h->csc_val)
       return set_error(SPMX_ERR_NOT_READY, "dxval needs the CSC with values (spmx_to_csc)");
     const long long warps = x_total;
@@ -295,4 +332,12 @@ extern "C" int spmx_spmspv_batched_backward(spmx_handle_t h, int nvec, int x_tot
                                              h->csc_row, h->csc_val, alpha, d_dY, d_dxval, h->d_err);
   }
   return launch_ok("batched spmspv backward");
+}
+
+extern "C" int spmx_set_batch_options(spmx_handle_t h, int flags) {
+  SPMX_CHECK_HANDLE(h);
+  if (flags & ~(SPMX_BATCH_REUSE_INVERSION | SPMX_BATCH_FUSED_DXVAL))
+    return set_error(SPMX_ERR_INVALID_VALUE, "unknown batch option flags");
+  h->batch_opts = flags;
+  return SPMX_SUCCESS;
 }

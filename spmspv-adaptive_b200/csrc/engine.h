@@ -128,6 +128,13 @@ struct spmx_handle_s {
   int* batch_invptr = nullptr;
   int batch_cap = 0;
   int batch_invptr_n = -1;
+  int batch_opts = 0;  // SPMX_BATCH_* flags (spmx_set_batch_options)
+  // the batch the current inversion belongs to (valid after a forward call)
+  const void* inv_xptr = nullptr;
+  const void* inv_xkey = nullptr;
+  int inv_nvec = -1, inv_total = -1;
+  const unsigned* inv_ent = nullptr;
+  const unsigned* inv_vec = nullptr;
   // hub chunks of the multi-source pull (built once per matrix)
   int4* ms_hchunk = nullptr;
   int* ms_hcnt = nullptr;

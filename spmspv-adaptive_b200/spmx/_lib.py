@@ -41,6 +41,7 @@ VEC_SPARSE, VEC_DENSE, VEC_BITARRAY = 0, 1, 2
 SPMV_HOLA, SPMV_CSR5, SPMV_TILED, SPMV_ROUND = 0, 1, 2, 3
 CSC_NAIVE, CSC_LB_MERGE, CSC_LB_TWOLAYER, CSC_BUCKET = 0, 1, 2, 3
 WB_ATOMIC, WB_SORT = 0, 1
+BATCH_REUSE_INVERSION, BATCH_FUSED_DXVAL = 1, 2
 (K_CSC_NAIVE_SORT, K_CSC_NAIVE_ATOMIC, K_CSC_LB_SORT, K_CSC_LB_ATOMIC,
  K_CSR_NAIVE_SPMSPV, K_CSR_LB_SPMSPV, K_NAIVE_SPMV, K_LB_SPMV) = range(8)
 NUM_KERNELS = 8
@@ -98,6 +99,7 @@ _SIGS = {
     "spmx_tiled_postprocess": (c_int, [P]),
     "spmx_tiled_info": (c_int, [P, P]),
     "spmx_spmspv_batched": (c_int, [P, c_int, c_int, P, P, P, c_float, P]),
+    "spmx_set_batch_options": (c_int, [P, c_int]),
     "spmx_spmspv_batched_backward": (c_int, [P, c_int, c_int, P, P, P, c_float, P, P, P]),
     "spmx_tiledspmv": (c_int, [P, c_float, P]),
     "spmx_tiledspmspv": (c_int, [P, c_float, P]),

@@ -454,6 +454,10 @@ class SpmspvHandle:
               "spmv_backward_sparse")
 
     # -- batched SpMSpV (no reference counterpart) ------------------------------
+    def set_batch_options(self, flags):
+        """SPMX_BATCH_REUSE_INVERSION (1) | SPMX_BATCH_FUSED_DXVAL (2); 0 = none."""
+        check(lib.spmx_set_batch_options(self._h, int(flags)), "set_batch_options")
+
     def spmspv_batched(self, xptr, xkey, xval, alpha, Y, x_total=None):
         """Y = alpha * A @ X for the nvec = len(xptr) - 1 sparse vectors of the
         concatenated (xkey, xval); Y is (m, nvec) float32 on the device.

@@ -195,3 +195,60 @@ def test_batched_deterministic(torch_cuda, problem):
         h.spmspv_batched_backward(xp, xk, xv, 1.0, dY, dxval, dvals)
         outs.append((dxval.cpu().numpy(), dvals.cpu().numpy()))
     assert np.array_equal(outs[0][0], outs[1][0]) and np.array_equal(outs[0][1], outs[1][1])
+
+
+@pytest.mark.parametrize("graph", [False, True])
+def test_batched_options_reuse_and_fused(torch_cuda, problem, graph):
+    """With SPMX_BATCH_REUSE_INVERSION | SPMX_BATCH_FUSED_DXVAL the backward
+    reuses the forward's inversion and accumulates dxval in the dvals pass;
+    results stay within the same bounds, directly and replayed from a graph.
+    A backward on another batch (other pointers) inverts again."""
+    torch = torch_cuda
+    from spmx import abi
+    A, xptr, xkey, xval = problem
+    h = make_handle(A, torch, hola=False)
+    h.set_batch_options(abi.BATCH_REUSE_INVERSION | abi.BATCH_FUSED_DXVAL)
+    nvec = len(xptr) - 1
+    xp, xk, xv = dev(xptr, torch), dev(xkey, torch), dev(xval, torch)
+    dYh = np.random.default_rng(12).standard_normal((A.m, nvec)).astype(np.float32)
+    dY = dev(dYh, torch)
+    Y = torch.empty((A.m, nvec), device="cuda")
+    dxval = torch.full((len(xkey),), 7.0, device="cuda")
+    dvals = torch.full((A.nnz,), 7.0, device="cuda")
+    tot = int(xptr[-1])
+    s = torch.cuda.Stream()
+    h.set_stream(s)
+
+    def work():
+        h.spmspv_batched(xp, xk, xv, 0.5, Y, x_total=tot)
+        h.spmspv_batched_backward(xp, xk, xv, 0.5, dY, dxval, dvals, x_total=tot)
+
+    with torch.cuda.stream(s):
+        work()
+    s.synchronize()
+    if graph:
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g, stream=s):
+            work()
+        for t in (Y, dxval, dvals):
+            t.fill_(3.0)
+        g.replay()
+        s.synchronize()
+    h.check_device_error()
+    _check_forward(A, xptr, xkey, xval, Y.cpu().numpy(), 0.5)
+    dx, dxm, dv, dvm = _refs(A, xptr, xkey, xval, dYh, 0.5)
+    assert _close(dxval.cpu().numpy(), dx, dxm)
+    assert _close(dvals.cpu().numpy(), dv, dvm)
+    # another batch: the backward must not reuse the first batch's inversion
+    xptr2, xkey2, xval2 = _batch(A.n, 5, seed=21, with_empty=False)
+    xp2, xk2, xv2 = dev(xptr2, torch), dev(xkey2, torch), dev(xval2, torch)
+    dY2h = dYh[:, :5].copy()
+    dxval2 = torch.empty(len(xkey2), device="cuda")
+    dvals2 = torch.empty(A.nnz, device="cuda")
+    with torch.cuda.stream(s):
+        h.spmspv_batched_backward(xp2, xk2, xv2, 1.0, dev(dY2h, torch), dxval2, dvals2)
+    s.synchronize()
+    h.check_device_error()
+    dx, dxm, dv, dvm = _refs(A, xptr2, xkey2, xval2, dY2h, 1.0)
+    assert _close(dxval2.cpu().numpy(), dx, dxm)
+    assert _close(dvals2.cpu().numpy(), dv, dvm)
