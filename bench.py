@@ -202,6 +202,8 @@ def ref_host_libs():
     P = ctypes.c_void_p
     h.ref_serialspmv.argtypes = [ctypes.c_int] * 3 + [P] * 5 + [ctypes.c_float]
     h.ref_serialspmv.restype = None
+    h.ref_serialspmv_slices.argtypes = [ctypes.c_int, P] + [ctypes.c_int] * 3 + [P] * 5 + [ctypes.c_float]
+    h.ref_serialspmv_slices.restype = None
     c.ref_spmspv_csc_host.argtypes = [ctypes.c_int] * 3 + [P] * 3 + [ctypes.c_int] + [P] * 5
     c.ref_spmspv_csc_host.restype = None
     return h, c
@@ -285,7 +287,6 @@ def run_reference(args, world, rank):
     kernels rebuilt for sm_100a on the same sweep."""
     if rank != 0:
         return 0
-    from concurrent.futures import ThreadPoolExecutor
     import oracle.oracle as orc
     A, xs = make_inputs_oracle()
     colptr, row, cval = A.to_csc()
@@ -297,19 +298,16 @@ def run_reference(args, world, rank):
     tot_bytes = sum(eff_bytes(m, n, nnz, len(k), b) for (_, k, _), b in zip(xs, binl))
     dense = [orc.sparse2dense_bits(n, k, v)[0] for _, k, v in xs]
     libs = ref_host_libs()
-    pool = ThreadPoolExecutor(max_workers=threads)
-    slices = row_slices(A.rowptr, 4 * threads)  # 4 per thread: a finer split balances better
-    rp_addr = A.rowptr.ctypes.data
+    slices = row_slices(A.rowptr, 8 * threads)  # several per thread: dynamic scheduling balances
+    bounds = np.array([a for a, _ in slices] + [slices[-1][1]], np.int32)
 
     def dense_leg(xd):
         if libs is None:
             orc.raw.cpu_spmv_omp(m, P(A.rowptr), P(A.col), P(A.val), P(xd), P(y), 1.0)
             return
-        host = libs[0]
-        # ctypes releases the GIL for the call: the slices run in parallel
-        list(pool.map(lambda r: host.ref_serialspmv(r[1] - r[0], n, nnz, rp_addr + 4 * r[0], P(A.col),
-                                                     P(A.val), P(xd), y.ctypes.data + 4 * r[0], 1.0),
-                      slices))
+        # the reference's serialspmv on each slice, an OpenMP loop over the slices
+        libs[0].ref_serialspmv_slices(len(slices), P(bounds), m, n, nnz, P(A.rowptr), P(A.col), P(A.val),
+                                      P(xd), P(y), 1.0)
 
     def step():
         t = 0.0
@@ -326,11 +324,11 @@ def run_reference(args, world, rank):
     for _ in range(args.warmup):
         step()
     ts = [step() for _ in range(args.steps)]
-    pool.shutdown()
     sec = sum(ts) / len(ts)
     gbs = tot_bytes / sec / 1e9
-    dense_what = ("the reference's own serialspmv (oracle/_ref) over %d nnz-balanced row slices on "
-                  "%d host threads" % (len(slices), threads)) if libs else "the oracle's serialspmv, OpenMP"
+    dense_what = ("the reference's own serialspmv (oracle/_ref) over %d nnz-balanced row slices, an "
+                  "OpenMP loop on %d host threads" % (len(slices), threads)) if libs else \
+        "the oracle's serialspmv, OpenMP"
     line = {"metric": METRIC, "value": gbs, "unit": "GB/s", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": sec * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
@@ -755,7 +753,7 @@ def run_batched_spmspv(torch, dev, stream, args):
     from spmx import gen
     import oracle.oracle as orc
     nvec = 256
-    A = gen.chung_lu(1 << 22, 2.1, 32.0, seed=5)
+    A = gen.chung_lu(1 << args.batched_log2n, 2.1, 32.0, seed=5)
     m, n = A.m, A.n
     rng = np.random.default_rng(5)
     sizes = np.exp(rng.uniform(np.log(10), np.log(100000), nvec)).astype(np.int64)
@@ -876,7 +874,7 @@ def run_batched_spmspv(torch, dev, stream, args):
     fwd_b = 12 * xn + 4 * (m + 1) + 8 * A.nnz + 4 * nvec * m
     bwd_b = 12 * xn + 2 * (4 * (m + 1) + 8 * A.nnz) + 4 * nvec * m + 4 * A.nnz + 4 * xn
     h.Destroy()
-    return {"matrix": "chung-lu n 4,194,304, exponent 2.1, average degree 32, seed 5",
+    return {"matrix": "chung-lu n %s, exponent 2.1, average degree 32, seed 5" % format(m, ","),
             "nnz": int(A.nnz), "nvec": nvec, "x_nnz_total": xn, "products": bins,
             "graph_fwd_bwd_ms": mb, "plain256_fwd_bwd_ms": mp, "speedup": mp / mb,
             "eff_gbs": (fwd_b + bwd_b) / (mb * 1e-3) / 1e9, "forward_within_1e-5": bool(ok),
@@ -1230,6 +1228,16 @@ def run_only(args):
         print(json.dumps(run_powerlaw(torch, dev, stream, args)))
         return 0
     A, xs = make_inputs()
+    if args.matrix != "zipf1m":
+        # the same x densities on a power-law matrix (SpMV kernels profile the dense x)
+        from spmx import gen
+        if args.matrix == "chunglu1m":
+            A = gen.chung_lu(1 << 20, 2.1, 32.0, seed=5)
+        else:
+            A = gen.rmat(20, 16, seed=1)
+            A.val = np.random.default_rng(7).uniform(-1, 1, A.nnz).astype(np.float32)
+        xs = [(dd, *gen.sparse_vector(A.n, gen.density_nnz(A.n, dd), dist="uniform",
+                                       seed=1000 + gen.density_nnz(A.n, dd))) for dd in DENSITIES]
     d = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)  # noqa: E731
     rp, cl, vl = d(A.rowptr), d(A.col), d(A.val)
     h = spmx.SpmspvHandle(A.m, A.n, A.nnz, stream=stream)
@@ -1297,6 +1305,11 @@ def main():
                          "whose serialised timings would mislead the tuner) reuses the first run's choices")
     ap.add_argument("--only", choices=ONLY, help="run one kernel (profiling helper)")
     ap.add_argument("--density", type=float, default=0.1)
+    ap.add_argument("--batched-log2n", type=int, default=22,
+                    help="log2 of the Chung-Lu size of the batched SpMSpV line (22 = the benchmark's; "
+                         "smaller for profiling)")
+    ap.add_argument("--matrix", default="zipf1m", choices=["zipf1m", "chunglu1m", "rmat20"],
+                    help="with --only: the matrix (the benchmark's Zipf matrix by default)")
     args = ap.parse_args()
     if args.only:
         return run_only(args)

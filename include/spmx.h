@@ -461,10 +461,10 @@ int spmx_spmspv_batched_backward(spmx_handle_t h, int nvec, int x_total, const i
 /* No reference counterpart.  Options of the batched entry points (flags,
  * default 0):
  *   SPMX_BATCH_REUSE_INVERSION: a backward call on the same batch (the same
- *     xptr / xkey pointers, nvec and x_total) as the handle's last forward
- *     call reuses that call's inversion of the batch instead of sorting it
- *     again.  The caller promises that xptr and xkey were not changed in
- *     between.
+ *     xptr / xkey / xval pointers, nvec and x_total) as the handle's last
+ *     forward call reuses that call's inversion of the batch instead of
+ *     sorting it again.  The caller promises that xptr, xkey and xval were not
+ *     changed in between.
  *   SPMX_BATCH_FUSED_DXVAL: when a backward call asks for both dxval and
  *     dvals, dxval is accumulated during the dvals pass (which holds dY's rows
  *     in shared memory) with atomic adds, instead of a separate pass over the

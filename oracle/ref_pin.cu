@@ -18,6 +18,19 @@ extern "C" void ref_serialspmv(int m, int n, int nnz, int* rowptr, int* col, flo
   serialspmv(m, n, nnz, rowptr, col, val, x, y, alpha);
 }
 
+// The reference's serialspmv on all OpenMP threads: rows are independent, so
+// each slice [r0, r1) of `nslices` nnz-balanced slices (bounds[0..nslices])
+// runs the reference routine on its own rows (bit-identical y).
+extern "C" void ref_serialspmv_slices(int nslices, const int* bounds, int m, int n, int nnz, int* rowptr,
+                                      int* col, float* val, float* x, float* y, float alpha) {
+#pragma omp parallel for schedule(dynamic, 1)
+  for (int q = 0; q < nslices; ++q) {
+    const int r0 = bounds[q], r1 = bounds[q + 1];
+    if (r1 > r0) serialspmv(r1 - r0, n, nnz, rowptr + r0, col, val, x, y + r0, alpha);
+  }
+  (void)m;
+}
+
 extern "C" void ref_mat_features(int m, int n, int nnz, int* rowptr, float* out7) {
   SpmspvHandle<int, unsigned, float> A(m, n, nnz);
   int mx = 0, mn = 0;

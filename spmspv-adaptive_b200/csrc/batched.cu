@@ -13,7 +13,8 @@
 //
 // Design: the batch is inverted once per call (a stable radix sort of the
 // entries by column gives, per column, the (vector, entry) pairs that use
-// it), then
+// it; each pair is then stored as one 8-byte record of its vector and its x
+// value, so a row walk reads one sector per pair), then
 //   forward  - one warp per row of A (CSR): lanes take the row's nonzeros,
 //              look up their columns' pairs and add a[k] * x into a shared
 //              row of nvec accumulators; the warp then stores the row of Y
@@ -28,6 +29,7 @@
 // one call outside stream capture (which sizes the scratch for x_total) both
 // entry points can be captured in a CUDA graph.
 #include <algorithm>
+#include <cstdint>
 #include <string>
 
 #include "common.cuh"
@@ -73,13 +75,20 @@ __global__ void batch_bounds_kernel(int total, const unsigned* __restrict__ skey
   invptr[j] = lo;
 }
 
+// rec[p] = (vector, x value bits) of sorted pair p
+__global__ void batch_rec_kernel(int total, const unsigned* __restrict__ inv_ent,
+                                 const unsigned* __restrict__ inv_vec, const float* __restrict__ xval,
+                                 int2* __restrict__ rec) {
+  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < total; p += gridDim.x * blockDim.x)
+    rec[p] = make_int2((int)__ldg(inv_vec + p), __float_as_int(__ldg(xval + __ldg(inv_ent + p))));
+}
+
 // Y[i][:] = alpha * sum_k A[i][k] * X[col_k][:], one warp per row
 __global__ void __launch_bounds__(kBatchWarps * 32)
 batch_forward_kernel(int m, int n, int nvec, const int* __restrict__ rowptr, const int* __restrict__ col,
                      const float* __restrict__ val, const int* __restrict__ invptr,
-                     const unsigned* __restrict__ inv_ent, const unsigned* __restrict__ inv_vec,
-                     const float* __restrict__ xval, float alpha, float* __restrict__ Y, int* err) {
-  extern __shared__ float s_acc[];  // kBatchWarps rows of nvec
+                     const int2* __restrict__ rec, float alpha, float* __restrict__ Y, int vec4, int* err) {
+  extern __shared__ __align__(16) float s_acc[];  // kBatchWarps rows of nvec
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   float* acc = s_acc + warp * nvec;
   for (int v = lane; v < nvec; v += 32) acc[v] = 0.f;
@@ -95,11 +104,24 @@ batch_forward_kernel(int m, int n, int nvec, const int* __restrict__ rowptr, con
       }
       const float a = __ldg(val + k);
       const int p1 = __ldg(invptr + j + 1);
-      for (int p = __ldg(invptr + j); p < p1; ++p)
-        atomicAdd(acc + __ldg(inv_vec + p), a * __ldg(xval + __ldg(inv_ent + p)));
+      for (int p = __ldg(invptr + j); p < p1; ++p) {
+        const int2 e = __ldg(rec + p);
+        atomicAdd(acc + e.x, a * __int_as_float(e.y));
+      }
     }
     __syncwarp();
     float* yr = Y + (long long)i * nvec;
+    if (vec4) {  // nvec % 4 == 0 and Y 16-byte aligned (checked on the host): vector stores
+      float4* y4 = reinterpret_cast<float4*>(yr);
+      float4* a4 = reinterpret_cast<float4*>(acc);
+      for (int v = lane; v < (nvec >> 2); v += 32) {
+        const float4 t = a4[v];
+        y4[v] = make_float4(alpha * t.x, alpha * t.y, alpha * t.z, alpha * t.w);
+        a4[v] = make_float4(0.f, 0.f, 0.f, 0.f);
+      }
+      __syncwarp();
+      continue;
+    }
     for (int v = lane; v < nvec; v += 32) {
       yr[v] = alpha * acc[v];
       acc[v] = 0.f;
@@ -115,10 +137,10 @@ batch_forward_kernel(int m, int n, int nvec, const int* __restrict__ rowptr, con
 __global__ void __launch_bounds__(kBatchWarps * 32)
 batch_dvals_kernel(int m, int n, int nvec, const int* __restrict__ rowptr, const int* __restrict__ col,
                    const int* __restrict__ invptr, const unsigned* __restrict__ inv_ent,
-                   const unsigned* __restrict__ inv_vec, const float* __restrict__ xval, float alpha,
+                   const int2* __restrict__ rec, float alpha,
                    const float* __restrict__ dY, float* __restrict__ dvals, const float* __restrict__ val,
-                   float* __restrict__ dxval, int* err) {
-  extern __shared__ float s_dy[];
+                   float* __restrict__ dxval, int vec4, int* err) {
+  extern __shared__ __align__(16) float s_dy[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   float* g = s_dy + warp * nvec;
   const int nw = gridDim.x * kBatchWarps;
@@ -126,7 +148,12 @@ batch_dvals_kernel(int m, int n, int nvec, const int* __restrict__ rowptr, const
     const int a0 = __ldg(rowptr + i), a1 = __ldg(rowptr + i + 1);
     if (a0 == a1) continue;  // warp-uniform
     const float* dyr = dY + (long long)i * nvec;
-    for (int v = lane; v < nvec; v += 32) g[v] = __ldg(dyr + v);
+    if (vec4) {  // nvec % 4 == 0 and dY 16-byte aligned (checked on the host)
+      for (int v = lane; v < (nvec >> 2); v += 32)
+        reinterpret_cast<float4*>(g)[v] = __ldg(reinterpret_cast<const float4*>(dyr) + v);
+    } else {
+      for (int v = lane; v < nvec; v += 32) g[v] = __ldg(dyr + v);
+    }
     __syncwarp();
     for (int k = a0 + lane; k < a1; k += 32) {
       const int j = __ldg(col + k);
@@ -135,10 +162,10 @@ batch_dvals_kernel(int m, int n, int nvec, const int* __restrict__ rowptr, const
         const int p1 = __ldg(invptr + j + 1);
         const float a = dxval ? alpha * __ldg(val + k) : 0.f;
         for (int p = __ldg(invptr + j); p < p1; ++p) {
-          const unsigned e = __ldg(inv_ent + p);
-          const float gv = g[__ldg(inv_vec + p)];
-          s += __ldg(xval + e) * gv;
-          if (dxval) atomicAdd(dxval + e, a * gv);
+          const int2 r = __ldg(rec + p);
+          const float gv = g[r.x];
+          s += __int_as_float(r.y) * gv;
+          if (dxval) atomicAdd(dxval + __ldg(inv_ent + p), a * gv);
         }
       } else {
         flag_error(err, kDevErrOob);
@@ -199,6 +226,8 @@ static int ensure_batch_scratch(spmx_handle_t h, int total) {
   dfree(h->batch_hist);
   dfree(h->batch_hoff);
   dfree(h->batch_invptr);
+  dfree(h->batch_rec);
+  h->batch_rec = nullptr;
   h->batch_hist = h->batch_hoff = h->batch_invptr = nullptr;
   h->batch_cap = 0;
   const char* what[6] = {"batch keys", "batch keys alt", "batch entries", "batch entries alt",
@@ -208,13 +237,14 @@ static int ensure_batch_scratch(spmx_handle_t h, int total) {
   SPMX_TRY(dalloc((void**)&h->batch_hist, 4 * hn, "batch hist"));
   SPMX_TRY(dalloc((void**)&h->batch_hoff, 4 * hn, "batch hist off"));
   SPMX_TRY(dalloc((void**)&h->batch_invptr, 4 * ((size_t)h->n + 1), "batch inverse pointers"));
+  SPMX_TRY(dalloc(&h->batch_rec, 8 * (size_t)cap, "batch pair records"));
   h->batch_cap = cap;
   h->batch_invptr_n = h->n;
   return SPMX_SUCCESS;
 }
 
 static void batch_forget_inversion(spmx_handle_t h) {
-  h->inv_xptr = h->inv_xkey = nullptr;
+  h->inv_xptr = h->inv_xkey = h->inv_xval = nullptr;
   h->inv_nvec = h->inv_total = -1;
   h->inv_ent = h->inv_vec = nullptr;
 }
@@ -223,11 +253,12 @@ static void batch_forget_inversion(spmx_handle_t h) {
 // A forward call records which batch the inversion belongs to; a backward
 // call with SPMX_BATCH_REUSE_INVERSION set reuses it for the same batch.
 static int batch_invert(spmx_handle_t h, int nvec, int total, const int* xptr, const int* xkey,
-                        bool forward, const unsigned** inv_ent, const unsigned** inv_vec) {
+                        const float* xval, bool forward, const unsigned** inv_ent, const int2** rec) {
   if (!forward && (h->batch_opts & SPMX_BATCH_REUSE_INVERSION) && h->inv_ent && h->inv_xptr == xptr &&
-      h->inv_xkey == xkey && h->inv_nvec == nvec && h->inv_total == total && h->batch_invptr_n == h->n) {
+      h->inv_xkey == xkey && h->inv_xval == xval && h->inv_nvec == nvec && h->inv_total == total &&
+      h->batch_invptr_n == h->n) {
     *inv_ent = h->inv_ent;
-    *inv_vec = h->inv_vec;
+    *rec = (const int2*)h->batch_rec;
     return SPMX_SUCCESS;
   }
   batch_forget_inversion(h);
@@ -246,16 +277,23 @@ static int batch_invert(spmx_handle_t h, int nvec, int total, const int* xptr, c
     return set_error(SPMX_ERR_INVALID_VALUE, "batch sort capacity");
   const unsigned* skey = rb.result_in_alt ? b[1] : b[0];
   *inv_ent = rb.result_in_alt ? b[3] : b[2];
-  *inv_vec = rb.result_in_alt ? b[5] : b[4];
+  const unsigned* inv_vec = rb.result_in_alt ? b[5] : b[4];
   note_launch();
   batch_bounds_kernel<<<(h->n + 1 + 255) / 256, 256, 0, st>>>(total, skey, h->n, h->batch_invptr);
+  if (total > 0) {
+    note_launch();
+    batch_rec_kernel<<<std::min((total + 255) / 256, h->num_sms * 8), 256, 0, st>>>(
+        total, *inv_ent, inv_vec, xval, (int2*)h->batch_rec);
+  }
+  *rec = (const int2*)h->batch_rec;
   if (forward) {
     h->inv_xptr = xptr;
     h->inv_xkey = xkey;
+    h->inv_xval = xval;
     h->inv_nvec = nvec;
     h->inv_total = total;
     h->inv_ent = *inv_ent;
-    h->inv_vec = *inv_vec;
+    h->inv_vec = inv_vec;
   }
   return SPMX_SUCCESS;
 }
@@ -287,16 +325,18 @@ extern "C" int spmx_spmspv_batched(spmx_handle_t h, int nvec, int x_total, const
   SPMX_TRY(batched_common(h, nvec, x_total, d_xptr));
   if (!d_Y && h->m > 0) return set_error(SPMX_ERR_INVALID_VALUE, "Y is NULL");
   if (x_total > 0 && (!d_xkey || !d_xval)) return set_error(SPMX_ERR_INVALID_VALUE, "NULL batch arrays");
-  const unsigned *ie = nullptr, *iv = nullptr;
-  SPMX_TRY(batch_invert(h, nvec, x_total, d_xptr, d_xkey, true, &ie, &iv));
+  const unsigned* ie = nullptr;
+  const int2* rec = nullptr;
+  SPMX_TRY(batch_invert(h, nvec, x_total, d_xptr, d_xkey, d_xval, true, &ie, &rec));
   if (h->m == 0) return SPMX_SUCCESS;
   const size_t smem = 4 * (size_t)kBatchWarps * nvec;
   if (smem > 48 * 1024)
     cudaFuncSetAttribute(batch_forward_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   note_launch();
   batch_forward_kernel<<<batch_rows_grid(h, (const void*)batch_forward_kernel, smem), kBatchWarps * 32, smem,
-                         h->stream>>>(h->m, h->n, nvec, h->rowptr, h->col, h->val, h->batch_invptr, ie, iv,
-                                      d_xval, alpha, d_Y, h->d_err);
+                         h->stream>>>(h->m, h->n, nvec, h->rowptr, h->col, h->val, h->batch_invptr, rec,
+                                      alpha, d_Y, (nvec % 4 == 0 && ((uintptr_t)d_Y & 15u) == 0) ? 1 : 0,
+                                      h->d_err);
   return launch_ok("batched spmspv");
 }
 
@@ -312,15 +352,17 @@ extern "C" int spmx_spmspv_batched_backward(spmx_handle_t h, int nvec, int x_tot
   const bool fused = (h->batch_opts & SPMX_BATCH_FUSED_DXVAL) && d_dxval && d_dvals && h->nnz > 0 && x_total > 0;
   if (fused) SPMX_CUDA(cudaMemsetAsync(d_dxval, 0, 4 * (size_t)x_total, st));
   if (d_dvals && h->nnz > 0) {
-    const unsigned *ie = nullptr, *iv = nullptr;
-    SPMX_TRY(batch_invert(h, nvec, x_total, d_xptr, d_xkey, false, &ie, &iv));
+    const unsigned* ie = nullptr;
+    const int2* rec = nullptr;
+    SPMX_TRY(batch_invert(h, nvec, x_total, d_xptr, d_xkey, d_xval, false, &ie, &rec));
     const size_t smem = 4 * (size_t)kBatchWarps * nvec;
     if (smem > 48 * 1024)
       cudaFuncSetAttribute(batch_dvals_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     note_launch();
     batch_dvals_kernel<<<batch_rows_grid(h, (const void*)batch_dvals_kernel, smem), kBatchWarps * 32, smem,
-                         st>>>(h->m, h->n, nvec, h->rowptr, h->col, h->batch_invptr, ie, iv, d_xval, alpha,
-                               d_dY, d_dvals, h->val, fused ? d_dxval : nullptr, h->d_err);
+                         st>>>(h->m, h->n, nvec, h->rowptr, h->col, h->batch_invptr, ie, rec, alpha,
+                               d_dY, d_dvals, h->val, fused ? d_dxval : nullptr,
+                               (nvec % 4 == 0 && ((uintptr_t)d_dY & 15u) == 0) ? 1 : 0, h->d_err);
   }
   if (d_dxval && x_total > 0 && !fused) {
     if (!h->has_csc || !h->csc_val)

@@ -211,7 +211,7 @@ extern "C" int spmx_destroy(spmx_handle_t h) {
   dfree(h->ms_q0); dfree(h->ms_q1); dfree(h->ms_srcs); dfree(h->ms_tmp); dfree(h->ms_ctrl);
   dfree(h->ms_hchunk); dfree(h->ms_hcnt); dfree(h->ms_hacc); dfree(h->ms_hleft); dfree(h->ms_hcounters);
   for (void* p : h->batch_buf) dfree(p);
-  dfree(h->batch_hist); dfree(h->batch_hoff); dfree(h->batch_invptr);
+  dfree(h->batch_hist); dfree(h->batch_hoff); dfree(h->batch_invptr); dfree(h->batch_rec);
   delete h;
   return SPMX_SUCCESS;
 }

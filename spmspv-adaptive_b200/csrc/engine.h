@@ -133,8 +133,10 @@ struct spmx_handle_s {
   const void* inv_xptr = nullptr;
   const void* inv_xkey = nullptr;
   int inv_nvec = -1, inv_total = -1;
+  const void* inv_xval = nullptr;
   const unsigned* inv_ent = nullptr;
   const unsigned* inv_vec = nullptr;
+  void* batch_rec = nullptr;  // per inverted pair: (vector, x value bits)
   // hub chunks of the multi-source pull (built once per matrix)
   int4* ms_hchunk = nullptr;
   int* ms_hcnt = nullptr;

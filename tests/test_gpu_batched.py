@@ -252,3 +252,31 @@ def test_batched_options_reuse_and_fused(torch_cuda, problem, graph):
     dx, dxm, dv, dvm = _refs(A, xptr2, xkey2, xval2, dY2h, 1.0)
     assert _close(dxval2.cpu().numpy(), dx, dxm)
     assert _close(dvals2.cpu().numpy(), dv, dvm)
+
+
+def test_batched_unaligned_outputs(torch_cuda, problem):
+    """Y and dY that start 4 bytes past a 16-byte boundary take the scalar
+    row stores / loads (nvec is a multiple of 4 here)."""
+    torch = torch_cuda
+    A, xptr, xkey, xval = problem
+    nvec = len(xptr) - 1
+    assert nvec % 4 == 0
+    h = make_handle(A, torch, hola=False)
+    xp, xk, xv = dev(xptr, torch), dev(xkey, torch), dev(xval, torch)
+    Ybuf = torch.full((A.m * nvec + 1,), 5.0, device="cuda")
+    Y = Ybuf[1:].view(A.m, nvec)
+    assert Y.data_ptr() % 16 == 4
+    h.spmspv_batched(xp, xk, xv, 1.0, Y)
+    h.check_device_error()
+    _check_forward(A, xptr, xkey, xval, Y.cpu().numpy(), 1.0)
+    dYh = np.random.default_rng(13).standard_normal((A.m, nvec)).astype(np.float32)
+    dYbuf = torch.empty(A.m * nvec + 1, device="cuda")
+    dYbuf[1:].copy_(torch.from_numpy(dYh.ravel()))
+    dY = dYbuf[1:].view(A.m, nvec)
+    dxval = torch.empty(len(xkey), device="cuda")
+    dvals = torch.empty(A.nnz, device="cuda")
+    h.spmspv_batched_backward(xp, xk, xv, 1.0, dY, dxval, dvals)
+    h.check_device_error()
+    dx, dxm, dv, dvm = _refs(A, xptr, xkey, xval, dYh, 1.0)
+    assert _close(dxval.cpu().numpy(), dx, dxm)
+    assert _close(dvals.cpu().numpy(), dv, dvm)
