@@ -479,6 +479,21 @@ def run_ours(args, world, rank, local):
     if os.path.exists(tp):
         with open(tp) as f:
             traffic = json.load(f).get(f"{kname}_spmv_zipf1m")
+    # what the chosen back-end's own format costs: a rebuild, timed on the
+    # host around a synchronised call, and the bytes of its stream
+    backend_cost = None
+    if kname == "round":
+        info0 = h.round_info()
+        torch.cuda.synchronize(dev)
+        t0 = time.perf_counter()
+        h.roundPreprocess(0, info0["parts"])
+        torch.cuda.synchronize(dev)
+        prep_ms = (time.perf_counter() - t0) * 1e3
+        info1 = h.round_info()
+        fmt_bytes = info1["rounds"] * 4096 * 8 + info1["rounds"] * 32 * 4 + 4 * (m + 1)
+        backend_cost = {"preprocess_ms": prep_ms, "format_bytes": fmt_bytes,
+                        "csr_bytes": 4 * (m + 1) + 8 * nnz,
+                        "spmv_calls_to_amortise": prep_ms / k_ms}
 
     # --- correctness of the sweep (rank 0): each density's y against the FP64
     # oracle with the parity tests' magnitude-scaled bound, plus the raw
@@ -618,6 +633,7 @@ def run_ours(args, world, rank, local):
                                        "std": float(np.std(np.diff(A.rowptr)))},
                        "spmv_backend": kname,
                        "parallelism": f"replicas x{world}" if world > 1 else "single"},
+            "spmv_backend_cost": backend_cost,
             "roofline": {"bound": "hbm", "kernel": f"{kname} SpMV (autotuned back-end), dense x",
                          "achieved": achieved, "peak": peak, "peak_kind": peak_kind,
                          "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,

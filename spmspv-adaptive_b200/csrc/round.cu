@@ -498,7 +498,7 @@ extern "C" int spmx_round_postprocess(spmx_handle_t h) {
 // (then a build with pad = true starts a new chunk at every 2^16-column
 // segment, which bounds every chunk's span)
 static int round_build(spmx_handle_t h, long long rcap, long long avail, int parts, bool inplace, bool pad,
-                       bool* overflow, bool* span) {
+                       int waves, bool* overflow, bool* span) {
   constexpr int E = kRoundE;
   spmx_round_postprocess(h);
   const int m = h->m, n = h->n, nnz = h->nnz;
@@ -510,26 +510,42 @@ static int round_build(spmx_handle_t h, long long rcap, long long avail, int par
   cudaStreamSynchronize(st);
   // row blocks: one wave of 2-CTA clusters when the rows fit, about equal
   // nonzero counts, boundaries on multiples of 4, at most rcap rows each
+  // row blocks: one wave of 2-CTA clusters (times `waves`) when the rows fit,
+  // about equal nonzero counts, boundaries on multiples of 4, at most rcap rows
+  // each.  Where the row cap makes some blocks take far more nonzeros than
+  // others (a power-law matrix: its many short rows fill blocks by rows, so
+  // the hub rows crowd into the first blocks), the block count doubles (more
+  // waves) until the largest block holds at most 1.3 times the mean.
   const long long need = std::max<long long>(1, (m + rcap - 1) / rcap);
-  int nrb = (int)std::max<long long>(need, std::min<long long>(h->num_sms / parts, std::max(1, m / 4)));
+  const long long max_blocks = std::max(1, m / 4);
+  int nrb = (int)std::max<long long>(need, std::min<long long>((long long)(h->num_sms / parts) * waves, max_blocks));
   nrb = std::max(1, nrb);
+  std::vector<int> rbr;
+  for (;;) {
+    rbr.assign((size_t)nrb + 1, 0);
+    rbr[nrb] = m;
+    for (int k = 1; k < nrb; ++k) {
+      const long long want_nz = (long long)nnz * k / nrb;
+      long long r = std::lower_bound(rp.begin(), rp.end(), (int)want_nz) - rp.begin();
+      r = (r + 2) & ~3LL;
+      const long long lo = std::max<long long>(rbr[k - 1], (long long)m - (long long)(nrb - k) * rcap);
+      const long long hi = std::min<long long>((long long)rbr[k - 1] + rcap, m);
+      r = std::max(r, (lo + 3) & ~3LL);
+      r = std::min(r, hi & ~3LL);
+      r = std::max<long long>(r, rbr[k - 1]);
+      rbr[k] = (int)r;
+    }
+    long long big = 0;
+    for (int k = 0; k < nrb; ++k) big = std::max<long long>(big, (long long)rp[rbr[k + 1]] - rp[rbr[k]]);
+    const double mean = (double)nnz / nrb;
+    if (nnz == 0 || (double)big <= 1.3 * mean || 2LL * nrb > max_blocks || nrb >= 16 * (h->num_sms / parts))
+      break;
+    nrb *= 2;
+  }
   const int cbits = bits_for((long long)std::max(n, 1));
   const int bbits = bits_for((long long)nrb + 1);
   if (cbits + bbits > 32)
     return set_error(SPMX_ERR_INVALID_VALUE, "round SpMV: row blocks x columns exceed a 32-bit sort key");
-  std::vector<int> rbr((size_t)nrb + 1, 0);
-  rbr[nrb] = m;
-  for (int k = 1; k < nrb; ++k) {
-    const long long want_nz = (long long)nnz * k / nrb;
-    long long r = std::lower_bound(rp.begin(), rp.end(), (int)want_nz) - rp.begin();
-    r = (r + 2) & ~3LL;
-    const long long lo = std::max<long long>(rbr[k - 1], (long long)m - (long long)(nrb - k) * rcap);
-    const long long hi = std::min<long long>((long long)rbr[k - 1] + rcap, m);
-    r = std::max(r, (lo + 3) & ~3LL);
-    r = std::min(r, hi & ~3LL);
-    r = std::max<long long>(r, rbr[k - 1]);
-    rbr[k] = (int)r;
-  }
   int rmax = 4;
   for (int k = 0; k < nrb; ++k) rmax = std::max(rmax, rbr[k + 1] - rbr[k]);
   if (rmax > rcap) return set_error(SPMX_ERR_INVALID_VALUE, "round SpMV: row blocks do not fit shared memory");
@@ -817,16 +833,24 @@ static int round_preprocess(spmx_handle_t h, int rb_rows, int parts) {
   long long rcap = std::min<long long>((avail / (inplace ? 4 : 8)) & ~3LL, 65532);
   if (rb_rows > 0) rcap = std::min<long long>(rcap, std::max(4, (rb_rows + 3) & ~3));
   if (rcap < 4) return set_error(SPMX_ERR_INVALID_VALUE, "round SpMV: no shared memory left for y");
+  // When the slots of some row block overflow, first take twice as many row
+  // blocks (shorter in nonzeros, so fewer slots each; up to 4 times the
+  // blocks), then shrink the row cap.
   bool pad = false;
+  int waves = 1;
   for (int attempt = 0;; ++attempt) {
     bool overflow = false, span = false;
-    const int rc = round_build(h, rcap, avail, parts, inplace, pad, &overflow, &span);
+    const int rc = round_build(h, rcap, avail, parts, inplace, pad, waves, &overflow, &span);
     if (rc == SPMX_SUCCESS) return rc;
     if (span && !pad) {
       pad = true;
       continue;
     }
-    if (!overflow || attempt >= (inplace ? 12 : 6) || rcap <= 64) return rc;
+    if (!overflow || attempt >= (inplace ? 14 : 8) || rcap <= 64) return rc;
+    if (waves < 4) {
+      waves *= 2;
+      continue;
+    }
     rcap = std::max<long long>(64, (inplace ? rcap * 85 / 100 : rcap / 2) & ~3LL);
   }
 }
