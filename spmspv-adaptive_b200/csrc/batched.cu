@@ -83,6 +83,37 @@ __global__ void batch_rec_kernel(int total, const unsigned* __restrict__ inv_ent
     rec[p] = make_int2((int)__ldg(inv_vec + p), __float_as_int(__ldg(xval + __ldg(inv_ent + p))));
 }
 
+// Software pipeline of the row walks.  A warp takes rows i, i + nw, i + 2nw,
+// ...; while it works on row i it already holds row i + nw's bounds and the
+// lane's first (column, value) of that row, and row i + 2nw's bounds are in
+// flight.  Only the pair-range and pair-record loads stay on the critical
+// path of a row.
+struct BatchRowHead {
+  int a0, a1;  // row bounds
+  int j;       // the lane's first column (a0 + lane), valid if has
+  float a;     // its value (forward) or unused
+  bool has;
+};
+
+__device__ __forceinline__ void batch_row_bounds(const int* __restrict__ rowptr, int m, long long i, int& a0,
+                                                 int& a1) {
+  a0 = a1 = 0;
+  if (i < m) {
+    a0 = __ldg(rowptr + i);
+    a1 = __ldg(rowptr + i + 1);
+  }
+}
+
+__device__ __forceinline__ BatchRowHead batch_row_head(const int* __restrict__ col, const float* __restrict__ val,
+                                                       int a0, int a1, int lane) {
+  BatchRowHead h{a0, a1, 0, 0.f, a0 + lane < a1};
+  if (h.has) {
+    h.j = __ldg(col + a0 + lane);
+    if (val) h.a = __ldg(val + a0 + lane);
+  }
+  return h;
+}
+
 // Y[i][:] = alpha * sum_k A[i][k] * X[col_k][:], one warp per row
 __global__ void __launch_bounds__(kBatchWarps * 32)
 batch_forward_kernel(int m, int n, int nvec, const int* __restrict__ rowptr, const int* __restrict__ col,
@@ -93,24 +124,47 @@ batch_forward_kernel(int m, int n, int nvec, const int* __restrict__ rowptr, con
   float* acc = s_acc + warp * nvec;
   for (int v = lane; v < nvec; v += 32) acc[v] = 0.f;
   __syncwarp();
-  const int nw = gridDim.x * kBatchWarps;
-  for (int i = blockIdx.x * kBatchWarps + warp; i < m; i += nw) {
-    const int a0 = __ldg(rowptr + i), a1 = __ldg(rowptr + i + 1);
-    for (int k = a0 + lane; k < a1; k += 32) {
+  const long long nw = (long long)gridDim.x * kBatchWarps;
+  long long i = (long long)blockIdx.x * kBatchWarps + warp;
+  int b0, b1;
+  batch_row_bounds(rowptr, m, i, b0, b1);
+  BatchRowHead cur = batch_row_head(col, val, b0, b1, lane);
+  batch_row_bounds(rowptr, m, i + nw, b0, b1);  // the next row's bounds
+  for (; i < m; i += nw) {
+    // the pair range of the lane's first nonzero of this row
+    int p0 = 0, p1 = 0;
+    if (cur.has) {
+      if ((unsigned)cur.j < (unsigned)n) {
+        p0 = __ldg(invptr + cur.j);
+        p1 = __ldg(invptr + cur.j + 1);
+      } else {
+        flag_error(err, kDevErrOob);
+      }
+    }
+    // in flight meanwhile: the next row's first (column, value), the bounds after it
+    const BatchRowHead nxt = batch_row_head(col, val, b0, b1, lane);
+    int c0, c1;
+    batch_row_bounds(rowptr, m, i + 2 * nw, c0, c1);
+    for (int p = p0; p < p1; ++p) {
+      const int2 e = __ldg(rec + p);
+      atomicAdd(acc + e.x, cur.a * __int_as_float(e.y));
+    }
+    // the row's nonzeros past the first 32
+    for (int k = cur.a0 + 32 + lane; k < cur.a1; k += 32) {
       const int j = __ldg(col + k);
       if ((unsigned)j >= (unsigned)n) {
         flag_error(err, kDevErrOob);
         continue;
       }
       const float a = __ldg(val + k);
-      const int p1 = __ldg(invptr + j + 1);
-      for (int p = __ldg(invptr + j); p < p1; ++p) {
+      const int q1 = __ldg(invptr + j + 1);
+      for (int p = __ldg(invptr + j); p < q1; ++p) {
         const int2 e = __ldg(rec + p);
         atomicAdd(acc + e.x, a * __int_as_float(e.y));
       }
     }
     __syncwarp();
-    float* yr = Y + (long long)i * nvec;
+    float* yr = Y + i * nvec;
     if (vec4) {  // nvec % 4 == 0 and Y 16-byte aligned (checked on the host): vector stores
       float4* y4 = reinterpret_cast<float4*>(yr);
       float4* a4 = reinterpret_cast<float4*>(acc);
@@ -119,21 +173,25 @@ batch_forward_kernel(int m, int n, int nvec, const int* __restrict__ rowptr, con
         y4[v] = make_float4(alpha * t.x, alpha * t.y, alpha * t.z, alpha * t.w);
         a4[v] = make_float4(0.f, 0.f, 0.f, 0.f);
       }
-      __syncwarp();
-      continue;
-    }
-    for (int v = lane; v < nvec; v += 32) {
-      yr[v] = alpha * acc[v];
-      acc[v] = 0.f;
+    } else {
+      for (int v = lane; v < nvec; v += 32) {
+        yr[v] = alpha * acc[v];
+        acc[v] = 0.f;
+      }
     }
     __syncwarp();
+    cur = nxt;
+    b0 = c0;
+    b1 = c1;
   }
 }
 
 // dvals[k] = alpha * sum over column col_k's pairs of xval[e] * dY[i][v(e)],
 // one warp per row with dY's row in shared memory.  With dxval (fused form,
 // dxval zeroed before) every pair also adds alpha * a[k] * dY[i][v(e)] into
-// dxval[e] with an atomic add.
+// dxval[e] with an atomic add.  The same pipeline as the forward; for
+// nvec <= 256 with 16-byte rows the next row of dY is also loaded into
+// registers (two float4 per lane) while this row is walked.
 __global__ void __launch_bounds__(kBatchWarps * 32)
 batch_dvals_kernel(int m, int n, int nvec, const int* __restrict__ rowptr, const int* __restrict__ col,
                    const int* __restrict__ invptr, const unsigned* __restrict__ inv_ent,
@@ -143,36 +201,68 @@ batch_dvals_kernel(int m, int n, int nvec, const int* __restrict__ rowptr, const
   extern __shared__ __align__(16) float s_dy[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   float* g = s_dy + warp * nvec;
-  const int nw = gridDim.x * kBatchWarps;
-  for (int i = blockIdx.x * kBatchWarps + warp; i < m; i += nw) {
-    const int a0 = __ldg(rowptr + i), a1 = __ldg(rowptr + i + 1);
-    if (a0 == a1) continue;  // warp-uniform
-    const float* dyr = dY + (long long)i * nvec;
-    if (vec4) {  // nvec % 4 == 0 and dY 16-byte aligned (checked on the host)
-      for (int v = lane; v < (nvec >> 2); v += 32)
-        reinterpret_cast<float4*>(g)[v] = __ldg(reinterpret_cast<const float4*>(dyr) + v);
-    } else {
-      for (int v = lane; v < nvec; v += 32) g[v] = __ldg(dyr + v);
+  const bool pre = vec4 && nvec <= 256;  // the next dY row fits two float4 per lane
+  const int n4 = nvec >> 2;
+  const long long nw = (long long)gridDim.x * kBatchWarps;
+  long long i = (long long)blockIdx.x * kBatchWarps + warp;
+  const float* aval = dxval ? val : nullptr;
+  int b0, b1;
+  batch_row_bounds(rowptr, m, i, b0, b1);
+  BatchRowHead cur = batch_row_head(col, aval, b0, b1, lane);
+  float4 gcur[2] = {make_float4(0.f, 0.f, 0.f, 0.f), make_float4(0.f, 0.f, 0.f, 0.f)};
+  if (pre && i < m && b0 < b1) {
+    const float4* d4 = reinterpret_cast<const float4*>(dY + i * nvec);
+    if (lane < n4) gcur[0] = __ldg(d4 + lane);
+    if (lane + 32 < n4) gcur[1] = __ldg(d4 + lane + 32);
+  }
+  batch_row_bounds(rowptr, m, i + nw, b0, b1);
+  for (; i < m; i += nw) {
+    // in flight meanwhile: the next row's head and dY row, the bounds after it
+    const BatchRowHead nxt = batch_row_head(col, aval, b0, b1, lane);
+    float4 gnxt[2] = {make_float4(0.f, 0.f, 0.f, 0.f), make_float4(0.f, 0.f, 0.f, 0.f)};
+    if (pre && i + nw < m && b0 < b1) {
+      const float4* d4 = reinterpret_cast<const float4*>(dY + (i + nw) * nvec);
+      if (lane < n4) gnxt[0] = __ldg(d4 + lane);
+      if (lane + 32 < n4) gnxt[1] = __ldg(d4 + lane + 32);
     }
-    __syncwarp();
-    for (int k = a0 + lane; k < a1; k += 32) {
-      const int j = __ldg(col + k);
-      float s = 0.f;
-      if ((unsigned)j < (unsigned)n) {
-        const int p1 = __ldg(invptr + j + 1);
-        const float a = dxval ? alpha * __ldg(val + k) : 0.f;
-        for (int p = __ldg(invptr + j); p < p1; ++p) {
-          const int2 r = __ldg(rec + p);
-          const float gv = g[r.x];
-          s += __int_as_float(r.y) * gv;
-          if (dxval) atomicAdd(dxval + __ldg(inv_ent + p), a * gv);
-        }
+    int c0, c1;
+    batch_row_bounds(rowptr, m, i + 2 * nw, c0, c1);
+    if (cur.a0 < cur.a1) {  // warp-uniform
+      if (pre) {
+        if (lane < n4) reinterpret_cast<float4*>(g)[lane] = gcur[0];
+        if (lane + 32 < n4) reinterpret_cast<float4*>(g)[lane + 32] = gcur[1];
+      } else if (vec4) {
+        const float4* d4 = reinterpret_cast<const float4*>(dY + i * nvec);
+        for (int v = lane; v < n4; v += 32) reinterpret_cast<float4*>(g)[v] = __ldg(d4 + v);
       } else {
-        flag_error(err, kDevErrOob);
+        for (int v = lane; v < nvec; v += 32) g[v] = __ldg(dY + i * nvec + v);
       }
-      dvals[k] = alpha * s;
+      __syncwarp();
+      for (int k = cur.a0 + lane; k < cur.a1; k += 32) {
+        const bool first = k == cur.a0 + lane;
+        const int j = first ? cur.j : __ldg(col + k);
+        float s = 0.f;
+        if ((unsigned)j < (unsigned)n) {
+          const int q1 = __ldg(invptr + j + 1);
+          const float a = dxval ? alpha * (first ? cur.a : __ldg(val + k)) : 0.f;
+          for (int p = __ldg(invptr + j); p < q1; ++p) {
+            const int2 r = __ldg(rec + p);
+            const float gv = g[r.x];
+            s += __int_as_float(r.y) * gv;
+            if (dxval) atomicAdd(dxval + __ldg(inv_ent + p), a * gv);
+          }
+        } else {
+          flag_error(err, kDevErrOob);
+        }
+        dvals[k] = alpha * s;
+      }
+      __syncwarp();
     }
-    __syncwarp();
+    cur = nxt;
+    gcur[0] = gnxt[0];
+    gcur[1] = gnxt[1];
+    b0 = c0;
+    b1 = c1;
   }
 }
 
