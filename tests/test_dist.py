@@ -59,3 +59,25 @@ def test_allmax_over_ranks():
         assert p.exitcode == 0
     got = dict(q.get(timeout=10) for _ in range(2))
     assert got == {0: 3.0, 1: 3.0}
+
+
+def test_reference_arm_loads_no_product_code(tmp_path):
+    """The reference arm builds its inputs with the oracle and times the
+    reference's own routines: the product package and libspmx.so stay
+    unloaded in that process."""
+    probe = tmp_path / "run_ref.py"
+    probe.write_text(
+        "import runpy, sys\n"
+        f"sys.argv = ['bench.py', '--impl', 'reference', '--steps', '1', '--warmup', '0', '--no-ref-gpu']\n"
+        f"sys.path.insert(0, {ROOT!r})\n"
+        "try:\n"
+        f"    runpy.run_path({os.path.join(ROOT, 'bench.py')!r}, run_name='__main__')\n"
+        "except SystemExit:\n"
+        "    pass\n"
+        "maps = open('/proc/self/maps').read()\n"
+        "print('PRODUCT_LOADED' if ('spmx' in sys.modules or 'libspmx' in maps) else 'PRODUCT_NOT_LOADED')\n")
+    r = subprocess.run([sys.executable, str(probe)], cwd=ROOT, capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr[-2000:]
+    assert "PRODUCT_NOT_LOADED" in r.stdout, r.stdout[-500:]
+    line = [ln for ln in r.stdout.splitlines() if ln.startswith("{")][-1]
+    assert json.loads(line)["impl"] == "reference"
