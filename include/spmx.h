@@ -235,8 +235,10 @@ int spmx_tiledspmspv(spmx_handle_t h, float alpha, float* d_y);
  * starting a new 128-entry chunk. */
 int spmx_round_preprocess(spmx_handle_t h, int rb_rows);
 /* No reference counterpart.  The round format with `parts` CTAs per row
- * block: 2 (what spmx_round_preprocess builds: one 2-CTA cluster per row
- * block) or 4 (two clusters per row block, each row block twice as tall, the
+ * block: 1 (row blocks half as tall, one CTA each over all columns, no
+ * cluster: each row's accumulators are summed straight into y), 2 (what
+ * spmx_round_preprocess builds: one 2-CTA cluster per row block) or 4 (two
+ * clusters per row block, each row block twice as tall, the
  * row sums folded into each row's first accumulator slot; the two clusters'
  * sums meet in a small device buffer and the second to finish a row slice
  * stores y, so every row is still added in a fixed order).  Taller row blocks
@@ -245,7 +247,7 @@ int spmx_round_preprocess(spmx_handle_t h, int rb_rows);
 int spmx_round_preprocess_parts(spmx_handle_t h, int rb_rows, int parts);
 int spmx_round_postprocess(spmx_handle_t h);
 /* geometry chosen by spmx_round_preprocess(_parts): info[0..7] = row blocks,
- * CTAs per row block (2 or 4; clusters are always 2 CTAs), rounds, nonzeros
+ * CTAs per row block (1, 2 or 4; clusters, where used, are 2 CTAs), rounds, nonzeros
  * per round, accumulator slots per CTA, rows per row block (at most), shared
  * bytes, grid */
 int spmx_round_info(spmx_handle_t h, int* info);

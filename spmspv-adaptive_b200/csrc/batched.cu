@@ -84,14 +84,19 @@ __global__ void batch_rec_kernel(int total, const unsigned* __restrict__ inv_ent
 }
 
 // Software pipeline of the row walks.  A warp takes rows i, i + nw, i + 2nw,
-// ...; while it works on row i it already holds row i + nw's bounds and the
-// lane's first (column, value) of that row, and row i + 2nw's bounds are in
-// flight.  Only the pair-range and pair-record loads stay on the critical
-// path of a row.
+// ...  In the forward, while it works on row i it already holds row i + nw's
+// head (bounds, the lane's first column and value) with that column's pair
+// range in flight, row i + 2nw's head in flight and row i + 3nw's bounds in
+// flight, so only the pair-record loads stay on the critical path of a row's
+// first 32 nonzeros.  The dvals walk, which also holds the next row of dY in
+// registers, runs one row shallower (row i + nw's head, row i + 2nw's
+// bounds): the deeper form needs 64 registers there and loses more to the
+// lower occupancy than it gains.
 struct BatchRowHead {
   int a0, a1;  // row bounds
   int j;       // the lane's first column (a0 + lane), valid if has
   float a;     // its value (forward) or unused
+  int p0, p1;  // the column's pair range, once looked up
   bool has;
 };
 
@@ -106,12 +111,40 @@ __device__ __forceinline__ void batch_row_bounds(const int* __restrict__ rowptr,
 
 __device__ __forceinline__ BatchRowHead batch_row_head(const int* __restrict__ col, const float* __restrict__ val,
                                                        int a0, int a1, int lane) {
-  BatchRowHead h{a0, a1, 0, 0.f, a0 + lane < a1};
+  BatchRowHead h{a0, a1, 0, 0.f, 0, 0, a0 + lane < a1};
   if (h.has) {
     h.j = __ldg(col + a0 + lane);
     if (val) h.a = __ldg(val + a0 + lane);
   }
   return h;
+}
+
+// the pair range of the head's column (empty for a lane without a nonzero or
+// an out-of-range column, which is flagged)
+__device__ __forceinline__ void batch_head_pairs(BatchRowHead& h, const int* __restrict__ invptr, int n, int* err) {
+  h.p0 = h.p1 = 0;
+  if (h.has) {
+    if ((unsigned)h.j < (unsigned)n) {
+      h.p0 = __ldg(invptr + h.j);
+      h.p1 = __ldg(invptr + h.j + 1);
+    } else {
+      flag_error(err, kDevErrOob);
+    }
+  }
+}
+
+// acc[v] += a * x over the pairs [p0, p1), two records in flight at a time
+__device__ __forceinline__ void batch_add_pairs(float* acc, const int2* __restrict__ rec, int p0, int p1, float a) {
+  int p = p0;
+  for (; p + 1 < p1; p += 2) {
+    const int2 e = __ldg(rec + p), f = __ldg(rec + p + 1);
+    atomicAdd(acc + e.x, a * __int_as_float(e.y));
+    atomicAdd(acc + f.x, a * __int_as_float(f.y));
+  }
+  if (p < p1) {
+    const int2 e = __ldg(rec + p);
+    atomicAdd(acc + e.x, a * __int_as_float(e.y));
+  }
 }
 
 // Y[i][:] = alpha * sum_k A[i][k] * X[col_k][:], one warp per row
@@ -129,39 +162,28 @@ batch_forward_kernel(int m, int n, int nvec, const int* __restrict__ rowptr, con
   int b0, b1;
   batch_row_bounds(rowptr, m, i, b0, b1);
   BatchRowHead cur = batch_row_head(col, val, b0, b1, lane);
-  batch_row_bounds(rowptr, m, i + nw, b0, b1);  // the next row's bounds
+  batch_row_bounds(rowptr, m, i + nw, b0, b1);
+  BatchRowHead nxt = batch_row_head(col, val, b0, b1, lane);
+  batch_head_pairs(cur, invptr, n, err);
+  batch_row_bounds(rowptr, m, i + 2 * nw, b0, b1);  // row i + 2nw's bounds
   for (; i < m; i += nw) {
-    // the pair range of the lane's first nonzero of this row
-    int p0 = 0, p1 = 0;
-    if (cur.has) {
-      if ((unsigned)cur.j < (unsigned)n) {
-        p0 = __ldg(invptr + cur.j);
-        p1 = __ldg(invptr + cur.j + 1);
-      } else {
-        flag_error(err, kDevErrOob);
-      }
-    }
-    // in flight meanwhile: the next row's first (column, value), the bounds after it
-    const BatchRowHead nxt = batch_row_head(col, val, b0, b1, lane);
+    // in flight meanwhile: row i + nw's pair range, row i + 2nw's head, the bounds after it
+    batch_head_pairs(nxt, invptr, n, err);
+    const BatchRowHead nn = batch_row_head(col, val, b0, b1, lane);
     int c0, c1;
-    batch_row_bounds(rowptr, m, i + 2 * nw, c0, c1);
-    for (int p = p0; p < p1; ++p) {
-      const int2 e = __ldg(rec + p);
-      atomicAdd(acc + e.x, cur.a * __int_as_float(e.y));
-    }
-    // the row's nonzeros past the first 32
-    for (int k = cur.a0 + 32 + lane; k < cur.a1; k += 32) {
-      const int j = __ldg(col + k);
-      if ((unsigned)j >= (unsigned)n) {
-        flag_error(err, kDevErrOob);
-        continue;
-      }
-      const float a = __ldg(val + k);
-      const int q1 = __ldg(invptr + j + 1);
-      for (int p = __ldg(invptr + j); p < q1; ++p) {
-        const int2 e = __ldg(rec + p);
-        atomicAdd(acc + e.x, a * __int_as_float(e.y));
-      }
+    batch_row_bounds(rowptr, m, i + 3 * nw, c0, c1);
+    batch_add_pairs(acc, rec, cur.p0, cur.p1, cur.a);
+    // the row's nonzeros past the first 32, two per lane at a time
+    for (int k = cur.a0 + 32 + lane; k < cur.a1; k += 64) {
+      const bool two = k + 32 < cur.a1;
+      const int j0 = __ldg(col + k), j1 = two ? __ldg(col + k + 32) : 0;
+      const float v0 = __ldg(val + k), v1 = two ? __ldg(val + k + 32) : 0.f;
+      const bool ok0 = (unsigned)j0 < (unsigned)n, ok1 = two && (unsigned)j1 < (unsigned)n;
+      if (!ok0 || (two && !ok1)) flag_error(err, kDevErrOob);
+      const int q00 = ok0 ? __ldg(invptr + j0) : 0, q01 = ok0 ? __ldg(invptr + j0 + 1) : 0;
+      const int q10 = ok1 ? __ldg(invptr + j1) : 0, q11 = ok1 ? __ldg(invptr + j1 + 1) : 0;
+      batch_add_pairs(acc, rec, q00, q01, v0);
+      batch_add_pairs(acc, rec, q10, q11, v1);
     }
     __syncwarp();
     float* yr = Y + i * nvec;
@@ -181,6 +203,7 @@ batch_forward_kernel(int m, int n, int nvec, const int* __restrict__ rowptr, con
     }
     __syncwarp();
     cur = nxt;
+    nxt = nn;
     b0 = c0;
     b1 = c1;
   }

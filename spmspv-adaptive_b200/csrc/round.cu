@@ -62,12 +62,12 @@ constexpr int kRoundParamCtas = 296;
 struct RoundGeom {
   int use;
   int cta_round[kRoundParamCtas + 1];
-  int rb_row[kRoundParamCtas / kRoundCS + 1];
+  int rb_row[kRoundParamCtas + 1];
 };
 
 struct RoundTables {
   int nrb = 0, grid = 0, rmax = 0, nrounds = 0, nslots = 0;
-  int parts = kRoundCS;           // CTAs per row block: one cluster, or two (then psum / pcnt)
+  int parts = kRoundCS;           // CTAs per row block: one, one cluster, or two (then psum / pcnt)
   bool inplace = false;           // row sums folded into each row's first slot
   float* psum = nullptr;          // parts > 2: each cluster's row sums, [parts / 2][m]
   unsigned* pcnt = nullptr;       // parts > 2: arrivals per (row block, row slice)
@@ -91,9 +91,10 @@ size_t round_smem(int nslots, int rmax, bool inplace) {
   return 4 * (size_t)(((nslots + 3) & ~3) + (inplace ? 0 : rmax));
 }
 
-// parts CTAs per row block, in clusters of 2; with parts = 4 each cluster
-// adds its two CTAs' row sums and the two clusters meet in psum: the second
-// to arrive at a row slice writes y (no waiting, a fixed order of addition).
+// parts CTAs per row block: one CTA, whose row sums are y (no cluster); or
+// clusters of 2, with parts = 4 two of them, in which case each cluster adds
+// its two CTAs' row sums and the two clusters meet in psum: the second to
+// arrive at a row slice writes y (no waiting, a fixed order of addition).
 template <bool GATED, bool INPLACE>
 __global__ void __launch_bounds__(kRoundNW * 32, 1)
 round_spmv_kernel(const __grid_constant__ RoundGeom geom, int nslots, int parts, const int* __restrict__ rb_row,
@@ -194,11 +195,13 @@ round_spmv_kernel(const __grid_constant__ RoundGeom geom, int nslots, int parts,
       if (r < rows) {
         float acc = 0.f;
         for (int s = lo[j] - base0; s < hi[j] - base0; ++s) acc += ys[s];
-        if (!INPLACE) F[r] = acc;
+        if (parts == 1) y[row0 + r] = alpha * acc;  // one CTA per row block: its row sums are y
+        else if (!INPLACE) F[r] = acc;
         else if (hi[j] > lo[j]) ys[lo[j] - base0] = acc;  // rows own disjoint slots
       }
     }
   }
+  if (parts == 1) return;
   // the cluster's row sums, added in rank order; each CTA takes a slice
   cg::cluster_group cl = cg::this_cluster();
   cl.sync();
@@ -508,9 +511,7 @@ static int round_build(spmx_handle_t h, long long rcap, long long avail, int par
       cudaMemcpyAsync(rp.data(), h->rowptr, 4 * ((size_t)m + 1), cudaMemcpyDeviceToHost, st) != cudaSuccess)
     return set_error(SPMX_ERR_CUDA, "round SpMV: row pointer copy");
   cudaStreamSynchronize(st);
-  // row blocks: one wave of 2-CTA clusters when the rows fit, about equal
-  // nonzero counts, boundaries on multiples of 4, at most rcap rows each
-  // row blocks: one wave of 2-CTA clusters (times `waves`) when the rows fit,
+  // row blocks: one wave of CTAs (times `waves`) when the rows fit,
   // about equal nonzero counts, boundaries on multiples of 4, at most rcap rows
   // each.  Where the row cap makes some blocks take far more nonzeros than
   // others (a power-law matrix: its many short rows fill blocks by rows, so
@@ -621,8 +622,8 @@ static int round_build(spmx_handle_t h, long long rcap, long long avail, int par
   }
   cudaError_t se = cudaStreamSynchronize(st);
   if (!rc && se != cudaSuccess) rc = set_error(SPMX_ERR_CUDA, std::string("round SpMV: ") + cudaGetErrorString(se));
-  // rounds (host): each row block's sorted nonzeros split in two halves of
-  // whole rounds, one per CTA of the cluster, each cut into rounds of E
+  // rounds (host): each row block's sorted nonzeros split in `parts` runs of
+  // whole rounds, one per CTA of the row block, each cut into rounds of E
   // stream positions.  With pad, a half's stream places every segment at a
   // multiple of the chunk length (a segment's last chunk is padded), and the
   // rounds are cut on that padded stream; a round then holds the real entries
@@ -756,7 +757,7 @@ static int round_build(spmx_handle_t h, long long rcap, long long avail, int par
     if (!rc) {
       for (int k = 0; k < nrb; ++k) nslots_real = std::max(nslots_real, bslots[k]);
       t->nslots = nslots_real + kRoundDummy;
-      t->smem = round_smem(t->nslots, rmax, inplace);
+      t->smem = round_smem(t->nslots, rmax, inplace || parts == 1);
       if (t->nslots >= 65536 || (long long)t->smem > avail) {
         *overflow = true;
         rc = set_error(SPMX_ERR_INVALID_VALUE,
@@ -812,6 +813,8 @@ static int round_build(spmx_handle_t h, long long rcap, long long avail, int par
   return SPMX_SUCCESS;
 }
 
+// parts = 1: one CTA per row block (no cluster), its row sums stored as y
+// straight from the slots (rows <= avail / 4);
 // parts = 2: one 2-CTA cluster per row block, row sums in their own shared
 // array (rows <= avail / 8), row blocks halved while the slots overflow;
 // parts = 4: two clusters per row block over twice as many rows, the row sums
@@ -824,13 +827,14 @@ static int round_preprocess(spmx_handle_t h, int rb_rows, int parts) {
   if (!h->has_csr || (!h->val && h->nnz > 0))
     return set_error(SPMX_ERR_NOT_READY, "round SpMV needs the CSR input with values");
   if (rb_rows < 0) return set_error(SPMX_ERR_INVALID_VALUE, "round SpMV: rb_rows must be >= 0");
-  if (parts != 2 && parts != 4) return set_error(SPMX_ERR_INVALID_VALUE, "round SpMV: parts must be 2 or 4");
+  if (parts != 1 && parts != 2 && parts != 4)
+    return set_error(SPMX_ERR_INVALID_VALUE, "round SpMV: parts must be 1, 2 or 4");
   int optin = 0;
   cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, h->device);
   const long long avail = (long long)optin - round_static_smem();
   const bool inplace = parts > 2;
-  // every nonempty row needs a slot (and, unless folded, a row sum)
-  long long rcap = std::min<long long>((avail / (inplace ? 4 : 8)) & ~3LL, 65532);
+  // every nonempty row needs a slot (and, unless folded or stored as y, a row sum)
+  long long rcap = std::min<long long>((avail / (inplace || parts == 1 ? 4 : 8)) & ~3LL, 65532);
   if (rb_rows > 0) rcap = std::min<long long>(rcap, std::max(4, (rb_rows + 3) & ~3));
   if (rcap < 4) return set_error(SPMX_ERR_INVALID_VALUE, "round SpMV: no shared memory left for y");
   // When the slots of some row block overflow, first take twice as many row
@@ -846,12 +850,12 @@ static int round_preprocess(spmx_handle_t h, int rb_rows, int parts) {
       pad = true;
       continue;
     }
-    if (!overflow || attempt >= (inplace ? 14 : 8) || rcap <= 64) return rc;
+    if (!overflow || attempt >= (inplace || parts == 1 ? 14 : 8) || rcap <= 64) return rc;
     if (waves < 4) {
       waves *= 2;
       continue;
     }
-    rcap = std::max<long long>(64, (inplace ? rcap * 85 / 100 : rcap / 2) & ~3LL);
+    rcap = std::max<long long>(64, (inplace || parts == 1 ? rcap * 85 / 100 : rcap / 2) & ~3LL);
   }
 }
 
@@ -870,7 +874,7 @@ static cudaError_t round_launch(spmx_handle_t h, RoundTables* t, float alpha, fl
   cfg.stream = h->stream;
   cudaLaunchAttribute at[2];
   at[0].id = cudaLaunchAttributeClusterDimension;
-  at[0].val.clusterDim.x = kRoundCS;
+  at[0].val.clusterDim.x = t->parts == 1 ? 1 : kRoundCS;
   at[0].val.clusterDim.y = 1;
   at[0].val.clusterDim.z = 1;
   at[1].id = cudaLaunchAttributeProgrammaticStreamSerialization;

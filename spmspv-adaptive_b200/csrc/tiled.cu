@@ -51,7 +51,6 @@ namespace spmx {
 
 constexpr int kTileBuf = 3;                  // stages in flight per CTA
 constexpr unsigned kPadEntry = 0xffffffffu;  // packed word of a padding entry
-constexpr long long kBarSpinLimit = 1LL << 22;
 constexpr int kTilePrefetch = 12;            // stages between L2 prefetch and bulk copy
 
 struct TileStage {
@@ -66,57 +65,6 @@ struct TileGeom {
   int chunk;  // entry capacity of a stage buffer (multiple of 4)
   int rmax;   // shared y entries (multiple of 4)
 };
-
-__device__ __forceinline__ unsigned smem_addr(const void* p) {
-  return (unsigned)__cvta_generic_to_shared(p);
-}
-
-__device__ __forceinline__ void bar_init(unsigned long long* b, int count) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(b)), "r"(count) : "memory");
-}
-
-__device__ __forceinline__ void bar_arrive(unsigned long long* b) {
-  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(b)) : "memory");
-}
-
-__device__ __forceinline__ void bar_arrive_tx(unsigned long long* b, unsigned bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(b)), "r"(bytes)
-               : "memory");
-}
-
-// waits for the phase of parity `parity` to complete; false after the limit
-// or once another warp has raised the abort flag
-__device__ __forceinline__ bool bar_wait(unsigned long long* b, int parity, const volatile int* abort) {
-  for (long long it = 0; it < kBarSpinLimit; ++it) {
-    unsigned done;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-        "selp.u32 %0, 1, 0, p;\n\t}"
-        : "=r"(done)
-        : "r"(smem_addr(b)), "r"(parity)
-        : "memory");
-    if (done) return true;
-    if ((it & 255) == 255 && *abort) return false;
-  }
-  return false;
-}
-
-// one bulk copy global -> this CTA's shared memory, counted on barrier b;
-// dst, src and bytes are multiples of 16
-__device__ __forceinline__ void bulk_load(void* dst, const void* src, unsigned bytes,
-                                          unsigned long long* b) {
-  asm volatile(
-      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-          smem_addr(dst)),
-      "l"(src), "r"(bytes), "r"(smem_addr(b))
-      : "memory");
-}
-
-// hint: bring `bytes` at src into L2 ahead of a later bulk copy
-__device__ __forceinline__ void l2_prefetch(const void* src, unsigned bytes) {
-  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(src), "r"(bytes) : "memory");
-}
 
 // Shared memory layout (dynamic): full[NB] and empty[NB] barriers, then per
 // buffer the x window (win floats), the bitmap window (win/32 words), packed

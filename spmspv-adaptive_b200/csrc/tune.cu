@@ -122,7 +122,7 @@ static int apply_params(spmx_handle_t h, const Params& p) {
     rc = spmx_tiled_preprocess(h, p.tiled_rb, p.tiled_win, 0, 0);
   } else if (p.spmv_type == SPMX_SPMV_ROUND) {
     // for the round back-end the window field holds the CTAs per row block
-    rc = spmx_round_preprocess_parts(h, p.tiled_rb, p.tiled_win == 4 ? 4 : 2);
+    rc = spmx_round_preprocess_parts(h, p.tiled_rb, p.tiled_win == 1 || p.tiled_win == 4 ? p.tiled_win : 2);
   }
   return rc;
 }
@@ -208,9 +208,9 @@ extern "C" int spmx_autotune(spmx_handle_t h, const char* cache_path, int* spmv_
       }
       spmx_tiled_postprocess(h);
     }
-    // round back-end with 2 or 4 CTAs per row block (a build that does not
-    // fit shared memory is skipped)
-    for (int parts : {2, 4}) {
+    // round back-end with 1, 2 or 4 CTAs per row block (a build that does
+    // not fit shared memory is skipped)
+    for (int parts : {1, 2, 4}) {
       if (spmx_round_preprocess_parts(h, 0, parts) != SPMX_SUCCESS) continue;
       const float t = time_us([&] { return spmx_roundspmv(h, 1.0f, y); });
       if (t < best_t) {

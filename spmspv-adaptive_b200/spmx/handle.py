@@ -264,8 +264,9 @@ class SpmspvHandle:
         check(lib.spmx_tiledspmspv(self._h, float(alpha), _f32(y)), "tiledspmspv")
 
     def roundPreprocess(self, rb_rows=0, parts=2):
-        """Round format with `parts` CTAs per row block (2, or 4: two clusters
-        over row blocks twice as tall)."""
+        """Round format with `parts` CTAs per row block (2; 1: one CTA per row
+        block, row blocks half as tall, no cluster; or 4: two clusters over
+        row blocks twice as tall)."""
         if parts == 2:
             check(lib.spmx_round_preprocess(self._h, int(rb_rows)), "roundPreprocess")
         else:

@@ -68,7 +68,7 @@ def _check_spmv(torch, h, A, alpha, x):
 
 @pytest.mark.parametrize("name,A", ALL, ids=[c[0] for c in ALL])
 @pytest.mark.parametrize("rb", [0, 64])
-@pytest.mark.parametrize("parts", [2, 4])
+@pytest.mark.parametrize("parts", [1, 2, 4])
 def test_round_spmv(torch_cuda, name, A, rb, parts):
     torch = torch_cuda
     h = make_handle(A, torch, csc=False, hola=False)
@@ -108,7 +108,7 @@ def test_round_spmv(torch_cuda, name, A, rb, parts):
     h.roundPostprocess()
 
 
-@pytest.mark.parametrize("parts", [2, 4])
+@pytest.mark.parametrize("parts", [1, 2, 4])
 def test_round_zipf_full_size(torch_cuda, parts):
     torch = torch_cuda
     from spmx import gen
