@@ -516,7 +516,10 @@ static int round_build(spmx_handle_t h, long long rcap, long long avail, int par
   // each.  Where the row cap makes some blocks take far more nonzeros than
   // others (a power-law matrix: its many short rows fill blocks by rows, so
   // the hub rows crowd into the first blocks), the block count doubles (more
-  // waves) until the largest block holds at most 1.3 times the mean.
+  // waves) until the largest block holds at most 1.3 times the mean, or until
+  // its CTAs' share is at most 3/4 of what one SM takes of the whole matrix
+  // (then it no longer sets the time; a single hub row can keep a block above
+  // 1.3 times the mean however many blocks there are).
   const long long need = std::max<long long>(1, (m + rcap - 1) / rcap);
   const long long max_blocks = std::max(1, m / 4);
   int nrb = (int)std::max<long long>(need, std::min<long long>((long long)(h->num_sms / parts) * waves, max_blocks));
@@ -539,7 +542,8 @@ static int round_build(spmx_handle_t h, long long rcap, long long avail, int par
     long long big = 0;
     for (int k = 0; k < nrb; ++k) big = std::max<long long>(big, (long long)rp[rbr[k + 1]] - rp[rbr[k]]);
     const double mean = (double)nnz / nrb;
-    if (nnz == 0 || (double)big <= 1.3 * mean || 2LL * nrb > max_blocks || nrb >= 16 * (h->num_sms / parts))
+    if (nnz == 0 || (double)big <= 1.3 * mean || (double)big / parts <= 0.75 * (double)nnz / h->num_sms ||
+        2LL * nrb > max_blocks || nrb >= 16 * (h->num_sms / parts))
       break;
     nrb *= 2;
   }
