@@ -491,7 +491,7 @@ def run_ours(args, world, rank, local):
         prep_ms = (time.perf_counter() - t0) * 1e3
         info1 = h.round_info()
         fmt_bytes = info1["rounds"] * 4096 * 8 + info1["rounds"] * 32 * 4 + 4 * (m + 1)
-        backend_cost = {"preprocess_ms": prep_ms, "format_bytes": fmt_bytes,
+        backend_cost = {"preprocess_ms": prep_ms, "format_bytes": fmt_bytes, "geometry": info1,
                         "csr_bytes": 4 * (m + 1) + 8 * nnz,
                         "spmv_calls_to_amortise": prep_ms / k_ms}
 
@@ -516,8 +516,8 @@ def run_ours(args, world, rank, local):
 
     # --- e2e through the public API with host buffers, one step = the sweep.
     # Every x is copied from pinned host memory on a copy stream (all six
-    # uploads back to back); each adaptive call waits for its own x only, so
-    # the later uploads overlap the earlier calls.  The result of each call is
+    # uploads back to back, largest first); each adaptive call waits for its
+    # own x only, so the later uploads overlap the earlier calls.  The result of each call is
     # read back without a host round trip: for a sparse x the nonzeros of y,
     # compacted straight into pinned host memory with their count
     # (spmx_dense2sparse_to_host), for the dense x the dense y.  One stream
@@ -538,17 +538,21 @@ def run_ours(args, world, rank, local):
     ev_in = [torch.cuda.Event() for _ in xs]
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
 
+    # the six calls are independent: the largest x goes first, so that its
+    # result's read-back overlaps the uploads and calls of the smaller ones
+    order = sorted(range(len(xs)), key=lambda i: -len(xs[i][1]))
+
     def e2e_step(check=False):
         flush.fill_(2.0)
         e0.record(stream)
         copy_stream.wait_event(e0)
         with torch.cuda.stream(copy_stream):
-            for i in range(len(xs)):
+            for i in order:
                 k = len(xs[i][1])
                 kbufs[i][:k].copy_(pin_k[i], non_blocking=True)
                 vbufs[i][:k].copy_(pin_v[i], non_blocking=True)
                 ev_in[i].record(copy_stream)
-        for i in range(len(xs)):
+        for i in order:
             stream.wait_event(ev_in[i])
             h.set_sparse_x(kbufs[i], vbufs[i], len(xs[i][1]))
             h.run_adaptive(1.0, y)
@@ -579,6 +583,39 @@ def run_ours(args, world, rank, local):
     d2h = sum(d2h_calls)
     e2e_val = world * total_bytes / (e2e_ms * 1e-3) / 1e9
     e2e_step(check=True)  # untimed: the host-side results against the FP64 oracle
+
+    # The PCIe share of e2e: the same bytes moved by copies alone, the uploads
+    # on the copy stream and the read-backs (one per array the step returns)
+    # on the compute stream, so that both directions run at once.
+    ynz_last = [int(ycnt_h[i]) if sparse_out[i] else m for i in range(len(xs))]
+
+    def copies_step():
+        flush.fill_(2.0)
+        e0.record(stream)
+        copy_stream.wait_event(e0)
+        with torch.cuda.stream(copy_stream):
+            for i in range(len(xs)):
+                k = len(xs[i][1])
+                kbufs[i][:k].copy_(pin_k[i], non_blocking=True)
+                vbufs[i][:k].copy_(pin_v[i], non_blocking=True)
+            ev_in[0].record(copy_stream)
+        for i in range(len(xs)):
+            nz = ynz_last[i]
+            if sparse_out[i]:
+                ycnt_h[i:i + 1].copy_(ycnt_d[i:i + 1], non_blocking=True)
+                ykey_h[i][:nz].copy_(y[:nz].view(torch.int32), non_blocking=True)
+                yval_h[i][:nz].copy_(y[:nz], non_blocking=True)
+            else:
+                yhost.copy_(y, non_blocking=True)
+        stream.wait_event(ev_in[0])
+        e1.record(stream)
+        stream.synchronize()
+        return e0.elapsed_time(e1)
+
+    ycnt_d = torch.zeros(len(xs), dtype=torch.int32, device=dev)
+    for _ in range(3):
+        copies_step()
+    copies_ms = allmax(statistics.mean([copies_step() for _ in range(args.steps)]), world)
 
     # --- the selector against exhaustive timing of all eight kernels (rank 0,
     # after the last collective) ---
@@ -640,6 +677,7 @@ def run_ours(args, world, rank, local):
                          "bytes_per_launch": sb, "ms_per_launch": k_ms},
             "e2e": {"value": e2e_val, "unit": "GB/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms,
+                    "copies_only_ms": copies_ms,
                     "host_results_within_1e-5": bool(e2e_ok) and all(e2e_ok)},
             "gpu_launches": int(launches),
             "gpu_launches_per_step": int(launches_per_step),
@@ -1262,7 +1300,7 @@ def run_only(args):
     h.holaPreprocess()
     h.CSR5Preprocess()
     h.tiledPreprocess()
-    h.roundPreprocess()
+    h.roundPreprocess(0, args.round_parts)
     h.allocPreBuffer()
     dens = 1.0 if args.only.endswith("spmv") else args.density
     k = [x for x in xs if abs(x[0] - dens) < 1e-12][0]
@@ -1321,6 +1359,8 @@ def main():
                          "whose serialised timings would mislead the tuner) reuses the first run's choices")
     ap.add_argument("--only", choices=ONLY, help="run one kernel (profiling helper)")
     ap.add_argument("--density", type=float, default=0.1)
+    ap.add_argument("--round-parts", type=int, default=1, choices=[1, 2, 4],
+                    help="--only round-spmv: CTAs per row block of the round format")
     ap.add_argument("--batched-log2n", type=int, default=22,
                     help="log2 of the Chung-Lu size of the batched SpMSpV line (22 = the benchmark's; "
                          "smaller for profiling)")
