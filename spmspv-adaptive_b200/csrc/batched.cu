@@ -41,6 +41,15 @@ namespace spmx {
 
 constexpr int kBatchWarps = 8;      // warps per CTA in the row kernels
 constexpr int kBatchMaxVec = 1024;  // nvec limit (shared row accumulators)
+// Row chunks of the row walks: a row weighs its nonzeros plus kBatchRowCost
+// (the fixed cost of a row: its Y row store and its latency chain); chunk k
+// holds the rows whose prefix weight rowptr[i] + kBatchRowCost * i starts in
+// [k * kBatchChunk, (k + 1) * kBatchChunk).  Warps take chunks in order from
+// a device counter, so the heavy rows (of a power-law matrix numbered by
+// weight, the first ones) spread over the warps instead of landing one per
+// warp in the first pass of a cyclic assignment.
+constexpr int kBatchChunk = 2048;
+constexpr int kBatchRowCost = 32;
 
 // sort keys (column) and payloads (entry, vector) of every batch entry
 __global__ void batch_keys_kernel(int n, int nvec, int total, const int* __restrict__ xptr,
@@ -75,6 +84,54 @@ __global__ void batch_bounds_kernel(int total, const unsigned* __restrict__ skey
   invptr[j] = lo;
 }
 
+// chunk_row[k] = first row i with rowptr[i] + kBatchRowCost * i >= k * kBatchChunk
+// (chunk_row[nch] = m)
+__global__ void batch_chunks_kernel(int m, const int* __restrict__ rowptr, int nch, int* __restrict__ chunk_row) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k > nch) return;
+  if (k == nch) {
+    chunk_row[k] = m;
+    return;
+  }
+  const long long target = (long long)k * kBatchChunk;
+  int lo = 0, hi = m;
+  while (lo < hi) {
+    const int mid = (lo + hi) >> 1;
+    if ((long long)__ldg(rowptr + mid) + (long long)kBatchRowCost * mid < target) lo = mid + 1;
+    else hi = mid;
+  }
+  chunk_row[k] = lo;
+}
+
+// A warp's rows, chunk by chunk: the next chunk is taken from the counter one
+// chunk ahead (lane 0's atomic, broadcast), so its bounds are in registers by
+// the time the current chunk runs out.  next() returns m once the chunks are
+// exhausted.  Warp-uniform.
+struct BatchRowIter {
+  int r, end;  // next row of the current chunk, the chunk's end
+  int n0, n1;  // the chunk taken ahead (n0 = m: none left)
+  __device__ __forceinline__ void take(int* ctr, int nch, const int* __restrict__ chunk_row, int m, int lane) {
+    int c = 0;
+    if (lane == 0) c = atomicAdd(ctr, 1);
+    c = __shfl_sync(0xffffffffu, c, 0);
+    n0 = c < nch ? __ldg(chunk_row + c) : m;
+    n1 = c < nch ? __ldg(chunk_row + c + 1) : m;
+  }
+  __device__ __forceinline__ void init(int* ctr, int nch, const int* __restrict__ chunk_row, int m, int lane) {
+    r = end = 0;
+    take(ctr, nch, chunk_row, m, lane);
+  }
+  __device__ __forceinline__ int next(int* ctr, int nch, const int* __restrict__ chunk_row, int m, int lane) {
+    while (r >= end) {  // at most nch iterations: every pass takes a chunk
+      if (n0 >= m) return m;
+      r = n0;
+      end = n1;
+      take(ctr, nch, chunk_row, m, lane);
+    }
+    return r++;
+  }
+};
+
 // rec[p] = (vector, x value bits) of sorted pair p
 __global__ void batch_rec_kernel(int total, const unsigned* __restrict__ inv_ent,
                                  const unsigned* __restrict__ inv_vec, const float* __restrict__ xval,
@@ -83,12 +140,14 @@ __global__ void batch_rec_kernel(int total, const unsigned* __restrict__ inv_ent
     rec[p] = make_int2((int)__ldg(inv_vec + p), __float_as_int(__ldg(xval + __ldg(inv_ent + p))));
 }
 
-// Software pipeline of the row walks.  A warp takes rows i, i + nw, i + 2nw,
-// ...  In the forward, while it works on row i it already holds row i + nw's
-// head (bounds, the lane's first column and value) with that column's pair
-// range in flight, row i + 2nw's head in flight and row i + 3nw's bounds in
-// flight, so only the pair-record loads stay on the critical path of a row's
-// first 32 nonzeros.  The dvals walk, which also holds the next row of dY in
+// Software pipeline of the row walks.  In the forward, a warp takes its rows
+// from the row chunks (BatchRowIter); while it works on a row it already
+// holds its next row's head (bounds, the lane's first column and value) with
+// that column's pair range in flight, the head of the row after in flight
+// and the bounds of the third in flight, so only the pair-record loads stay
+// on the critical path of a row's first 32 nonzeros.  The dvals walk takes its
+// rows from the chunks too, one row shallower (the next row's head and dY
+// row, the bounds of the row after).  The dvals walk, which also holds the next row of dY in
 // registers, runs one row shallower (row i + nw's head, row i + 2nw's
 // bounds): the deeper form needs 64 registers there and loses more to the
 // lower occupancy than it gains.
@@ -151,27 +210,32 @@ __device__ __forceinline__ void batch_add_pairs(float* acc, const int2* __restri
 __global__ void __launch_bounds__(kBatchWarps * 32)
 batch_forward_kernel(int m, int n, int nvec, const int* __restrict__ rowptr, const int* __restrict__ col,
                      const float* __restrict__ val, const int* __restrict__ invptr,
-                     const int2* __restrict__ rec, float alpha, float* __restrict__ Y, int vec4, int* err) {
+                     const int2* __restrict__ rec, float alpha, float* __restrict__ Y, int vec4,
+                     const int* __restrict__ chunk_row, int nch, int* ctr, int* err) {
   extern __shared__ __align__(16) float s_acc[];  // kBatchWarps rows of nvec
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   float* acc = s_acc + warp * nvec;
   for (int v = lane; v < nvec; v += 32) acc[v] = 0.f;
   __syncwarp();
-  const long long nw = (long long)gridDim.x * kBatchWarps;
-  long long i = (long long)blockIdx.x * kBatchWarps + warp;
+  BatchRowIter it;
+  it.init(ctr, nch, chunk_row, m, lane);
+  int i = it.next(ctr, nch, chunk_row, m, lane);  // this row, then the next three of the warp
+  int i1 = it.next(ctr, nch, chunk_row, m, lane);
+  int i2 = it.next(ctr, nch, chunk_row, m, lane);
   int b0, b1;
   batch_row_bounds(rowptr, m, i, b0, b1);
   BatchRowHead cur = batch_row_head(col, val, b0, b1, lane);
-  batch_row_bounds(rowptr, m, i + nw, b0, b1);
+  batch_row_bounds(rowptr, m, i1, b0, b1);
   BatchRowHead nxt = batch_row_head(col, val, b0, b1, lane);
   batch_head_pairs(cur, invptr, n, err);
-  batch_row_bounds(rowptr, m, i + 2 * nw, b0, b1);  // row i + 2nw's bounds
-  for (; i < m; i += nw) {
-    // in flight meanwhile: row i + nw's pair range, row i + 2nw's head, the bounds after it
+  batch_row_bounds(rowptr, m, i2, b0, b1);  // row i2's bounds
+  while (i < m) {
+    // in flight meanwhile: row i1's pair range, row i2's head, the bounds of the row after
     batch_head_pairs(nxt, invptr, n, err);
     const BatchRowHead nn = batch_row_head(col, val, b0, b1, lane);
+    const int i3 = it.next(ctr, nch, chunk_row, m, lane);
     int c0, c1;
-    batch_row_bounds(rowptr, m, i + 3 * nw, c0, c1);
+    batch_row_bounds(rowptr, m, i3, c0, c1);
     batch_add_pairs(acc, rec, cur.p0, cur.p1, cur.a);
     // the row's nonzeros past the first 32, two per lane at a time
     for (int k = cur.a0 + 32 + lane; k < cur.a1; k += 64) {
@@ -186,7 +250,7 @@ batch_forward_kernel(int m, int n, int nvec, const int* __restrict__ rowptr, con
       batch_add_pairs(acc, rec, q10, q11, v1);
     }
     __syncwarp();
-    float* yr = Y + i * nvec;
+    float* yr = Y + (size_t)i * nvec;
     if (vec4) {  // nvec % 4 == 0 and Y 16-byte aligned (checked on the host): vector stores
       float4* y4 = reinterpret_cast<float4*>(yr);
       float4* a4 = reinterpret_cast<float4*>(acc);
@@ -206,59 +270,79 @@ batch_forward_kernel(int m, int n, int nvec, const int* __restrict__ rowptr, con
     nxt = nn;
     b0 = c0;
     b1 = c1;
+    i = i1;
+    i1 = i2;
+    i2 = i3;
   }
+}
+
+// 16-byte asynchronous copy global -> shared (L2 only), and its group waits
+__device__ __forceinline__ void batch_cp16(void* dst, const void* src) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_addr(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void batch_cp_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void batch_cp_wait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
 }
 
 // dvals[k] = alpha * sum over column col_k's pairs of xval[e] * dY[i][v(e)],
 // one warp per row with dY's row in shared memory.  With dxval (fused form,
 // dxval zeroed before) every pair also adds alpha * a[k] * dY[i][v(e)] into
 // dxval[e] with an atomic add.  The same pipeline as the forward; for
-// nvec <= 256 with 16-byte rows the next row of dY is also loaded into
-// registers (two float4 per lane) while this row is walked.
-__global__ void __launch_bounds__(kBatchWarps * 32)
+// nvec <= 256 with 16-byte rows (pre) each warp has two shared dY rows, and
+// the next row of dY is copied into the other one (cp.async, no registers
+// held) while this row is walked.
+__global__ void __launch_bounds__(kBatchWarps * 32, 5)
 batch_dvals_kernel(int m, int n, int nvec, const int* __restrict__ rowptr, const int* __restrict__ col,
                    const int* __restrict__ invptr, const unsigned* __restrict__ inv_ent,
                    const int2* __restrict__ rec, float alpha,
                    const float* __restrict__ dY, float* __restrict__ dvals, const float* __restrict__ val,
-                   float* __restrict__ dxval, int vec4, int* err) {
+                   float* __restrict__ dxval, int vec4, const int* __restrict__ chunk_row, int nch, int* ctr,
+                   int* err) {
   extern __shared__ __align__(16) float s_dy[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  float* g = s_dy + warp * nvec;
-  const bool pre = vec4 && nvec <= 256;  // the next dY row fits two float4 per lane
+  const bool pre = vec4 && nvec <= 256;  // two shared dY rows per warp (the host sizes them)
+  float* const g0 = s_dy + (size_t)warp * (pre ? 2 : 1) * nvec;
   const int n4 = nvec >> 2;
-  const long long nw = (long long)gridDim.x * kBatchWarps;
-  long long i = (long long)blockIdx.x * kBatchWarps + warp;
+  int buf = 0;  // pre: the shared row holding this row's dY
+  // pre: row r's dY (if the row has nonzeros) into shared row `into`; one
+  // commit group per call, empty or not
+  auto fetch = [&](int r, int a0, int a1, int into) {
+    if (r < m && a0 < a1) {
+      const float4* d4 = reinterpret_cast<const float4*>(dY + (size_t)r * nvec);
+      float4* s4 = reinterpret_cast<float4*>(g0 + into * nvec);
+      if (lane < n4) batch_cp16(s4 + lane, d4 + lane);
+      if (lane + 32 < n4) batch_cp16(s4 + lane + 32, d4 + lane + 32);
+    }
+    batch_cp_commit();
+  };
+  BatchRowIter it;
+  it.init(ctr, nch, chunk_row, m, lane);
+  int i = it.next(ctr, nch, chunk_row, m, lane);  // this row and the warp's next
+  int i1 = it.next(ctr, nch, chunk_row, m, lane);
   const float* aval = dxval ? val : nullptr;
   int b0, b1;
   batch_row_bounds(rowptr, m, i, b0, b1);
   BatchRowHead cur = batch_row_head(col, aval, b0, b1, lane);
-  float4 gcur[2] = {make_float4(0.f, 0.f, 0.f, 0.f), make_float4(0.f, 0.f, 0.f, 0.f)};
-  if (pre && i < m && b0 < b1) {
-    const float4* d4 = reinterpret_cast<const float4*>(dY + i * nvec);
-    if (lane < n4) gcur[0] = __ldg(d4 + lane);
-    if (lane + 32 < n4) gcur[1] = __ldg(d4 + lane + 32);
-  }
-  batch_row_bounds(rowptr, m, i + nw, b0, b1);
-  for (; i < m; i += nw) {
+  if (pre) fetch(i, b0, b1, 0);
+  batch_row_bounds(rowptr, m, i1, b0, b1);
+  while (i < m) {
     // in flight meanwhile: the next row's head and dY row, the bounds after it
     const BatchRowHead nxt = batch_row_head(col, aval, b0, b1, lane);
-    float4 gnxt[2] = {make_float4(0.f, 0.f, 0.f, 0.f), make_float4(0.f, 0.f, 0.f, 0.f)};
-    if (pre && i + nw < m && b0 < b1) {
-      const float4* d4 = reinterpret_cast<const float4*>(dY + (i + nw) * nvec);
-      if (lane < n4) gnxt[0] = __ldg(d4 + lane);
-      if (lane + 32 < n4) gnxt[1] = __ldg(d4 + lane + 32);
-    }
+    if (pre) fetch(i1, b0, b1, buf ^ 1);  // the other row was last read before the previous __syncwarp
+    const int i2 = it.next(ctr, nch, chunk_row, m, lane);
     int c0, c1;
-    batch_row_bounds(rowptr, m, i + 2 * nw, c0, c1);
+    batch_row_bounds(rowptr, m, i2, c0, c1);
     if (cur.a0 < cur.a1) {  // warp-uniform
+      float* const g = g0 + (pre ? buf * nvec : 0);
       if (pre) {
-        if (lane < n4) reinterpret_cast<float4*>(g)[lane] = gcur[0];
-        if (lane + 32 < n4) reinterpret_cast<float4*>(g)[lane + 32] = gcur[1];
+        batch_cp_wait<1>();  // every group but the next row's: this row's dY has landed
       } else if (vec4) {
-        const float4* d4 = reinterpret_cast<const float4*>(dY + i * nvec);
+        const float4* d4 = reinterpret_cast<const float4*>(dY + (size_t)i * nvec);
         for (int v = lane; v < n4; v += 32) reinterpret_cast<float4*>(g)[v] = __ldg(d4 + v);
       } else {
-        for (int v = lane; v < nvec; v += 32) g[v] = __ldg(dY + i * nvec + v);
+        for (int v = lane; v < nvec; v += 32) g[v] = __ldg(dY + (size_t)i * nvec + v);
       }
       __syncwarp();
       for (int k = cur.a0 + lane; k < cur.a1; k += 32) {
@@ -282,11 +366,13 @@ batch_dvals_kernel(int m, int n, int nvec, const int* __restrict__ rowptr, const
       __syncwarp();
     }
     cur = nxt;
-    gcur[0] = gnxt[0];
-    gcur[1] = gnxt[1];
+    buf ^= 1;
     b0 = c0;
     b1 = c1;
+    i = i1;
+    i1 = i2;
   }
+  batch_cp_wait<0>();
 }
 
 // dxval[e] = alpha * sum_i A[i][xkey[e]] * dY[i][v(e)], one warp per entry
@@ -411,6 +497,27 @@ static int batch_invert(spmx_handle_t h, int nvec, int total, const int* xptr, c
   return SPMX_SUCCESS;
 }
 
+// the row chunks of the matrix (built once per CSR input; the counters they
+// are taken from are zeroed before every launch)
+static int ensure_batch_chunks(spmx_handle_t h) {
+  if (h->batch_chunk_ready) return SPMX_SUCCESS;
+  const long long w = (long long)h->nnz + (long long)kBatchRowCost * h->m;
+  const long long nch = w / kBatchChunk + 1;
+  if (nch >= INT32_MAX) return set_error(SPMX_ERR_INVALID_VALUE, "batched SpMSpV: too many row chunks");
+  if (!h->batch_chunk || h->batch_nch != (int)nch) {
+    dfree(h->batch_chunk);
+    h->batch_chunk = nullptr;
+    SPMX_TRY(dalloc((void**)&h->batch_chunk, 4 * ((size_t)nch + 1), "batch row chunks"));
+  }
+  if (!h->batch_ctr) SPMX_TRY(dalloc((void**)&h->batch_ctr, 2 * sizeof(int), "batch chunk counters"));
+  note_launch();
+  batch_chunks_kernel<<<(unsigned)((nch + 1 + 255) / 256), 256, 0, h->stream>>>(h->m, h->rowptr, (int)nch,
+                                                                                h->batch_chunk);
+  h->batch_nch = (int)nch;
+  h->batch_chunk_ready = true;
+  return launch_ok("batch row chunks");
+}
+
 static int batched_common(spmx_handle_t h, int nvec, int total, const int* xptr) {
   if (nvec < 1 || nvec > kBatchMaxVec)
     return set_error(SPMX_ERR_INVALID_VALUE, "nvec must be in [1, 1024]");
@@ -442,6 +549,8 @@ extern "C" int spmx_spmspv_batched(spmx_handle_t h, int nvec, int x_total, const
   const int2* rec = nullptr;
   SPMX_TRY(batch_invert(h, nvec, x_total, d_xptr, d_xkey, d_xval, true, &ie, &rec));
   if (h->m == 0) return SPMX_SUCCESS;
+  SPMX_TRY(ensure_batch_chunks(h));
+  SPMX_CUDA(cudaMemsetAsync(h->batch_ctr, 0, sizeof(int), h->stream));
   const size_t smem = 4 * (size_t)kBatchWarps * nvec;
   if (smem > 48 * 1024)
     cudaFuncSetAttribute(batch_forward_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -449,7 +558,7 @@ extern "C" int spmx_spmspv_batched(spmx_handle_t h, int nvec, int x_total, const
   batch_forward_kernel<<<batch_rows_grid(h, (const void*)batch_forward_kernel, smem), kBatchWarps * 32, smem,
                          h->stream>>>(h->m, h->n, nvec, h->rowptr, h->col, h->val, h->batch_invptr, rec,
                                       alpha, d_Y, (nvec % 4 == 0 && ((uintptr_t)d_Y & 15u) == 0) ? 1 : 0,
-                                      h->d_err);
+                                      h->batch_chunk, h->batch_nch, h->batch_ctr, h->d_err);
   return launch_ok("batched spmspv");
 }
 
@@ -468,14 +577,18 @@ extern "C" int spmx_spmspv_batched_backward(spmx_handle_t h, int nvec, int x_tot
     const unsigned* ie = nullptr;
     const int2* rec = nullptr;
     SPMX_TRY(batch_invert(h, nvec, x_total, d_xptr, d_xkey, d_xval, false, &ie, &rec));
-    const size_t smem = 4 * (size_t)kBatchWarps * nvec;
+    SPMX_TRY(ensure_batch_chunks(h));
+    SPMX_CUDA(cudaMemsetAsync(h->batch_ctr + 1, 0, sizeof(int), st));
+    const bool vec4 = nvec % 4 == 0 && ((uintptr_t)d_dY & 15u) == 0;
+    // with 16-byte rows of at most 256 entries each warp double-buffers its dY row
+    const size_t smem = 4 * (size_t)kBatchWarps * nvec * (vec4 && nvec <= 256 ? 2 : 1);
     if (smem > 48 * 1024)
       cudaFuncSetAttribute(batch_dvals_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     note_launch();
     batch_dvals_kernel<<<batch_rows_grid(h, (const void*)batch_dvals_kernel, smem), kBatchWarps * 32, smem,
                          st>>>(h->m, h->n, nvec, h->rowptr, h->col, h->batch_invptr, ie, rec, alpha,
-                               d_dY, d_dvals, h->val, fused ? d_dxval : nullptr,
-                               (nvec % 4 == 0 && ((uintptr_t)d_dY & 15u) == 0) ? 1 : 0, h->d_err);
+                               d_dY, d_dvals, h->val, fused ? d_dxval : nullptr, vec4 ? 1 : 0, h->batch_chunk,
+                               h->batch_nch, h->batch_ctr + 1, h->d_err);
   }
   if (d_dxval && x_total > 0 && !fused) {
     if (!h->has_csc || !h->csc_val)

@@ -212,6 +212,7 @@ extern "C" int spmx_destroy(spmx_handle_t h) {
   dfree(h->ms_hchunk); dfree(h->ms_hcnt); dfree(h->ms_hacc); dfree(h->ms_hleft); dfree(h->ms_hcounters);
   for (void* p : h->batch_buf) dfree(p);
   dfree(h->batch_hist); dfree(h->batch_hoff); dfree(h->batch_invptr); dfree(h->batch_rec);
+  dfree(h->batch_chunk); dfree(h->batch_ctr);
   delete h;
   return SPMX_SUCCESS;
 }
@@ -272,6 +273,7 @@ extern "C" int spmx_input_csr(spmx_handle_t h, int nnz, const int* rowptr,
   h->has_csr = true;
   h->mat_feat_ready = false;
   h->std_row_ready = false;
+  h->batch_chunk_ready = false;
   return SPMX_SUCCESS;
 }
 

@@ -137,6 +137,12 @@ struct spmx_handle_s {
   const unsigned* inv_ent = nullptr;
   const unsigned* inv_vec = nullptr;
   void* batch_rec = nullptr;  // per inverted pair: (vector, x value bits)
+  // row chunks of the batched row walks (rows cut where rowptr[i] + 32 i
+  // crosses a multiple of 2,048; warps take chunks from a device counter)
+  int* batch_chunk = nullptr;
+  int batch_nch = 0;
+  bool batch_chunk_ready = false;
+  int* batch_ctr = nullptr;  // [0] the forward walk's chunk counter, [1] the dvals walk's
   // hub chunks of the multi-source pull (built once per matrix)
   int4* ms_hchunk = nullptr;
   int* ms_hcnt = nullptr;
