@@ -70,18 +70,16 @@ __global__ void batch_keys_kernel(int n, int nvec, int total, const int* __restr
   }
 }
 
-// invptr[j] = first sorted position of column j, j in [0, n]
+// invptr[j] = first sorted position whose key is >= j, j in [0, n]: sorted
+// position p (p in [0, total]) owns the columns after its predecessor's key
+// up to its own key (n at p = total), so every column is written once
 __global__ void batch_bounds_kernel(int total, const unsigned* __restrict__ skey, int n,
                                     int* __restrict__ invptr) {
-  const int j = blockIdx.x * blockDim.x + threadIdx.x;
-  if (j > n) return;
-  int lo = 0, hi = total;
-  while (lo < hi) {
-    const int mid = (lo + hi) >> 1;
-    if ((int)__ldg(skey + mid) < j) lo = mid + 1;
-    else hi = mid;
+  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p <= total; p += gridDim.x * blockDim.x) {
+    const int lo = p == 0 ? 0 : (int)__ldg(skey + p - 1) + 1;
+    const int hi = p == total ? n : min((int)__ldg(skey + p), n);
+    for (int j = lo; j <= hi; ++j) invptr[j] = p;
   }
-  invptr[j] = lo;
 }
 
 // chunk_row[k] = first row i with rowptr[i] + kBatchRowCost * i >= k * kBatchChunk
@@ -478,7 +476,8 @@ static int batch_invert(spmx_handle_t h, int nvec, int total, const int* xptr, c
   *inv_ent = rb.result_in_alt ? b[3] : b[2];
   const unsigned* inv_vec = rb.result_in_alt ? b[5] : b[4];
   note_launch();
-  batch_bounds_kernel<<<(h->n + 1 + 255) / 256, 256, 0, st>>>(total, skey, h->n, h->batch_invptr);
+  batch_bounds_kernel<<<std::min((total + 1 + 255) / 256, h->num_sms * 8), 256, 0, st>>>(total, skey, h->n,
+                                                                                         h->batch_invptr);
   if (total > 0) {
     note_launch();
     batch_rec_kernel<<<std::min((total + 255) / 256, h->num_sms * 8), 256, 0, st>>>(
