@@ -124,41 +124,58 @@ csc_lb_kernel(CscArgs a, CscScratch s, int variant, float* __restrict__ y,
 // column bounds and the first row / value while y is being cleared, and waits
 // (griddepcontrol.wait, a no-op without the launch attribute) only before its
 // first atomic.
-template <int G>
+template <int G, int U>
 __global__ void __launch_bounds__(256)
 csc_naive_kernel(CscArgs a, float* __restrict__ y) {
+  // G lanes per x entry; each lane group takes U entries, gid / G + u * groups,
+  // whose loads are issued phase by phase (all keys, then all column bounds,
+  // then all first nonzeros), so one chain of memory round trips covers U
+  // entries
   const long long gid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  const int i = (int)(gid / G);
+  const long long groups = (long long)gridDim.x * blockDim.x / G;
   const int g = (int)(gid % G);
-  int cs = 0, ce = 0, r0 = -1;
-  float xv = 0.f, v0 = 0.f;
-  bool ok = i < a.x_nnz;
-  if (ok) {
-    const int key = __ldg(a.x_key + i);
-    if ((unsigned)key >= (unsigned)a.n) {
-      if (g == 0) flag_error(a.err, kDevErrOob);
-      ok = false;
-    } else {
-      cs = __ldg(a.colptr + key);
-      ce = __ldg(a.colptr + key + 1);
-      xv = (float)(a.alpha * (double)__ldg(a.x_val + i));
-      if (cs + g < ce) {
-        r0 = __ldg(a.row + cs + g);
-        v0 = __ldg(a.val + cs + g);
-      }
+  int key[U], cs[U], ce[U], r0[U];
+  float xv[U], v0[U];
+#pragma unroll
+  for (int u = 0; u < U; ++u) {
+    const long long i = gid / G + u * groups;
+    key[u] = i < a.x_nnz ? __ldg(a.x_key + i) : -1;
+    xv[u] = i < a.x_nnz ? __ldg(a.x_val + i) : 0.f;
+  }
+#pragma unroll
+  for (int u = 0; u < U; ++u) {
+    const long long i = gid / G + u * groups;
+    const bool ok = (unsigned)key[u] < (unsigned)a.n;
+    if (i < a.x_nnz && !ok && g == 0) flag_error(a.err, kDevErrOob);
+    cs[u] = ok ? __ldg(a.colptr + key[u]) : 0;
+    ce[u] = ok ? __ldg(a.colptr + key[u] + 1) : 0;
+    xv[u] = (float)(a.alpha * (double)xv[u]);
+  }
+#pragma unroll
+  for (int u = 0; u < U; ++u) {
+    r0[u] = -1;
+    v0[u] = 0.f;
+    if (cs[u] + g < ce[u]) {
+      r0[u] = __ldg(a.row + cs[u] + g);
+      v0[u] = __ldg(a.val + cs[u] + g);
     }
   }
   asm volatile("griddepcontrol.wait;" ::: "memory");
-  if (!ok) return;
-  if (cs + g < ce) {
-    if ((unsigned)r0 < (unsigned)a.m) atomicAdd(y + r0, v0 * xv);
-    else flag_error(a.err, kDevErrOob);
+#pragma unroll
+  for (int u = 0; u < U; ++u) {
+    if (cs[u] + g < ce[u]) {
+      if ((unsigned)r0[u] < (unsigned)a.m) atomicAdd(y + r0[u], v0[u] * xv[u]);
+      else flag_error(a.err, kDevErrOob);
+    }
   }
+#pragma unroll
+  for (int u = 0; u < U; ++u) {
 #pragma unroll 4
-  for (int k = cs + g + G; k < ce; k += G) {
-    const int r = __ldg(a.row + k);
-    if ((unsigned)r < (unsigned)a.m) atomicAdd(y + r, __ldg(a.val + k) * xv);
-    else flag_error(a.err, kDevErrOob);
+    for (int k = cs[u] + g + G; k < ce[u]; k += G) {
+      const int r = __ldg(a.row + k);
+      if ((unsigned)r < (unsigned)a.m) atomicAdd(y + r, __ldg(a.val + k) * xv[u]);
+      else flag_error(a.err, kDevErrOob);
+    }
   }
 }
 
@@ -247,9 +264,13 @@ int launch_csc_naive_zeroed(const CscArgs& a, int group, float* y, int num_sms, 
     zero_fill_kernel<<<(unsigned)std::max(1LL, blocks), 256, 0, st>>>(y, a.m);
   }
   if (a.x_nnz <= 0) return 0;
+  // entries per lane group: enough that the grid is about one wave of
+  // resident threads (2,048 per SM), at most 4
   const long long threads = (long long)a.x_nnz * group;
+  const long long resident = (long long)num_sms * 2048;
+  const int U = threads <= resident ? 1 : threads <= 2 * resident ? 2 : 4;
   cudaLaunchConfig_t cfg = {};
-  cfg.gridDim = dim3((unsigned)((threads + 255) / 256));
+  cfg.gridDim = dim3((unsigned)((threads + 256LL * U - 1) / (256LL * U)));
   cfg.blockDim = dim3(256);
   cfg.stream = st;
   cudaLaunchAttribute at[1];
@@ -259,7 +280,13 @@ int launch_csc_naive_zeroed(const CscArgs& a, int group, float* y, int num_sms, 
   cfg.numAttrs = 1;
   note_launch();
   cudaError_t e = cudaSuccess;
-  SPMX_GROUP_SWITCH(group, (e = cudaLaunchKernelEx(&cfg, csc_naive_kernel<G>, a, y)));
+  if (U == 1) {
+    SPMX_GROUP_SWITCH(group, (e = cudaLaunchKernelEx(&cfg, csc_naive_kernel<G, 1>, a, y)));
+  } else if (U == 2) {
+    SPMX_GROUP_SWITCH(group, (e = cudaLaunchKernelEx(&cfg, csc_naive_kernel<G, 2>, a, y)));
+  } else {
+    SPMX_GROUP_SWITCH(group, (e = cudaLaunchKernelEx(&cfg, csc_naive_kernel<G, 4>, a, y)));
+  }
   return e == cudaSuccess ? 0 : -2;
 }
 
@@ -268,7 +295,7 @@ int launch_csc_naive(const CscArgs& a, int group, float* y, cudaStream_t st) {
   const long long threads = (long long)a.x_nnz * group;
   const unsigned grid = (unsigned)((threads + 255) / 256);
   note_launch();
-  SPMX_GROUP_SWITCH(group, (csc_naive_kernel<G><<<grid, 256, 0, st>>>(a, y)));
+  SPMX_GROUP_SWITCH(group, (csc_naive_kernel<G, 1><<<grid, 256, 0, st>>>(a, y)));
   return 0;
 }
 

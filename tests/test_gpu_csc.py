@@ -76,6 +76,26 @@ def test_csc_atomic(torch_cuda, mat, vname, variant, frac):
     assert np.array_equal(yv[:ynnz].cpu().numpy(), ev)
 
 
+@pytest.mark.parametrize("k", [50_000, 200_000])
+def test_csc_naive_several_entries_per_lane_group(torch_cuda, k):
+    """An x large enough that the naive scatter gives each lane group two
+    (k = 50,000) or four (k = 200,000) entries, on the 1M-row Zipf matrix."""
+    torch = torch_cuda
+    from spmx import gen
+    A = gen.zipf_1m()
+    h = make_handle(A, torch, hola=False)
+    key, val = _x(A.n, k, 5)
+    set_sparse(h, key, val, torch)
+    y = torch.full((A.m,), 3.0, device="cuda")
+    h.spmspv_csc(0, 0, 1.5, y, sync=False)
+    h.check_device_error()
+    colptr, row, cval = A.to_csc()
+    y64, mag, _ = orc.spmspv_csc_f64(A.m, colptr, row, cval, key, val, alpha=1.5)
+    yh = y.cpu().numpy()
+    ok, _ = orc.within_tol(yh, y64, mag, RTOL)
+    assert ok, orc.max_scaled_err(yh, y64, mag)
+
+
 @pytest.mark.parametrize("mat", ["uniform", "skewed"])
 @pytest.mark.parametrize("vname,variant", VARIANTS)
 @pytest.mark.parametrize("frac", [0.001, 0.1, 1.0])
