@@ -180,6 +180,51 @@ round_spmv_kernel(const __grid_constant__ RoundGeom geom, int nslots, int parts,
   // each row's slots, summed in slot order, into F[r] or (INPLACE) into the
   // row's first slot; a row without slots has the sum 0
   const int base0 = __ldg(vbg + row0);
+  if (parts == 1) {
+    // one CTA per row block: each row's slot sum is y.  Row blocks start on
+    // multiples of 4, so a thread takes groups of 4 consecutive rows: one
+    // 16-byte load of their slot bounds (plus the next row's), one 16-byte
+    // store of y where y allows it; VG groups per thread per pass, their
+    // loads issued together
+    constexpr int VG = 4;
+    const bool y16 = (((uintptr_t)(y + row0)) & 15u) == 0;
+    const int full = rows & ~3;
+    for (int rb = 0; rb < full; rb += 4 * VG * (int)blockDim.x) {
+      int4 lo[VG];
+      int hi[VG];
+#pragma unroll
+      for (int j = 0; j < VG; ++j) {
+        const int r = rb + 4 * (j * (int)blockDim.x + (int)threadIdx.x);
+        lo[j] = r < full ? __ldg(reinterpret_cast<const int4*>(vbg + row0 + r)) : make_int4(0, 0, 0, 0);
+        hi[j] = r < full ? __ldg(vbg + row0 + r + 4) : 0;
+      }
+#pragma unroll
+      for (int j = 0; j < VG; ++j) {
+        const int r = rb + 4 * (j * (int)blockDim.x + (int)threadIdx.x);
+        if (r >= full) continue;
+        const int b[5] = {lo[j].x - base0, lo[j].y - base0, lo[j].z - base0, lo[j].w - base0, hi[j] - base0};
+        float t[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          float acc = 0.f;
+          for (int s = b[q]; s < b[q + 1]; ++s) acc += ys[s];
+          t[q] = alpha * acc;
+        }
+        if (y16) {
+          *reinterpret_cast<float4*>(y + row0 + r) = make_float4(t[0], t[1], t[2], t[3]);
+        } else {
+#pragma unroll
+          for (int q = 0; q < 4; ++q) y[row0 + r + q] = t[q];
+        }
+      }
+    }
+    for (int r = full + (int)threadIdx.x; r < rows; r += blockDim.x) {  // the last block's ragged end
+      float acc = 0.f;
+      for (int s = __ldg(vbg + row0 + r) - base0; s < __ldg(vbg + row0 + r + 1) - base0; ++s) acc += ys[s];
+      y[row0 + r] = alpha * acc;
+    }
+    return;
+  }
   constexpr int FU = 8;  // rows per thread per pass: their slot bounds are loaded together
   for (int rb4 = 0; rb4 < rows; rb4 += FU * (int)blockDim.x) {
     int lo[FU], hi[FU];
@@ -195,13 +240,11 @@ round_spmv_kernel(const __grid_constant__ RoundGeom geom, int nslots, int parts,
       if (r < rows) {
         float acc = 0.f;
         for (int s = lo[j] - base0; s < hi[j] - base0; ++s) acc += ys[s];
-        if (parts == 1) y[row0 + r] = alpha * acc;  // one CTA per row block: its row sums are y
-        else if (!INPLACE) F[r] = acc;
+        if (!INPLACE) F[r] = acc;
         else if (hi[j] > lo[j]) ys[lo[j] - base0] = acc;  // rows own disjoint slots
       }
     }
   }
-  if (parts == 1) return;
   // the cluster's row sums, added in rank order; each CTA takes a slice
   cg::cluster_group cl = cg::this_cluster();
   cl.sync();

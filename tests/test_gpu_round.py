@@ -122,6 +122,29 @@ def test_round_zipf_full_size(torch_cuda, parts):
     _check_spmv(torch, h, A, 1.0, x)
 
 
+@pytest.mark.parametrize("parts", [1, 2])
+@pytest.mark.parametrize("offset", [0, 1])
+def test_round_ragged_rows_and_unaligned_y(torch_cuda, parts, offset):
+    """m not a multiple of 4 (the last row block ends off a 4-row group) and,
+    with offset 1, a y that is not 16-byte aligned (the one-CTA fold's scalar
+    stores)."""
+    torch = torch_cuda
+    A = rand_csr(10003, 5000, density=0.004, seed=51)
+    h = make_handle(A, torch, csc=False, hola=False)
+    h.roundPreprocess(0, parts)
+    x = np.random.default_rng(52).uniform(-1, 1, A.n).astype(np.float32)
+    h.set_x(dev(x, torch))
+    ybuf = torch.full((A.m + 1,), 7.0, device="cuda")
+    y = ybuf[offset:offset + A.m]
+    h.roundspmv(-0.5, y)
+    h.check_device_error()
+    y64, mag = orc.spmv_f64(A.rowptr, A.col, A.val, x, alpha=-0.5)
+    ok, _ = orc.within_tol(y.cpu().numpy(), y64, mag, RTOL)
+    assert ok
+    edge = ybuf[A.m] if offset == 0 else ybuf[0]
+    assert float(edge) == 7.0  # nothing written outside y
+
+
 def test_round_refusals_keep_handle_usable(torch_cuda):
     torch = torch_cuda
     from spmx import SpmxError
