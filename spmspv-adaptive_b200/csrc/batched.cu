@@ -14,7 +14,8 @@
 // Design: the batch is inverted once per call (a stable radix sort of the
 // entries by column gives, per column, the (vector, entry) pairs that use
 // it; each pair is then stored as one 8-byte record of its vector and its x
-// value, so a row walk reads one sector per pair), then
+// value for the forward, and one 16-byte record that adds its entry for the
+// backward, so a row walk reads one sector per pair), then
 //   forward  - one warp per row of A (CSR): lanes take the row's nonzeros,
 //              look up their columns' pairs and add a[k] * x into a shared
 //              row of nvec accumulators; the warp then stores the row of Y
@@ -130,12 +131,18 @@ struct BatchRowIter {
   }
 };
 
-// rec[p] = (vector, x value bits) of sorted pair p
+// rec[p] = (vector, x value bits) of sorted pair p, for the forward walk (four
+// records per sector); rec4[p] = (vector, x value bits, entry, 0), for the
+// backward walk, whose dxval atomic needs the entry
 __global__ void batch_rec_kernel(int total, const unsigned* __restrict__ inv_ent,
                                  const unsigned* __restrict__ inv_vec, const float* __restrict__ xval,
-                                 int2* __restrict__ rec) {
-  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < total; p += gridDim.x * blockDim.x)
-    rec[p] = make_int2((int)__ldg(inv_vec + p), __float_as_int(__ldg(xval + __ldg(inv_ent + p))));
+                                 int2* __restrict__ rec, int4* __restrict__ rec4) {
+  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < total; p += gridDim.x * blockDim.x) {
+    const int v = (int)__ldg(inv_vec + p), e = (int)__ldg(inv_ent + p);
+    const int xb = __float_as_int(__ldg(xval + e));
+    rec[p] = make_int2(v, xb);
+    rec4[p] = make_int4(v, xb, e, 0);
+  }
 }
 
 // Software pipeline of the row walks.  In the forward, a warp takes its rows
@@ -293,8 +300,7 @@ __device__ __forceinline__ void batch_cp_wait() {
 // held) while this row is walked.
 __global__ void __launch_bounds__(kBatchWarps * 32, 5)
 batch_dvals_kernel(int m, int n, int nvec, const int* __restrict__ rowptr, const int* __restrict__ col,
-                   const int* __restrict__ invptr, const unsigned* __restrict__ inv_ent,
-                   const int2* __restrict__ rec, float alpha,
+                   const int* __restrict__ invptr, const int4* __restrict__ rec, float alpha,
                    const float* __restrict__ dY, float* __restrict__ dvals, const float* __restrict__ val,
                    float* __restrict__ dxval, int vec4, const int* __restrict__ chunk_row, int nch, int* ctr,
                    int* err) {
@@ -351,10 +357,10 @@ batch_dvals_kernel(int m, int n, int nvec, const int* __restrict__ rowptr, const
           const int q1 = __ldg(invptr + j + 1);
           const float a = dxval ? alpha * (first ? cur.a : __ldg(val + k)) : 0.f;
           for (int p = __ldg(invptr + j); p < q1; ++p) {
-            const int2 r = __ldg(rec + p);
+            const int4 r = __ldg(rec + p);
             const float gv = g[r.x];
             s += __int_as_float(r.y) * gv;
-            if (dxval) atomicAdd(dxval + __ldg(inv_ent + p), a * gv);
+            if (dxval) atomicAdd(dxval + r.z, a * gv);
           }
         } else {
           flag_error(err, kDevErrOob);
@@ -411,6 +417,9 @@ using namespace spmx;
 // scratch for the inverted batch of x_total entries (grown, never shrunk)
 static void batch_forget_inversion(spmx_handle_t h);
 
+// the pair records: cap int2 records, then (at a 256-byte boundary) cap int4 records
+static size_t batch_rec4_offset(int cap) { return (8 * (size_t)cap + 255) & ~(size_t)255; }
+
 static int ensure_batch_scratch(spmx_handle_t h, int total) {
   if (h->batch_cap >= total && h->batch_invptr_n == h->n && h->batch_invptr) return SPMX_SUCCESS;
   batch_forget_inversion(h);
@@ -434,7 +443,7 @@ static int ensure_batch_scratch(spmx_handle_t h, int total) {
   SPMX_TRY(dalloc((void**)&h->batch_hist, 4 * hn, "batch hist"));
   SPMX_TRY(dalloc((void**)&h->batch_hoff, 4 * hn, "batch hist off"));
   SPMX_TRY(dalloc((void**)&h->batch_invptr, 4 * ((size_t)h->n + 1), "batch inverse pointers"));
-  SPMX_TRY(dalloc(&h->batch_rec, 8 * (size_t)cap, "batch pair records"));
+  SPMX_TRY(dalloc(&h->batch_rec, batch_rec4_offset(cap) + 16 * (size_t)cap, "batch pair records"));
   h->batch_cap = cap;
   h->batch_invptr_n = h->n;
   return SPMX_SUCCESS;
@@ -450,12 +459,14 @@ static void batch_forget_inversion(spmx_handle_t h) {
 // A forward call records which batch the inversion belongs to; a backward
 // call with SPMX_BATCH_REUSE_INVERSION set reuses it for the same batch.
 static int batch_invert(spmx_handle_t h, int nvec, int total, const int* xptr, const int* xkey,
-                        const float* xval, bool forward, const unsigned** inv_ent, const int2** rec) {
+                        const float* xval, bool forward, const unsigned** inv_ent, const int2** rec,
+                        const int4** rec4) {
   if (!forward && (h->batch_opts & SPMX_BATCH_REUSE_INVERSION) && h->inv_ent && h->inv_xptr == xptr &&
       h->inv_xkey == xkey && h->inv_xval == xval && h->inv_nvec == nvec && h->inv_total == total &&
       h->batch_invptr_n == h->n) {
     *inv_ent = h->inv_ent;
     *rec = (const int2*)h->batch_rec;
+    *rec4 = (const int4*)((const char*)h->batch_rec + batch_rec4_offset(h->batch_cap));
     return SPMX_SUCCESS;
   }
   batch_forget_inversion(h);
@@ -481,9 +492,11 @@ static int batch_invert(spmx_handle_t h, int nvec, int total, const int* xptr, c
   if (total > 0) {
     note_launch();
     batch_rec_kernel<<<std::min((total + 255) / 256, h->num_sms * 8), 256, 0, st>>>(
-        total, *inv_ent, inv_vec, xval, (int2*)h->batch_rec);
+        total, *inv_ent, inv_vec, xval, (int2*)h->batch_rec,
+        (int4*)((char*)h->batch_rec + batch_rec4_offset(h->batch_cap)));
   }
   *rec = (const int2*)h->batch_rec;
+  *rec4 = (const int4*)((const char*)h->batch_rec + batch_rec4_offset(h->batch_cap));
   if (forward) {
     h->inv_xptr = xptr;
     h->inv_xkey = xkey;
@@ -546,7 +559,8 @@ extern "C" int spmx_spmspv_batched(spmx_handle_t h, int nvec, int x_total, const
   if (x_total > 0 && (!d_xkey || !d_xval)) return set_error(SPMX_ERR_INVALID_VALUE, "NULL batch arrays");
   const unsigned* ie = nullptr;
   const int2* rec = nullptr;
-  SPMX_TRY(batch_invert(h, nvec, x_total, d_xptr, d_xkey, d_xval, true, &ie, &rec));
+  const int4* rec4 = nullptr;
+  SPMX_TRY(batch_invert(h, nvec, x_total, d_xptr, d_xkey, d_xval, true, &ie, &rec, &rec4));
   if (h->m == 0) return SPMX_SUCCESS;
   SPMX_TRY(ensure_batch_chunks(h));
   SPMX_CUDA(cudaMemsetAsync(h->batch_ctr, 0, sizeof(int), h->stream));
@@ -575,7 +589,8 @@ extern "C" int spmx_spmspv_batched_backward(spmx_handle_t h, int nvec, int x_tot
   if (d_dvals && h->nnz > 0) {
     const unsigned* ie = nullptr;
     const int2* rec = nullptr;
-    SPMX_TRY(batch_invert(h, nvec, x_total, d_xptr, d_xkey, d_xval, false, &ie, &rec));
+    const int4* rec4 = nullptr;
+    SPMX_TRY(batch_invert(h, nvec, x_total, d_xptr, d_xkey, d_xval, false, &ie, &rec, &rec4));
     SPMX_TRY(ensure_batch_chunks(h));
     SPMX_CUDA(cudaMemsetAsync(h->batch_ctr + 1, 0, sizeof(int), st));
     const bool vec4 = nvec % 4 == 0 && ((uintptr_t)d_dY & 15u) == 0;
@@ -585,7 +600,7 @@ extern "C" int spmx_spmspv_batched_backward(spmx_handle_t h, int nvec, int x_tot
       cudaFuncSetAttribute(batch_dvals_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     note_launch();
     batch_dvals_kernel<<<batch_rows_grid(h, (const void*)batch_dvals_kernel, smem), kBatchWarps * 32, smem,
-                         st>>>(h->m, h->n, nvec, h->rowptr, h->col, h->batch_invptr, ie, rec, alpha,
+                         st>>>(h->m, h->n, nvec, h->rowptr, h->col, h->batch_invptr, rec4, alpha,
                                d_dY, d_dvals, h->val, fused ? d_dxval : nullptr, vec4 ? 1 : 0, h->batch_chunk,
                                h->batch_nch, h->batch_ctr + 1, h->d_err);
   }

@@ -136,7 +136,9 @@ struct spmx_handle_s {
   const void* inv_xval = nullptr;
   const unsigned* inv_ent = nullptr;
   const unsigned* inv_vec = nullptr;
-  void* batch_rec = nullptr;  // per inverted pair: (vector, x value bits)
+  // per inverted pair: int2 (vector, x value bits), then, at a 256-byte
+  // boundary, int4 (vector, x value bits, entry, 0)
+  void* batch_rec = nullptr;
   // row chunks of the batched row walks (rows cut where rowptr[i] + 32 i
   // crosses a multiple of 2,048; warps take chunks from a device counter)
   int* batch_chunk = nullptr;
