@@ -254,6 +254,36 @@ def test_batched_options_reuse_and_fused(torch_cuda, problem, graph):
     assert _close(dvals2.cpu().numpy(), dv, dvm)
 
 
+def test_batched_rows_heavier_than_a_chunk(torch_cuda):
+    """A row of 9,000 nonzeros spans several row chunks (the chunks whose
+    weight boundaries fall inside it are empty and must be skipped), between
+    empty rows and short ones; forward and fused backward against FP64."""
+    torch = torch_cuda
+    from conftest import rand_csr
+    rng = np.random.default_rng(61)
+    lens = rng.integers(0, 8, 3000)
+    lens[rng.choice(3000, 400, replace=False)] = 0
+    lens[7] = 9000
+    lens[2999] = 5000
+    A = rand_csr(3000, 12000, lens=lens, seed=62)
+    xptr, xkey, xval = _batch(A.n, 8, seed=63, lo=50, hi=3000)
+    h = make_handle(A, torch, hola=False)
+    h.set_batch_options(3)
+    nvec, tot = len(xptr) - 1, int(xptr[-1])
+    Y = torch.empty((A.m, nvec), device="cuda")
+    xp, xk, xv = dev(xptr, torch), dev(xkey, torch), dev(xval, torch)
+    h.spmspv_batched(xp, xk, xv, 1.25, Y, x_total=tot)
+    dY = np.random.default_rng(64).standard_normal((A.m, nvec)).astype(np.float32)
+    dxval = torch.empty(tot, device="cuda")
+    dvals = torch.empty(A.nnz, device="cuda")
+    h.spmspv_batched_backward(xp, xk, xv, 1.25, dev(dY, torch), dxval, dvals, x_total=tot)
+    h.check_device_error()
+    _check_forward(A, xptr, xkey, xval, Y.cpu().numpy(), 1.25)
+    dx, dxm, dv, dvm = _refs(A, xptr, xkey, xval, dY, 1.25)
+    assert _close(dxval.cpu().numpy(), dx, dxm)
+    assert _close(dvals.cpu().numpy(), dv, dvm)
+
+
 def test_batched_unaligned_outputs(torch_cuda, problem):
     """Y and dY that start 4 bytes past a 16-byte boundary take the scalar
     row stores / loads (nvec is a multiple of 4 here)."""
