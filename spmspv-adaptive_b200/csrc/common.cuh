@@ -387,7 +387,8 @@ __device__ __forceinline__ bool grid_sync(const GridBarrier& b, int* err) {
 // Launch with an L2 access-policy window: the window [base, base + bytes) is
 // marked persisting for this launch only (no stream state changes), so a
 // small gathered operand (the dense x, a frontier bitmap) stays in L2 while
-// the streamed matrix passes through it.  bytes == 0 launches plainly.
+// the streamed matrix passes through it.  bytes == 0 launches plainly; the
+// window is off unless SPMX_L2_WINDOW is set to a non-zero value.
 // ---------------------------------------------------------------------------
 size_t l2_window_bytes(const void* base, size_t bytes);  // clamp; 0 = disabled
 
