@@ -219,8 +219,8 @@ int spmx_tiledspmspv(spmx_handle_t h, float alpha, float* d_y);
 /* Round SpMV / bitmap-gated SpMSpV (no reference counterpart; a fourth
  * back-end for the load-balanced SpMV of the selector, spmv_type 3).  Rows
  * are cut into row blocks (at most rb_rows rows; 0 = as many as fit), one per
- * cluster of 2 CTAs; each CTA streams half of its block's nonzeros sorted by
- * (column, row) in rounds of 4096.  Every row owns as many shared-memory
+ * CTA (spmx_round_preprocess_parts below has the clustered layouts); a CTA
+ * streams its block's nonzeros sorted by (column, row) in rounds of 4096.  Every row owns as many shared-memory
  * accumulators as it has nonzeros in its densest round; the k-th nonzero of
  * a row in a round adds into the row's k-th accumulator with a plain
  * read-modify-write (all distinct within a round), one barrier per round;
@@ -235,10 +235,12 @@ int spmx_tiledspmspv(spmx_handle_t h, float alpha, float* d_y);
  * starting a new 128-entry chunk. */
 int spmx_round_preprocess(spmx_handle_t h, int rb_rows);
 /* No reference counterpart.  The round format with `parts` CTAs per row
- * block: 1 (row blocks half as tall, one CTA each over all columns, no
- * cluster: each row's accumulators are summed straight into y), 2 (what
- * spmx_round_preprocess builds: one 2-CTA cluster per row block) or 4 (two
- * clusters per row block, each row block twice as tall, the
+ * block: 1 (what spmx_round_preprocess builds: one CTA per row block over all
+ * columns, no cluster, each row's accumulators summed straight into y; the
+ * fastest layout measured), 2 (one 2-CTA cluster per row block, twice as
+ * tall, each CTA over half the columns, the row sums combined through
+ * distributed shared memory) or 4 (two clusters per row block, each row block
+ * four times as tall, the
  * row sums folded into each row's first accumulator slot; the two clusters'
  * sums meet in a small device buffer and the second to finish a row slice
  * stores y, so every row is still added in a fixed order).  Taller row blocks

@@ -225,6 +225,84 @@ round_spmv_kernel(const __grid_constant__ RoundGeom geom, int nslots, int parts,
     }
     return;
   }
+  if (!INPLACE && parts == kRoundCS) {
+    // one 2-CTA cluster per row block: the same groups of 4 rows into F, then
+    // each CTA adds a slice of the rows (a multiple of 4) from both CTAs' F in
+    // rank order, 16 bytes at a time through distributed shared memory
+    constexpr int VG = 4;
+    const int full = rows & ~3;
+    for (int rb = 0; rb < full; rb += 4 * VG * (int)blockDim.x) {
+      int4 lo[VG];
+      int hi[VG];
+#pragma unroll
+      for (int j = 0; j < VG; ++j) {
+        const int r = rb + 4 * (j * (int)blockDim.x + (int)threadIdx.x);
+        lo[j] = r < full ? __ldg(reinterpret_cast<const int4*>(vbg + row0 + r)) : make_int4(0, 0, 0, 0);
+        hi[j] = r < full ? __ldg(vbg + row0 + r + 4) : 0;
+      }
+#pragma unroll
+      for (int j = 0; j < VG; ++j) {
+        const int r = rb + 4 * (j * (int)blockDim.x + (int)threadIdx.x);
+        if (r >= full) continue;
+        const int b[5] = {lo[j].x - base0, lo[j].y - base0, lo[j].z - base0, lo[j].w - base0, hi[j] - base0};
+        float t[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          float acc = 0.f;
+          for (int s = b[q]; s < b[q + 1]; ++s) acc += ys[s];
+          t[q] = acc;
+        }
+        *reinterpret_cast<float4*>(F + r) = make_float4(t[0], t[1], t[2], t[3]);
+      }
+    }
+    for (int r = full + (int)threadIdx.x; r < rows; r += blockDim.x) {
+      float acc = 0.f;
+      for (int s = __ldg(vbg + row0 + r) - base0; s < __ldg(vbg + row0 + r + 1) - base0; ++s) acc += ys[s];
+      F[r] = acc;
+    }
+    cg::cluster_group cl = cg::this_cluster();
+    cl.sync();
+    const int rank = (int)cl.block_rank();
+    const int slice = ((rows + 7) / 8) * 4;
+    const int r0 = rank * slice, r1 = min(rows, r0 + slice);
+    const float* F0 = cl.map_shared_rank(F, 0);
+    const float* F1 = cl.map_shared_rank(F, 1);
+    const bool y16 = (((uintptr_t)(y + row0)) & 15u) == 0;
+    const int g1 = r0 + ((max(0, r1 - r0)) & ~3);  // the slice's groups of 4 end here
+    constexpr int CG = 2;  // groups of 4 rows per thread per pass: their peer reads are issued together
+    for (int rc = r0; rc < g1; rc += 4 * CG * (int)blockDim.x) {
+      float4 a[CG], c[CG];
+#pragma unroll
+      for (int j = 0; j < CG; ++j) {
+        const int r = rc + 4 * (j * (int)blockDim.x + (int)threadIdx.x);
+        a[j] = r < g1 ? *reinterpret_cast<const float4*>(F0 + r) : make_float4(0.f, 0.f, 0.f, 0.f);
+        c[j] = r < g1 ? *reinterpret_cast<const float4*>(F1 + r) : make_float4(0.f, 0.f, 0.f, 0.f);
+      }
+#pragma unroll
+      for (int j = 0; j < CG; ++j) {
+        const int r = rc + 4 * (j * (int)blockDim.x + (int)threadIdx.x);
+        if (r >= g1) continue;
+        float t[4] = {0.f, 0.f, 0.f, 0.f};
+        t[0] += a[j].x; t[1] += a[j].y; t[2] += a[j].z; t[3] += a[j].w;
+        t[0] += c[j].x; t[1] += c[j].y; t[2] += c[j].z; t[3] += c[j].w;
+        if (y16) {
+          *reinterpret_cast<float4*>(y + row0 + r) =
+              make_float4(alpha * t[0], alpha * t[1], alpha * t[2], alpha * t[3]);
+        } else {
+#pragma unroll
+          for (int q = 0; q < 4; ++q) y[row0 + r + q] = alpha * t[q];
+        }
+      }
+    }
+    for (int r = g1 + (int)threadIdx.x; r < r1; r += blockDim.x) {  // the slice's ragged end
+      float acc = 0.f;
+      acc += F0[r];
+      acc += F1[r];
+      y[row0 + r] = alpha * acc;
+    }
+    cl.sync();  // the peer reads this CTA's F until here
+    return;
+  }
   constexpr int FU = 8;  // rows per thread per pass: their slot bounds are loaded together
   for (int rb4 = 0; rb4 < rows; rb4 += FU * (int)blockDim.x) {
     int lo[FU], hi[FU];
@@ -906,7 +984,7 @@ static int round_preprocess(spmx_handle_t h, int rb_rows, int parts) {
   }
 }
 
-extern "C" int spmx_round_preprocess(spmx_handle_t h, int rb_rows) { return round_preprocess(h, rb_rows, 2); }
+extern "C" int spmx_round_preprocess(spmx_handle_t h, int rb_rows) { return round_preprocess(h, rb_rows, 1); }
 
 extern "C" int spmx_round_preprocess_parts(spmx_handle_t h, int rb_rows, int parts) {
   return round_preprocess(h, rb_rows, parts);

@@ -263,11 +263,11 @@ class SpmspvHandle:
     def tiledspmspv(self, alpha, y):
         check(lib.spmx_tiledspmspv(self._h, float(alpha), _f32(y)), "tiledspmspv")
 
-    def roundPreprocess(self, rb_rows=0, parts=2):
-        """Round format with `parts` CTAs per row block (2; 1: one CTA per row
-        block, row blocks half as tall, no cluster; or 4: two clusters over
-        row blocks twice as tall)."""
-        if parts == 2:
+    def roundPreprocess(self, rb_rows=0, parts=1):
+        """Round format with `parts` CTAs per row block (1: one CTA per row
+        block, no cluster; 2: a 2-CTA cluster over row blocks twice as tall;
+        4: two clusters over row blocks four times as tall)."""
+        if parts == 1:
             check(lib.spmx_round_preprocess(self._h, int(rb_rows)), "roundPreprocess")
         else:
             check(lib.spmx_round_preprocess_parts(self._h, int(rb_rows), int(parts)), "roundPreprocess")

@@ -123,15 +123,17 @@ def test_graph_bfs(torch_cuda):
     del graph
 
 
-def test_graph_round_spmv_chain(torch_cuda):
+@pytest.mark.parametrize("parts", [1, 2])
+def test_graph_round_spmv_chain(torch_cuda, parts):
     """The round back-end launched as the dependent of the sparse-to-dense
     scatter (cluster and programmatic-dependent-launch attributes) replays
-    from a graph: sparse x -> dense x -> SpMV, and the gated form."""
+    from a graph: sparse x -> dense x -> SpMV, and the gated form; one CTA
+    per row block and 2-CTA clusters."""
     torch = torch_cuda
     from spmx import gen
     A = gen.zipf_rows(1 << 15, 1.5, 16, 3000, seed=24)
     h = make_handle(A, torch, csc=False, hola=False)
-    h.roundPreprocess()
+    h.roundPreprocess(0, parts)
     h.set_spmv_type(3)
     rng = np.random.default_rng(25)
     k = A.n // 3
