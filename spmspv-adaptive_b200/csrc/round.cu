@@ -440,6 +440,21 @@ __global__ void round_bounds_kernel(int nnz, const unsigned* __restrict__ skey, 
   out[t] = lo;
 }
 
+// *out = 1 when some run of up to 128 consecutive sorted entries of one row
+// block spans 2^16 columns or more.  The layout's chunks are such runs (they
+// start at multiples of 128 from their row block's first entry), so without
+// a flag no chunk needs the padded layout.  Valid entries end at bounds[nrb].
+__global__ void round_span_kernel(int nnz, const unsigned* __restrict__ skey, int nrb, int cbits,
+                                  const int* __restrict__ bounds, int* __restrict__ out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nnz || i >= __ldg(bounds + nrb)) return;
+  const unsigned cmask = (1u << cbits) - 1u;
+  const unsigned ki = __ldg(skey + i);
+  const int b = (int)(ki >> cbits);
+  const int j = min(i + 127, __ldg(bounds + b + 1) - 1);
+  if ((__ldg(skey + j) & cmask) - (ki & cmask) >= 65536u) *out = 1;
+}
+
 // out[t] = first sorted position with key >= (rb << cbits) | (seg << 16),
 // t = rb * nseg + seg in [0, nrb * nseg]: where each 2^16-column segment of
 // each row block starts (t = nrb * nseg gives the end of the last block)
@@ -728,6 +743,18 @@ static int round_build(spmx_handle_t h, long long rcap, long long avail, int par
       if (cudaMemcpyAsync(bounds.data(), d_bounds, 4 * ((size_t)nrb + 1), cudaMemcpyDeviceToHost, st) !=
           cudaSuccess)
         rc = set_error(SPMX_ERR_CUDA, "round SpMV: block bounds");
+    }
+    // a wide column span switches the padded layout on here, so the sort is
+    // not repeated (the layout kernel still checks every chunk)
+    if (!rc && !pad) {
+      int wide = 0;
+      note_launch();
+      round_span_kernel<<<(unsigned)(((long long)nnz + 255) / 256), 256, 0, st>>>(nnz, skey, nrb, cbits, d_bounds,
+                                                                                 flags + 1);
+      if (cudaMemcpyAsync(&wide, flags + 1, sizeof(int), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+          cudaStreamSynchronize(st) != cudaSuccess)
+        rc = set_error(SPMX_ERR_CUDA, "round SpMV: span check");
+      if (!rc && wide) pad = true;
     }
   }
   // with pad: where each 2^16-column segment of each row block starts
