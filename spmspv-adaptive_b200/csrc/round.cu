@@ -91,6 +91,47 @@ size_t round_smem(int nslots, int rmax, bool inplace) {
   return 4 * (size_t)(((nslots + 3) & ~3) + (inplace ? 0 : rmax));
 }
 
+// The slot sums (in slot order) of the rows [0, rows) of a row block that
+// starts at row0, a multiple of 4: a thread takes groups of 4 consecutive
+// rows, one 16-byte load of their slot bounds plus the next row's, VG groups
+// per pass with their loads issued together; then the ragged end one row at a
+// time.  store4(r, t) receives rows r .. r + 3, store1(r, v) one row.
+template <class Store4, class Store1>
+__device__ __forceinline__ void round_fold4(int rows, int row0, const int* __restrict__ vbg, int base0,
+                                            const float* ys, Store4 store4, Store1 store1) {
+  constexpr int VG = 4;
+  const int full = rows & ~3;
+  for (int rb = 0; rb < full; rb += 4 * VG * (int)blockDim.x) {
+    int4 lo[VG];
+    int hi[VG];
+#pragma unroll
+    for (int j = 0; j < VG; ++j) {
+      const int r = rb + 4 * (j * (int)blockDim.x + (int)threadIdx.x);
+      lo[j] = r < full ? __ldg(reinterpret_cast<const int4*>(vbg + row0 + r)) : make_int4(0, 0, 0, 0);
+      hi[j] = r < full ? __ldg(vbg + row0 + r + 4) : 0;
+    }
+#pragma unroll
+    for (int j = 0; j < VG; ++j) {
+      const int r = rb + 4 * (j * (int)blockDim.x + (int)threadIdx.x);
+      if (r >= full) continue;
+      const int b[5] = {lo[j].x - base0, lo[j].y - base0, lo[j].z - base0, lo[j].w - base0, hi[j] - base0};
+      float t[4];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        float acc = 0.f;
+        for (int s = b[q]; s < b[q + 1]; ++s) acc += ys[s];
+        t[q] = acc;
+      }
+      store4(r, t);
+    }
+  }
+  for (int r = full + (int)threadIdx.x; r < rows; r += blockDim.x) {
+    float acc = 0.f;
+    for (int s = __ldg(vbg + row0 + r) - base0; s < __ldg(vbg + row0 + r + 1) - base0; ++s) acc += ys[s];
+    store1(r, acc);
+  }
+}
+
 // parts CTAs per row block: one CTA, whose row sums are y (no cluster); or
 // clusters of 2, with parts = 4 two of them, in which case each cluster adds
 // its two CTAs' row sums and the two clusters meet in psum: the second to
@@ -181,85 +222,30 @@ round_spmv_kernel(const __grid_constant__ RoundGeom geom, int nslots, int parts,
   // row's first slot; a row without slots has the sum 0
   const int base0 = __ldg(vbg + row0);
   if (parts == 1) {
-    // one CTA per row block: each row's slot sum is y.  Row blocks start on
-    // multiples of 4, so a thread takes groups of 4 consecutive rows: one
-    // 16-byte load of their slot bounds (plus the next row's), one 16-byte
-    // store of y where y allows it; VG groups per thread per pass, their
-    // loads issued together
-    constexpr int VG = 4;
+    // one CTA per row block: each row's slot sum is y (16-byte stores where
+    // y allows them)
     const bool y16 = (((uintptr_t)(y + row0)) & 15u) == 0;
-    const int full = rows & ~3;
-    for (int rb = 0; rb < full; rb += 4 * VG * (int)blockDim.x) {
-      int4 lo[VG];
-      int hi[VG];
+    round_fold4(
+        rows, row0, vbg, base0, ys,
+        [&](int r, const float (&t)[4]) {
+          if (y16) {
+            *reinterpret_cast<float4*>(y + row0 + r) = make_float4(alpha * t[0], alpha * t[1], alpha * t[2], alpha * t[3]);
+          } else {
 #pragma unroll
-      for (int j = 0; j < VG; ++j) {
-        const int r = rb + 4 * (j * (int)blockDim.x + (int)threadIdx.x);
-        lo[j] = r < full ? __ldg(reinterpret_cast<const int4*>(vbg + row0 + r)) : make_int4(0, 0, 0, 0);
-        hi[j] = r < full ? __ldg(vbg + row0 + r + 4) : 0;
-      }
-#pragma unroll
-      for (int j = 0; j < VG; ++j) {
-        const int r = rb + 4 * (j * (int)blockDim.x + (int)threadIdx.x);
-        if (r >= full) continue;
-        const int b[5] = {lo[j].x - base0, lo[j].y - base0, lo[j].z - base0, lo[j].w - base0, hi[j] - base0};
-        float t[4];
-#pragma unroll
-        for (int q = 0; q < 4; ++q) {
-          float acc = 0.f;
-          for (int s = b[q]; s < b[q + 1]; ++s) acc += ys[s];
-          t[q] = alpha * acc;
-        }
-        if (y16) {
-          *reinterpret_cast<float4*>(y + row0 + r) = make_float4(t[0], t[1], t[2], t[3]);
-        } else {
-#pragma unroll
-          for (int q = 0; q < 4; ++q) y[row0 + r + q] = t[q];
-        }
-      }
-    }
-    for (int r = full + (int)threadIdx.x; r < rows; r += blockDim.x) {  // the last block's ragged end
-      float acc = 0.f;
-      for (int s = __ldg(vbg + row0 + r) - base0; s < __ldg(vbg + row0 + r + 1) - base0; ++s) acc += ys[s];
-      y[row0 + r] = alpha * acc;
-    }
+            for (int q = 0; q < 4; ++q) y[row0 + r + q] = alpha * t[q];
+          }
+        },
+        [&](int r, float v) { y[row0 + r] = alpha * v; });
     return;
   }
   if (!INPLACE && parts == kRoundCS) {
-    // one 2-CTA cluster per row block: the same groups of 4 rows into F, then
-    // each CTA adds a slice of the rows (a multiple of 4) from both CTAs' F in
-    // rank order, 16 bytes at a time through distributed shared memory
-    constexpr int VG = 4;
-    const int full = rows & ~3;
-    for (int rb = 0; rb < full; rb += 4 * VG * (int)blockDim.x) {
-      int4 lo[VG];
-      int hi[VG];
-#pragma unroll
-      for (int j = 0; j < VG; ++j) {
-        const int r = rb + 4 * (j * (int)blockDim.x + (int)threadIdx.x);
-        lo[j] = r < full ? __ldg(reinterpret_cast<const int4*>(vbg + row0 + r)) : make_int4(0, 0, 0, 0);
-        hi[j] = r < full ? __ldg(vbg + row0 + r + 4) : 0;
-      }
-#pragma unroll
-      for (int j = 0; j < VG; ++j) {
-        const int r = rb + 4 * (j * (int)blockDim.x + (int)threadIdx.x);
-        if (r >= full) continue;
-        const int b[5] = {lo[j].x - base0, lo[j].y - base0, lo[j].z - base0, lo[j].w - base0, hi[j] - base0};
-        float t[4];
-#pragma unroll
-        for (int q = 0; q < 4; ++q) {
-          float acc = 0.f;
-          for (int s = b[q]; s < b[q + 1]; ++s) acc += ys[s];
-          t[q] = acc;
-        }
-        *reinterpret_cast<float4*>(F + r) = make_float4(t[0], t[1], t[2], t[3]);
-      }
-    }
-    for (int r = full + (int)threadIdx.x; r < rows; r += blockDim.x) {
-      float acc = 0.f;
-      for (int s = __ldg(vbg + row0 + r) - base0; s < __ldg(vbg + row0 + r + 1) - base0; ++s) acc += ys[s];
-      F[r] = acc;
-    }
+    // one 2-CTA cluster per row block: the slot sums into F, then each CTA
+    // adds a slice of the rows (a multiple of 4) from both CTAs' F in rank
+    // order, 16 bytes at a time through distributed shared memory
+    round_fold4(
+        rows, row0, vbg, base0, ys,
+        [&](int r, const float (&t)[4]) { *reinterpret_cast<float4*>(F + r) = make_float4(t[0], t[1], t[2], t[3]); },
+        [&](int r, float v) { F[r] = v; });
     cg::cluster_group cl = cg::this_cluster();
     cl.sync();
     const int rank = (int)cl.block_rank();
