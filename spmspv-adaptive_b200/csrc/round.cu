@@ -638,15 +638,17 @@ static int round_build(spmx_handle_t h, long long rcap, long long avail, int par
   // each.  Where the row cap makes some blocks take far more nonzeros than
   // others (a power-law matrix: its many short rows fill blocks by rows, so
   // the hub rows crowd into the first blocks), the block count doubles (more
-  // waves) until the largest block holds at most 1.3 times the mean, or until
+  // waves) until the largest block holds at most 1.5 times the mean, or until
   // its CTAs' share is at most 3/4 of what one SM takes of the whole matrix
-  // (then it no longer sets the time; a single hub row can keep a block above
-  // 1.3 times the mean however many blocks there are).
+  // (then it no longer sets the time).  A doubling that leaves the largest
+  // block above 2/3 of its size (a single hub row fills it) is undone: a
+  // second wave costs more than the imbalance it removes.
   const long long need = std::max<long long>(1, (m + rcap - 1) / rcap);
   const long long max_blocks = std::max(1, m / 4);
   int nrb = (int)std::max<long long>(need, std::min<long long>((long long)(h->num_sms / parts) * waves, max_blocks));
   nrb = std::max(1, nrb);
-  std::vector<int> rbr;
+  std::vector<int> rbr, prev_rbr;
+  long long prev_big = -1;
   for (;;) {
     rbr.assign((size_t)nrb + 1, 0);
     rbr[nrb] = m;
@@ -664,9 +666,18 @@ static int round_build(spmx_handle_t h, long long rcap, long long avail, int par
     long long big = 0;
     for (int k = 0; k < nrb; ++k) big = std::max<long long>(big, (long long)rp[rbr[k + 1]] - rp[rbr[k]]);
     const double mean = (double)nnz / nrb;
-    if (nnz == 0 || (double)big <= 1.3 * mean || (double)big / parts <= 0.75 * (double)nnz / h->num_sms ||
+    if (prev_big >= 0 && 3 * big > 2 * prev_big) {
+      // doubling left the largest block above 2/3 of its size (one hub row
+      // fills it): the extra wave would only cost, keep the previous count
+      rbr.swap(prev_rbr);
+      nrb /= 2;
+      break;
+    }
+    if (nnz == 0 || (double)big <= 1.5 * mean || (double)big / parts <= 0.75 * (double)nnz / h->num_sms ||
         2LL * nrb > max_blocks || nrb >= 16 * (h->num_sms / parts))
       break;
+    prev_big = big;
+    prev_rbr = rbr;
     nrb *= 2;
   }
   const int cbits = bits_for((long long)std::max(n, 1));
