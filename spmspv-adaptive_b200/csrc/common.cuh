@@ -384,6 +384,31 @@ __device__ __forceinline__ bool grid_sync(const GridBarrier& b, int* err) {
 }
 
 // ---------------------------------------------------------------------------
+// Programmatic dependent launch: the grid may start while the grid before it
+// on the stream is still running, once that grid has executed
+// griddepcontrol.launch_dependents (or exited).  A kernel launched this way
+// executes griddepcontrol.wait in every thread before it touches memory that
+// an earlier grid on the stream writes, and before it writes memory that an
+// earlier grid reads; and it executes launch_dependents only after that wait,
+// so that whatever it lets start finds every earlier grid complete.
+// ---------------------------------------------------------------------------
+template <class... KArgs, class... Args>
+cudaError_t launch_pdl(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t st,
+                       Args&&... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
+}
+
+// ---------------------------------------------------------------------------
 // Launch with an L2 access-policy window: the window [base, base + bytes) is
 // marked persisting for this launch only (no stream state changes), so a
 // small gathered operand (the dense x, a frontier bitmap) stays in L2 while

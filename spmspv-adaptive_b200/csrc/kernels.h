@@ -94,6 +94,8 @@ struct CscScratch {
 
 constexpr int kCscScanNT = 256, kCscScanVT = 8;   // 2048 x entries per tile
 constexpr int kCscLbNT = 256, kCscLbVT = 8;       // 2048 items per LB block
+// lanes-per-column value that selects the warp-tile scatter (csc_tile_kernel)
+constexpr int kColTile = 64;
 
 int launch_csc_scan(const CscArgs& a, const CscScratch& s, ScanScratch& ls,
                     int block_items, cudaStream_t st);

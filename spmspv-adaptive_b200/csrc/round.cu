@@ -194,6 +194,8 @@ round_spmv_kernel(const __grid_constant__ RoundGeom geom, int nslots, int parts,
   // launched as a programmatic dependent of the grid that writes x: nothing
   // above touches x or y
   asm volatile("griddepcontrol.wait;" ::: "memory");
+  // (no griddepcontrol.launch_dependents here: with it the kernel took 48.0
+  // instead of 46.1 us on the 1M-row Zipf matrix, followed by no dependent)
   if (k0 < k1) gather(pa, ba, xa);
   __syncthreads();
   // one round: issue the next round's gathers, add this round into its

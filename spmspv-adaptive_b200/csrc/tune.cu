@@ -23,6 +23,8 @@
 #include "engine.h"
 #include "kernels.h"
 
+static_assert(spmx::kColTile == SPMX_COL_WARP_TILES, "warp-tile lanes value");
+
 using namespace spmx;
 
 namespace {
@@ -125,6 +127,16 @@ static int apply_params(spmx_handle_t h, const Params& p) {
     rc = spmx_round_preprocess_parts(h, p.tiled_rb, p.tiled_win == 1 || p.tiled_win == 4 ? p.tiled_win : 2);
   }
   return rc;
+}
+
+extern "C" int spmx_set_naive_lanes(spmx_handle_t h, int row_lanes, int col_lanes) {
+  if (!h) return set_error(SPMX_ERR_INVALID_VALUE, "NULL handle");
+  auto ok = [](int g) { return g == 0 || g == 1 || g == 2 || g == 4 || g == 8 || g == 16 || g == 32; };
+  if (!ok(row_lanes) || !(ok(col_lanes) || col_lanes == SPMX_COL_WARP_TILES))
+    return set_error(SPMX_ERR_INVALID_VALUE, "lanes must be 0, 1, 2, 4, 8, 16 or 32 (or warp tiles for columns)");
+  h->naive_row_group = row_lanes;
+  h->naive_col_group = col_lanes;
+  return SPMX_SUCCESS;
 }
 
 extern "C" int spmx_autotune(spmx_handle_t h, const char* cache_path, int* spmv_type_out) {
@@ -233,7 +245,7 @@ extern "C" int spmx_autotune(spmx_handle_t h, const char* cache_path, int* spmv_
       h->x_val = xval;
       h->x_nnz = k;
       bt = 1e30f;
-      for (int g : {1, 2, 4, 8, 16, 32}) {
+      for (int g : {1, 2, 4, 8, 16, 32, kColTile}) {
         h->naive_col_group = g;
         const float t = time_us([&] {
           return spmx_spmspv_csc(h, SPMX_CSC_NAIVE, SPMX_WB_ATOMIC, 1.0f, y, nullptr, nullptr, nullptr);

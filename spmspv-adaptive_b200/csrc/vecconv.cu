@@ -30,7 +30,6 @@ __global__ void scatter_kernel(int nvals, int len, const int* __restrict__ key,
 __global__ void scatter_after_fill_kernel(int nvals, int len, const int* __restrict__ key,
                                           const float* __restrict__ val, float* __restrict__ dense,
                                           int* err) {
-  asm volatile("griddepcontrol.launch_dependents;");
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   int k = 0;
   float v = 0.f;
@@ -39,6 +38,7 @@ __global__ void scatter_after_fill_kernel(int nvals, int len, const int* __restr
     v = val ? __ldg(val + i) : 1.0f;
   }
   asm volatile("griddepcontrol.wait;" ::: "memory");
+  asm volatile("griddepcontrol.launch_dependents;");
   if (i >= nvals) return;
   if ((unsigned)k >= (unsigned)len) {
     flag_error(err, kDevErrOob);

@@ -140,6 +140,7 @@ _SIGS = {
     "spmx_select_features": (c_int, [PD, PI]),
     "spmx_selector_inputs": (c_int, [P, PD]),
     "spmx_run_adaptive": (c_int, [P, c_float, P, PI]),
+    "spmx_set_naive_lanes": (c_int, [P, c_int, c_int]),
     "spmx_run_kernel": (c_int, [P, c_int, c_float, P]),
     "spmx_autotune": (c_int, [P, ctypes.c_char_p, PI]),
     "spmx_bfs": (c_int, [P, c_int, P, PI]),

@@ -441,6 +441,12 @@ class SpmspvHandle:
                                 ctypes.byref(t)), "autotune")
         return t.value
 
+    def set_naive_lanes(self, row_lanes=0, col_lanes=0):
+        """Lanes per row / column of the naive kernels (0: from the mean
+        length; col_lanes = SPMX_COL_WARP_TILES (64) selects the warp-tile
+        CSC scatter)."""
+        check(lib.spmx_set_naive_lanes(self._h, int(row_lanes), int(col_lanes)), "set_naive_lanes")
+
     def run_kernel(self, kid, alpha, y):
         check(lib.spmx_run_kernel(self._h, int(kid), float(alpha), _f32(y)), "run_kernel")
 
