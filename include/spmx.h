@@ -408,10 +408,7 @@ int spmx_run_kernel(spmx_handle_t h, int kernel_id, float alpha, float* d_y);
 /* The naive kernels' lanes per row (CSR SpMV) and per column (CSC SpMSpV),
  * as the autotuner sets them (no reference counterpart: the reference fixes
  * one thread per row / column, DEV/csc_sort_spmspv.cuh:98-119).  Each is 0
- * (derived from the mean row / column length) or 1, 2, 4, 8, 16, 32; the
- * column value SPMX_COL_WARP_TILES selects the warp-tile scatter (a warp per
- * 32 x entries, half a warp per column). */
-#define SPMX_COL_WARP_TILES 64
+ * (derived from the mean row / column length) or 1, 2, 4, 8, 16, 32. */
 int spmx_set_naive_lanes(spmx_handle_t h, int row_lanes, int col_lanes);
 
 /* ======================= BFS (Boolean OR-AND semiring) ==================== */

@@ -182,82 +182,6 @@ csc_naive_kernel(CscArgs a, float* __restrict__ y) {
   }
 }
 
-// The same scatter in warp tiles: a warp takes 32 consecutive x entries (one
-// per lane: key, value, column bounds), then walks their columns two at a
-// time, half a warp per column, 16 lanes apart.  A pass issues the loads of
-// 16 nonzeros of all 32 columns (nonzeros 0-15, then 16-31) before any of its
-// reductions, so a lane keeps 32 loads in flight and the grid needs one tile
-// per warp (x_nnz / 32 warps, under one wave at density 0.1 of a 1M-column
-// matrix) instead of several waves of lane groups, each waiting on its own
-// chain of memory round trips.  Longer columns finish in a per-column loop.
-// y is zero-filled by the grid launched before this one, as for
-// csc_naive_kernel.
-__global__ void __launch_bounds__(256, 3)
-csc_tile_kernel(CscArgs a, float* __restrict__ y) {
-  constexpr unsigned FULL = 0xffffffffu;
-  const int lane = threadIdx.x & 31, half = lane >> 4, g = lane & 15;
-  const long long warp0 = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
-  bool waited = false;
-  for (long long t = warp0; t * 32 < a.x_nnz; t += nwarps) {
-    const long long i = t * 32 + lane;
-    int key = -1;
-    float xv = 0.f;
-    if (i < a.x_nnz) {
-      key = __ldg(a.x_key + i);
-      xv = __ldg(a.x_val + i);
-    }
-    const bool ok = (unsigned)key < (unsigned)a.n;
-    if (i < a.x_nnz && !ok) flag_error(a.err, kDevErrOob);
-    const int cs = ok ? __ldg(a.colptr + key) : 0;
-    const int ce = ok ? __ldg(a.colptr + key + 1) : 0;
-    xv = (float)(a.alpha * (double)xv);
-#pragma unroll 1
-    for (int p = 0; p < 2; ++p) {
-      // step s: this half-warp's column is entry 2s + half, its nonzero 16p + g
-      int r[16];
-      float v[16];
-      unsigned has = 0;
-#pragma unroll
-      for (int s = 0; s < 16; ++s) {
-        const int k = __shfl_sync(FULL, cs, 2 * s + half) + 16 * p + g;
-        r[s] = 0;
-        v[s] = 0.f;
-        if (k < __shfl_sync(FULL, ce, 2 * s + half)) {
-          r[s] = __ldg(a.row + k);
-          v[s] = __ldg(a.val + k);
-          has |= 1u << s;
-        }
-      }
-      if (!waited) {
-        asm volatile("griddepcontrol.wait;" ::: "memory");
-        asm volatile("griddepcontrol.launch_dependents;");
-        waited = true;
-      }
-#pragma unroll
-      for (int s = 0; s < 16; ++s) {
-        const float xe = __shfl_sync(FULL, xv, 2 * s + half);
-        if ((has >> s) & 1u) {
-          if ((unsigned)r[s] < (unsigned)a.m) atomicAdd(y + r[s], v[s] * xe);
-          else flag_error(a.err, kDevErrOob);
-        }
-      }
-    }
-    // nonzeros 32 and beyond of the longer columns
-    for (int s = 0; s < 16; ++s) {
-      const int c0 = __shfl_sync(FULL, cs, 2 * s + half);
-      const int c1 = __shfl_sync(FULL, ce, 2 * s + half);
-      const float xe = __shfl_sync(FULL, xv, 2 * s + half);
-      for (int k = c0 + 32 + g; k < c1; k += 16) {
-        const int rr = __ldg(a.row + k);
-        if ((unsigned)rr < (unsigned)a.m) atomicAdd(y + rr, __ldg(a.val + k) * xe);
-        else flag_error(a.err, kDevErrOob);
-      }
-    }
-  }
-  if (!waited) asm volatile("griddepcontrol.wait;" ::: "memory");
-}
-
 template <int G>
 __global__ void __launch_bounds__(256)
 csc_naive_pairs_kernel(CscArgs a, CscScratch s, int* __restrict__ prow,
@@ -346,31 +270,10 @@ int launch_zero_fill(float* y, long long m, int num_sms, cudaStream_t st) {
              : -2;
 }
 
-// the warp-tile scatter: one tile of 32 x entries per warp, the grid capped
-// at the CTAs that fit on the GPU at once (warps loop over the tiles beyond)
-static int launch_csc_tile(const CscArgs& a, float* y, int num_sms, cudaStream_t st) {
-  static int per_sm = 0;
-  if (per_sm == 0) {
-    int b = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, csc_tile_kernel, 256, 0) != cudaSuccess) {
-      cudaGetLastError();
-      b = 2;
-    }
-    per_sm = b > 0 ? b : 1;
-  }
-  const long long warps = ((long long)a.x_nnz + 31) / 32;
-  const long long ctas = std::min<long long>((warps + 7) / 8, (long long)num_sms * per_sm);
-  note_launch();
-  return launch_pdl(csc_tile_kernel, dim3((unsigned)std::max(1LL, ctas)), dim3(256), 0, st, a, y) == cudaSuccess
-             ? 0
-             : -2;
-}
-
 // zero y, then the naive CSC SpMSpV as a programmatic dependent launch
 int launch_csc_naive_zeroed(const CscArgs& a, int group, float* y, int num_sms, cudaStream_t st) {
   if (a.m > 0 && launch_zero_fill(y, a.m, num_sms, st)) return -2;
   if (a.x_nnz <= 0) return 0;
-  if (group == kColTile) return launch_csc_tile(a, y, num_sms, st);
   // entries per lane group: enough that the grid is about one wave of
   // resident threads (2,048 per SM), at most 4
   const long long threads = (long long)a.x_nnz * group;
@@ -399,12 +302,6 @@ int launch_csc_naive_zeroed(const CscArgs& a, int group, float* y, int num_sms, 
 
 int launch_csc_naive(const CscArgs& a, int group, float* y, cudaStream_t st) {
   if (a.x_nnz <= 0) return 0;
-  if (group == kColTile) {
-    int dev = 0, sms = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    return launch_csc_tile(a, y, sms, st);
-  }
   const long long threads = (long long)a.x_nnz * group;
   const unsigned grid = (unsigned)((threads + 255) / 256);
   note_launch();
@@ -415,7 +312,6 @@ int launch_csc_naive(const CscArgs& a, int group, float* y, cudaStream_t st) {
 int launch_csc_naive_pairs(const CscArgs& a, const CscScratch& s, int group,
                            int* pairs_row, float* pairs_val, cudaStream_t st) {
   if (a.x_nnz <= 0) return 0;
-  if (group == kColTile) group = 16;  // the pairs kernel has no tile form
   const long long threads = (long long)a.x_nnz * group;
   const unsigned grid = (unsigned)((threads + 255) / 256);
   note_launch();

@@ -145,6 +145,7 @@ extern "C" int spmx_create(int m, int n, int nnz, spmx_handle_t* out) {
   rc = rc ? rc : dalloc((void**)&h->ls.status, sizeof(unsigned long long) * h->ls.status_len,
                         "lookback status");
   rc = rc ? rc : dalloc((void**)&h->ls.ticket, sizeof(unsigned) * 4, "ticket");
+  rc = rc ? rc : dalloc((void**)&h->ls.counts, sizeof(unsigned) * h->ls.status_len, "range counts");
   if (!rc && cudaMallocHost((void**)&h->h_pinned, sizeof(int) * 16) != cudaSuccess) {
     cudaGetLastError();
     rc = set_error(SPMX_ERR_ALLOC, "cudaMallocHost(pinned counters)");
@@ -197,7 +198,7 @@ extern "C" int spmx_destroy(spmx_handle_t h) {
   if (h->stream) cudaStreamSynchronize(h->stream); else cudaDeviceSynchronize();
   cudaGetLastError();
   dfree(h->d_counts); dfree(h->d_err); dfree(h->d_facc); dfree(h->d_iacc); dfree(h->d_u64);
-  dfree(h->ls.status); dfree(h->ls.ticket);
+  dfree(h->ls.status); dfree(h->ls.ticket); dfree(h->ls.counts);
   if (h->h_pinned) cudaFreeHost(h->h_pinned);
   dfree(h->own_colptr); dfree(h->own_row); dfree(h->own_cval);
   dfree(h->own_csr_rowptr); dfree(h->own_csr_col); dfree(h->own_csr_val);
@@ -523,9 +524,13 @@ static int ensure_scan_tiles(spmx_handle_t h, long long tiles) {
   if (tiles <= h->ls.status_len) return SPMX_SUCCESS;
   SPMX_CUDA(cudaStreamSynchronize(h->stream));
   dfree(h->ls.status);
+  dfree(h->ls.counts);
   h->ls.status = nullptr;
+  h->ls.counts = nullptr;
+  h->ls.status_len = 0;
   const int len = (int)(tiles + 4);
   SPMX_TRY(dalloc((void**)&h->ls.status, sizeof(unsigned long long) * len, "lookback status"));
+  SPMX_TRY(dalloc((void**)&h->ls.counts, sizeof(unsigned) * len, "range counts"));
   SPMX_CUDA(cudaMemset(h->ls.status, 0, sizeof(unsigned long long) * len));
   h->ls.status_len = len;
   return SPMX_SUCCESS;

@@ -55,6 +55,7 @@ struct ScanScratch {
   unsigned long long* status;  // tile status words
   int status_len;              // capacity in tiles
   unsigned* ticket;            // 4 words, zeroed once: ticket, epoch, publish count
+  unsigned* counts;            // status_len per-range counts (the compaction's first pass)
 };
 
 // indices into the handle's device counter block
@@ -94,8 +95,6 @@ struct CscScratch {
 
 constexpr int kCscScanNT = 256, kCscScanVT = 8;   // 2048 x entries per tile
 constexpr int kCscLbNT = 256, kCscLbVT = 8;       // 2048 items per LB block
-// lanes-per-column value that selects the warp-tile scatter (csc_tile_kernel)
-constexpr int kColTile = 64;
 
 int launch_csc_scan(const CscArgs& a, const CscScratch& s, ScanScratch& ls,
                     int block_items, cudaStream_t st);

@@ -23,8 +23,6 @@
 #include "engine.h"
 #include "kernels.h"
 
-static_assert(spmx::kColTile == SPMX_COL_WARP_TILES, "warp-tile lanes value");
-
 using namespace spmx;
 
 namespace {
@@ -132,8 +130,8 @@ static int apply_params(spmx_handle_t h, const Params& p) {
 extern "C" int spmx_set_naive_lanes(spmx_handle_t h, int row_lanes, int col_lanes) {
   if (!h) return set_error(SPMX_ERR_INVALID_VALUE, "NULL handle");
   auto ok = [](int g) { return g == 0 || g == 1 || g == 2 || g == 4 || g == 8 || g == 16 || g == 32; };
-  if (!ok(row_lanes) || !(ok(col_lanes) || col_lanes == SPMX_COL_WARP_TILES))
-    return set_error(SPMX_ERR_INVALID_VALUE, "lanes must be 0, 1, 2, 4, 8, 16 or 32 (or warp tiles for columns)");
+  if (!ok(row_lanes) || !ok(col_lanes))
+    return set_error(SPMX_ERR_INVALID_VALUE, "lanes must be 0, 1, 2, 4, 8, 16 or 32");
   h->naive_row_group = row_lanes;
   h->naive_col_group = col_lanes;
   return SPMX_SUCCESS;
@@ -245,7 +243,7 @@ extern "C" int spmx_autotune(spmx_handle_t h, const char* cache_path, int* spmv_
       h->x_val = xval;
       h->x_nnz = k;
       bt = 1e30f;
-      for (int g : {1, 2, 4, 8, 16, 32, kColTile}) {
+      for (int g : {1, 2, 4, 8, 16, 32}) {
         h->naive_col_group = g;
         const float t = time_us([&] {
           return spmx_spmspv_csc(h, SPMX_CSC_NAIVE, SPMX_WB_ATOMIC, 1.0f, y, nullptr, nullptr, nullptr);

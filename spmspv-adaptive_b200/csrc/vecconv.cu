@@ -5,10 +5,11 @@
 // dense2bits: one warp per 32-bit word, ballot of (x != 0); no atomics, no
 //   memset (the reference memsets and atomically ORs, and tests `!val`,
 //   setting the bits of zeros, H:1362).
-// compact_nonzero: dense -> (key, val) of the entries != 0, in index order, in
-//   ONE pass: per-warp ballot/popc ranks, a block scan of warp counts and a
-//   decoupled look-back across tiles (the reference runs a flag kernel, a CUB
-//   scan with a temporary allocation and a compaction kernel, H:1883-1928).
+// compact: dense -> (key, val) of the entries != 0, in index order, in two
+//   chained grids: per-range nonzero counts, then per-range prefixes from
+//   those counts and the writes (per-warp ballot/popc ranks, a block scan of
+//   warp counts); the reference runs a flag kernel, a CUB scan with a
+//   temporary allocation and a compaction kernel, H:1883-1928.
 #include "kernels.h"
 #include "common.cuh"
 
@@ -58,50 +59,115 @@ __global__ void dense2bits_kernel(int len, const float* __restrict__ dense,
   if (lane == 0 && word * 32 < len) bits[word] = (int)b;
 }
 
+// Compaction in two grids, chained by programmatic dependent launch.  Pass 1
+// counts the nonzeros of each CTA's range of `per` elements; pass 2 adds the
+// counts of the ranges before its own (at most kCompactMaxRanges of them, a
+// few loads per thread), then writes its range's nonzeros sub-tile by sub-tile
+// of NT * VT elements.  A single pass with a decoupled look-back took 11-14 us
+// for 1M elements whatever the look-back window: its CTAs sat at a barrier
+// while warp 0 took a ticket, published and looked back.  Here nothing waits
+// on another CTA.
+constexpr int kCompactMaxRanges = 1024;
+
 template <int NT, int VT>
 __global__ void __launch_bounds__(NT)
-compact_nonzero_kernel(int len, const float* __restrict__ dense,
-                       int* __restrict__ key, float* __restrict__ val,
-                       int* d_count, LookbackState st, int ntiles, int* err) {
+compact_count_kernel(long long len, long long per, const float* __restrict__ dense,
+                     unsigned* __restrict__ counts) {
   constexpr int NW = NT / 32;
-  __shared__ unsigned s_cnt[VT * NW];
-  __shared__ unsigned s_wtmp[NT / 32 + 1];
-  __shared__ int s_tile;
-  __shared__ unsigned s_prefix;
-  __shared__ unsigned s_total;
-  const int tile = lb_acquire_tile(st, ntiles, &s_tile);
-  const int base = tile * NT * VT;
-  const int tid = threadIdx.x, w = tid >> 5, lane = tid & 31;
-  float v[VT];
-  unsigned mask[VT];
+  __shared__ unsigned s_w[NW];
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  asm volatile("griddepcontrol.launch_dependents;");
+  const long long r0 = (long long)blockIdx.x * per, r1 = min(len, r0 + per);
+  unsigned c = 0;
+  for (long long b = r0; b < r1; b += (long long)NT * VT) {
 #pragma unroll
-  for (int j = 0; j < VT; ++j) {
-    const int i = base + j * NT + tid;
-    v[j] = (i < len) ? __ldg(dense + i) : 0.0f;
-    mask[j] = __ballot_sync(0xffffffffu, v[j] != 0.0f);
-    if (lane == 0) s_cnt[j * NW + w] = __popc(mask[j]);
-  }
-  __syncthreads();
-  // exclusive scan of the VT*NW counts, in (j, w) order == index order
-  unsigned c = (tid < VT * NW) ? s_cnt[tid] : 0u;
-  unsigned total;
-  const unsigned ex = block_exclusive_sum<NT>(c, s_wtmp, &total);
-  if (tid < VT * NW) s_cnt[tid] = ex;
-  if (tid < 32) {
-    const unsigned p = lb_warp_lookback(st, tile, ntiles, total, err);
-    if (tid == 0) { s_prefix = p; s_total = total; }
-  }
-  __syncthreads();
-  const unsigned prefix = s_prefix;
-#pragma unroll
-  for (int j = 0; j < VT; ++j) {
-    if (v[j] != 0.0f) {
-      const unsigned pos = prefix + s_cnt[j * NW + w] + __popc(mask[j] & lanemask_lt());
-      key[pos] = base + j * NT + tid;
-      val[pos] = v[j];
+    for (int j = 0; j < VT; ++j) {
+      const long long i = b + j * NT + threadIdx.x;
+      c += (i < r1 && __ldg(dense + i) != 0.0f) ? 1u : 0u;
     }
   }
-  if (tile == ntiles - 1 && tid == 0) *d_count = (int)(prefix + s_total);
+  c = warp_sum(c);
+  if (lane_id() == 0) s_w[threadIdx.x >> 5] = c;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    unsigned t = threadIdx.x < NW ? s_w[threadIdx.x] : 0u;
+    t = warp_sum(t);
+    if (threadIdx.x == 0) counts[blockIdx.x] = t;
+  }
+}
+
+template <int NT, int VT>
+__global__ void __launch_bounds__(NT)
+compact_write_kernel(long long len, long long per, const float* __restrict__ dense,
+                     const unsigned* __restrict__ counts, int* __restrict__ key,
+                     float* __restrict__ val, int* d_count) {
+  constexpr int NW = NT / 32;
+  __shared__ unsigned s_cnt[VT * NW];
+  __shared__ unsigned s_wtmp[NW + 1];
+  __shared__ unsigned s_red[NW];
+  __shared__ int s_key[NT * VT];
+  __shared__ float s_val[NT * VT];
+  const int tid = threadIdx.x, w = tid >> 5, lane = tid & 31;
+  const long long r0 = (long long)blockIdx.x * per, r1 = min(len, r0 + per);
+  // the first sub-tile's values: dense was written before pass 1 waited, so
+  // it is complete once this grid starts
+  float v[VT];
+#pragma unroll
+  for (int j = 0; j < VT; ++j) {
+    const long long i = r0 + j * NT + tid;
+    v[j] = (i < r1) ? __ldg(dense + i) : 0.0f;
+  }
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  asm volatile("griddepcontrol.launch_dependents;");
+  // nonzeros before this range
+  unsigned pre = 0;
+  for (int t = tid; t < (int)blockIdx.x; t += NT) pre += __ldcg(counts + t);
+  pre = warp_sum(pre);
+  if (lane == 0) s_red[w] = pre;
+  __syncthreads();
+  unsigned run = 0;
+#pragma unroll
+  for (int q = 0; q < NW; ++q) run += s_red[q];
+  for (long long b = r0; b < r1; b += (long long)NT * VT) {
+    if (b != r0) {
+#pragma unroll
+      for (int j = 0; j < VT; ++j) {
+        const long long i = b + j * NT + tid;
+        v[j] = (i < r1) ? __ldg(dense + i) : 0.0f;
+      }
+    }
+    unsigned mask[VT];
+#pragma unroll
+    for (int j = 0; j < VT; ++j) {
+      mask[j] = __ballot_sync(0xffffffffu, v[j] != 0.0f);
+      if (lane == 0) s_cnt[j * NW + w] = __popc(mask[j]);
+    }
+    __syncthreads();
+    // exclusive scan of the VT * NW counts, in (j, w) order == index order
+    const unsigned c = (tid < VT * NW) ? s_cnt[tid] : 0u;
+    unsigned total;
+    const unsigned ex = block_exclusive_sum<NT>(c, s_wtmp, &total);
+    if (tid < VT * NW) s_cnt[tid] = ex;
+    __syncthreads();
+    // staged in index order, then written by consecutive threads: a warp's
+    // stores are contiguous (full PCIe write packets for pinned host memory)
+#pragma unroll
+    for (int j = 0; j < VT; ++j) {
+      if (v[j] != 0.0f) {
+        const unsigned pos = s_cnt[j * NW + w] + __popc(mask[j] & lanemask_lt());
+        s_key[pos] = (int)(b + j * NT + tid);
+        s_val[pos] = v[j];
+      }
+    }
+    __syncthreads();
+    for (unsigned t = tid; t < total; t += NT) {
+      key[run + t] = s_key[t];
+      val[run + t] = s_val[t];
+    }
+    run += total;
+    __syncthreads();
+  }
+  if (blockIdx.x == gridDim.x - 1 && tid == 0) *d_count = (int)run;
 }
 
 int launch_scatter(int nvals, int len, const int* key, const float* val,
@@ -145,13 +211,20 @@ int launch_compact_nonzero(int len, const float* dense, int* key, float* val,
                            int* d_count, ScanScratch& ls, int* err,
                            cudaStream_t st) {
   constexpr int NT = 256, VT = 8;
+  (void)err;
   if (len <= 0) { cudaMemsetAsync(d_count, 0, sizeof(int), st); return 0; }
-  const int ntiles = (len + NT * VT - 1) / (NT * VT);
-  if (ntiles > ls.status_len) return -1;
-  LookbackState lbs{ls.status, ls.ticket};
-  note_launch();
-  compact_nonzero_kernel<NT, VT><<<ntiles, NT, 0, st>>>(len, dense, key, val, d_count,
-                                                       lbs, ntiles, err);
+  // ranges of whole sub-tiles, at most kCompactMaxRanges of them
+  const long long sub = NT * VT;
+  const long long subs = (len + sub - 1) / sub;
+  const long long per = sub * ((subs + kCompactMaxRanges - 1) / kCompactMaxRanges);
+  const long long ranges = (len + per - 1) / per;
+  if (ranges > ls.status_len || !ls.counts) return -1;
+  note_launch(2);
+  if (launch_pdl(compact_count_kernel<NT, VT>, dim3((unsigned)ranges), dim3(NT), 0, st, (long long)len, per,
+                 dense, ls.counts) != cudaSuccess ||
+      launch_pdl(compact_write_kernel<NT, VT>, dim3((unsigned)ranges), dim3(NT), 0, st, (long long)len, per,
+                 dense, (const unsigned*)ls.counts, key, val, d_count) != cudaSuccess)
+    return -2;
   return 0;
 }
 

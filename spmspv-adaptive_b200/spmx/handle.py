@@ -443,8 +443,7 @@ class SpmspvHandle:
 
     def set_naive_lanes(self, row_lanes=0, col_lanes=0):
         """Lanes per row / column of the naive kernels (0: from the mean
-        length; col_lanes = SPMX_COL_WARP_TILES (64) selects the warp-tile
-        CSC scatter)."""
+        length; else 1, 2, 4, 8, 16 or 32), as the autotuner sets them."""
         check(lib.spmx_set_naive_lanes(self._h, int(row_lanes), int(col_lanes)), "set_naive_lanes")
 
     def run_kernel(self, kid, alpha, y):
