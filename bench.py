@@ -1275,7 +1275,7 @@ def cpu_baseline(A, xs, binl):
 
 
 ONLY = ("powerlaw", "hybrid", "ingest", "batched-spmspv", "adjoint", "hola-spmv", "csr5-spmv", "naive-spmv", "tiled-spmv", "round-spmv", "hola-spmspv", "csc-lb-atomic",
-        "csc-naive-atomic", "csc-bucket", "csc-lb-sort", "bfs-rmat14", "bfs-batched")
+        "csc-naive-atomic", "csc-bucket", "csc-lb-sort", "bfs-rmat14", "bfs-batched", "compact", "compact-to-host")
 
 
 def run_only(args):
@@ -1335,7 +1335,24 @@ def run_only(args):
     y = torch.empty(A.m, device=dev)
     yk = torch.empty(A.m, dtype=torch.int32, device=dev)
     yv = torch.empty(A.m, device=dev)
+    if args.only.startswith("compact"):
+        # the compaction of y = A x at the chosen density: to device buffers,
+        # or straight into pinned host memory (the e2e path's read-back)
+        from spmx import abi
+        h.spmspv_csc(0, 0, 1.0, y, sync=False)
+        hk = torch.empty(A.m, dtype=torch.int32).pin_memory()
+        hv = torch.empty(A.m, dtype=torch.float32).pin_memory()
+        hc = torch.zeros(1, dtype=torch.int32).pin_memory()
+
+        def compact(to_host):
+            rc = (abi.lib.spmx_dense2sparse_to_host(h._h, A.m, y.data_ptr(), hk.data_ptr(), hv.data_ptr(),
+                                                     hc.data_ptr()) if to_host else
+                  abi.lib.spmx_dense2sparse_outer(h._h, A.m, y.data_ptr(), None, yk.data_ptr(), yv.data_ptr()))
+            if rc:
+                raise RuntimeError(f"compaction failed: {rc}")
     run = {
+        "compact": lambda: compact(False),
+        "compact-to-host": lambda: compact(True),
         "hola-spmv": lambda: h.holaspmv(1.0, y),
         "csr5-spmv": lambda: h.csr5spmv(1.0, y),
         "naive-spmv": lambda: h.naivespmv(1.0, y),
