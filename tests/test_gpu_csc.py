@@ -256,6 +256,36 @@ def test_vector_conversions(torch_cuda):
         h.dense2sparse_to_host(70000, dd_d, dk.cpu(), hv, hc)  # not pinned
 
 
+@pytest.mark.parametrize("length,frac", [(1, 1.0), (2047, 0.5), (2048, 0.0), (2049, 1.0), (2_097_152, 0.01),
+                                         (2_097_153, 0.3), (5_000_001, 0.05)])
+def test_compaction_lengths(torch_cuda, length, frac):
+    """Dense -> (key, value) of the nonzeros, to device buffers and straight
+    into pinned host memory, against numpy: ragged last ranges, no nonzeros,
+    every element nonzero, and vectors longer than 1,024 ranges of 2,048
+    elements (each CTA then compacts several sub-tiles in turn)."""
+    torch = torch_cuda
+    h = make_handle(rand_csr(64, 64, density=0.1, seed=3), torch, hola=False)
+    rng = np.random.default_rng(length)
+    d = rng.uniform(-1, 1, length).astype(np.float32)
+    d[rng.random(length) >= frac] = 0
+    ek, ev = orc.dense2sparse(d)
+    dd = dev(d, torch)
+    dk = torch.full((length,), -1, dtype=torch.int32, device="cuda")
+    dv = torch.zeros(length, device="cuda")
+    cnt = h.dense2sparse_outer(length, dd, dk, dv)
+    assert cnt == len(ek)
+    assert np.array_equal(dk[:cnt].cpu().numpy(), ek) and np.array_equal(dv[:cnt].cpu().numpy(), ev)
+    hk = torch.full((length,), -1, dtype=torch.int32).pin_memory()
+    hv = torch.zeros(length).pin_memory()
+    hc = torch.full((1,), -1, dtype=torch.int32).pin_memory()
+    h.dense2sparse_to_host(length, dd, hk, hv, hc)
+    torch.cuda.synchronize()
+    c = int(hc[0])
+    assert c == len(ek)
+    assert np.array_equal(hk[:c].numpy(), ek) and np.array_equal(hv[:c].numpy(), ev)
+    h.check_device_error()
+
+
 def test_features(torch_cuda):
     torch = torch_cuda
     from spmx import gen
