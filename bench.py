@@ -441,6 +441,24 @@ def run_ours(args, world, rank, local):
         if it >= 3:
             per_call += np.array([a.elapsed_time(b) for a, b in ev1])
     per_call /= args.steps
+    # --- each call's share of the chained step: the step cut after call k
+    # (the same flush, events and calls as a step), minus the step cut after
+    # call k - 1; the first share includes the cost of the step's first launch
+    # after the flush ---
+    prefix = np.zeros(len(dx))
+    for it in range(3 + args.steps):
+        for kk in range(1, len(dx) + 1):
+            flush.fill_(1.0)
+            s_ev.record(stream)
+            for i in range(kk):
+                h.set_sparse_x(dx[i][1], dx[i][2], dx[i][3])
+                h.run_adaptive(1.0, ys[i])
+            e_ev.record(stream)
+            stream.synchronize()
+            if it >= 3:
+                prefix[kk - 1] += s_ev.elapsed_time(e_ev)
+    prefix /= args.steps
+    in_step = np.diff(np.concatenate([[0.0], prefix]))
     # the same timing around a kernel that writes one float: what an event
     # pair around any single launch costs after the flush
     tiny = torch.zeros(1, device=dev)
@@ -679,8 +697,9 @@ def run_ours(args, world, rank, local):
     if rank == 0:
         cpu = cpu_baseline(A, xs, binl) if not args.no_cpu and world == 1 else None
         sweep = [{"density": dd, "x_nnz": k, "bin_len": b, "kernel": abi.KERNEL_NAMES[c],
-                  "ms_alone_flushed": float(t1), "eff_gbs_alone_flushed": eb / (t1 * 1e-3) / 1e9}
-                 for (dd, _, _, k), b, c, t1, eb in zip(dx, binl, chosen, per_call, ebytes)]
+                  "ms_alone_flushed": float(t1), "eff_gbs_alone_flushed": eb / (t1 * 1e-3) / 1e9,
+                  "ms_in_step": float(t2)}
+                 for (dd, _, _, k), b, c, t1, eb, t2 in zip(dx, binl, chosen, per_call, ebytes, in_step)]
         line = {
             "metric": METRIC, "value": value, "unit": "GB/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": step_ms_max,
