@@ -286,6 +286,45 @@ def test_compaction_lengths(torch_cuda, length, frac):
     h.check_device_error()
 
 
+def test_compaction_on_read_back_stream(torch_cuda):
+    """The e2e pattern: SpMSpV calls on one stream, each result compacted into
+    pinned host memory on a second stream (the handle switched to it for that
+    call) while the next calls run; every host result against the oracle."""
+    torch = torch_cuda
+    from spmx import gen
+    A = gen.zipf_rows(200_000, 1.5, 16, 2000, seed=4)
+    h = make_handle(A, torch, hola=False)
+    s1, s2 = torch.cuda.Stream(), torch.cuda.Stream()
+    h.set_stream(s1)
+    colptr, row, cval = A.to_csc()
+    xs = [_x(A.n, k, 20 + k) for k in (3, 200, 5_000, 60_000)]
+    keys = [dev(k, torch) for k, _ in xs]
+    vals = [dev(v, torch) for _, v in xs]
+    ys = [torch.empty(A.m, device="cuda") for _ in xs]
+    hk = [torch.empty(A.m, dtype=torch.int32).pin_memory() for _ in xs]
+    hv = [torch.empty(A.m).pin_memory() for _ in xs]
+    hc = torch.full((len(xs),), -1, dtype=torch.int32).pin_memory()
+    evs = [torch.cuda.Event() for _ in xs]
+    for rep in range(2):
+        for i in range(len(xs)):
+            h.set_sparse_x(keys[i], vals[i], len(xs[i][0]))
+            h.spmspv_csc(0, 0, 1.0, ys[i], sync=False)
+            evs[i].record(s1)
+            s2.wait_event(evs[i])
+            h.set_stream(s2)
+            h.dense2sparse_to_host(A.m, ys[i], hk[i], hv[i], hc[i:i + 1])
+            h.set_stream(s1)
+        torch.cuda.synchronize()
+        h.check_device_error()
+        for i, (key, val) in enumerate(xs):
+            y64, mag, _ = orc.spmspv_csc_f64(A.m, colptr, row, cval, key, val)
+            got = np.zeros(A.m)
+            c = int(hc[i])
+            got[hk[i][:c].numpy()] = hv[i][:c].numpy()
+            ok, _ = orc.within_tol(got, y64, mag, RTOL)
+            assert ok, (rep, i)
+
+
 def test_features(torch_cuda):
     torch = torch_cuda
     from spmx import gen
