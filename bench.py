@@ -1366,6 +1366,8 @@ def run_only(args):
     h.tiledPreprocess()
     h.roundPreprocess(0, args.round_parts)
     h.allocPreBuffer()
+    if args.col_lanes:
+        h.set_naive_lanes(0, args.col_lanes)
     dens = 1.0 if args.only.endswith("spmv") else args.density
     k = [x for x in xs if abs(x[0] - dens) < 1e-12][0]
     kd, vd = d(k[1]), d(k[2])
@@ -1440,6 +1442,8 @@ def main():
                          "whose serialised timings would mislead the tuner) reuses the first run's choices")
     ap.add_argument("--only", choices=ONLY, help="run one kernel (profiling helper)")
     ap.add_argument("--density", type=float, default=0.1)
+    ap.add_argument("--col-lanes", type=int, default=0,
+                    help="with --only: lanes per x entry of the naive CSC scatter (0: from the mean column length)")
     ap.add_argument("--round-parts", type=int, default=1, choices=[1, 2, 4],
                     help="--only round-spmv: CTAs per row block of the round format")
     ap.add_argument("--batched-log2n", type=int, default=22,
