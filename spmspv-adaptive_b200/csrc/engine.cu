@@ -9,6 +9,7 @@
 #include <cmath>
 #include <cstring>
 #include <string>
+#include <vector>
 
 #include "common.cuh"
 #include "engine.h"
@@ -41,6 +42,26 @@ int dalloc(void** p, size_t bytes, const char* what) {
 
 void dfree(void* p) {
   if (p) cudaFree(p);
+}
+
+cudaError_t kernel_smem_limit(const void* kernel, size_t bytes) {
+  static std::mutex mu;
+  static std::vector<std::pair<std::pair<const void*, int>, size_t>> set;  // (kernel, device) -> bytes
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  std::lock_guard<std::mutex> lock(mu);
+  for (auto& s : set) {
+    if (s.first.first == kernel && s.first.second == dev) {
+      if (s.second == bytes) return cudaSuccess;
+      e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+      if (e == cudaSuccess) s.second = bytes;
+      return e;
+    }
+  }
+  e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  if (e == cudaSuccess) set.push_back({{kernel, dev}, bytes});
+  return e;
 }
 
 static std::atomic<unsigned long long> g_launches{0};

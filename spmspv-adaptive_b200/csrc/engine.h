@@ -169,6 +169,10 @@ namespace spmx {
 int set_error(int code, const std::string& msg);
 int dalloc(void** p, size_t bytes, const char* what);
 void dfree(void* p);
+// A kernel's dynamic shared-memory limit is a property of the function on a
+// device, shared by every handle: set it to `bytes` unless it already is
+// (cached per function and device), right before a launch that needs it.
+cudaError_t kernel_smem_limit(const void* kernel, size_t bytes);
 }  // namespace spmx
 
 // Status plumbing shared by the entry points: return the first failure.

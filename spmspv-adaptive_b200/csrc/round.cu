@@ -585,7 +585,7 @@ int bits_for(long long v) {  // bits to hold values in [0, v)
 
 template <bool GATED, bool INPLACE>
 static void round_set_smem(size_t smem) {
-  cudaFuncSetAttribute(round_spmv_kernel<GATED, INPLACE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  kernel_smem_limit((const void*)round_spmv_kernel<GATED, INPLACE>, smem);
 }
 
 static long long round_static_smem() {
@@ -1060,6 +1060,9 @@ static cudaError_t round_launch(spmx_handle_t h, RoundTables* t, float alpha, fl
   at[1].val.programmaticStreamSerializationAllowed = 1;
   cfg.attrs = at;
   cfg.numAttrs = 2;
+  // another handle's build may have set this kernel's limit for its own size
+  const cudaError_t e = kernel_smem_limit((const void*)round_spmv_kernel<GATED, INPLACE>, t->smem);
+  if (e != cudaSuccess) return e;
   return cudaLaunchKernelEx(&cfg, round_spmv_kernel<GATED, INPLACE>, t->geom, t->nslots, t->parts,
                             (const int*)t->rb_row, (const int*)t->cta_round, (const uint4*)t->packed,
                             (const float4*)t->val, (const int*)t->cbase, (const int*)t->vbg,

@@ -532,8 +532,8 @@ extern "C" int spmx_tiled_postprocess(spmx_handle_t h) {
 
 template <int NW>
 static void tiled_set_smem(size_t smem) {
-  cudaFuncSetAttribute(tiled_spmv_kernel<NW, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  cudaFuncSetAttribute(tiled_spmv_kernel<NW, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  kernel_smem_limit((const void*)tiled_spmv_kernel<NW, false>, smem);
+  kernel_smem_limit((const void*)tiled_spmv_kernel<NW, true>, smem);
 }
 
 // clusters of `cs` CTAs that can be resident at once (0 if unknown)
@@ -850,6 +850,9 @@ static cudaError_t tiled_launch(spmx_handle_t h, TiledTables* t, float alpha, fl
   at[1].val.programmaticStreamSerializationAllowed = 1;
   cfg.attrs = at;
   cfg.numAttrs = 2;
+  // another handle's build may have set this kernel's limit for its own size
+  const cudaError_t e = kernel_smem_limit((const void*)tiled_spmv_kernel<NW, GATED>, t->smem);
+  if (e != cudaSuccess) return e;
   return cudaLaunchKernelEx(&cfg, tiled_spmv_kernel<NW, GATED>, h->n, t->g, t->cs, (const int*)t->rb_row,
                             (const int*)t->cta_stage, (const TileStage*)t->stages, (const int*)t->offsets,
                             (const unsigned*)t->packed, (const float*)t->val, (const float*)h->x_dense, bits,

@@ -170,3 +170,30 @@ def test_round_refusals_keep_handle_usable(torch_cuda):
     ok = bad < A.n
     y64, mag = orc.spmv_f64(A.rowptr, np.where(ok, bad, 0), np.where(ok, A.val, 0), x)
     assert orc.within_tol(y.cpu().numpy(), y64, mag, RTOL)[0]
+
+
+def test_two_handles_with_different_shared_memory(torch_cuda):
+    """A kernel's dynamic shared-memory limit belongs to the function, not to
+    a handle: a handle whose format needs more shared memory than the format
+    built last (by another handle) still launches, for the round and the tiled
+    back-ends, and both results match the FP64 oracle."""
+    torch = torch_cuda
+    big = dict(EXTRA)["hubs"]
+    small = rand_csr(2000, 1500, density=0.004, seed=61)
+    hb, hs = make_handle(big, torch, hola=False), make_handle(small, torch, hola=False)
+    hb.roundPreprocess(0, 1)
+    hs.roundPreprocess(0, 1)
+    assert hb.round_info()["smem"] > hs.round_info()["smem"]
+    hb.tiledPreprocess()
+    hs.tiledPreprocess(rb_rows=256)
+    assert hb.tiled_info()["smem"] > hs.tiled_info()["smem"]
+    for h, A in ((hb, big), (hs, small), (hb, big)):
+        x = np.random.default_rng(A.m).uniform(-1, 1, A.n).astype(np.float32)
+        h.set_x(dev(x, torch))
+        y64, mag = orc.spmv_f64(A.rowptr, A.col, A.val, x)
+        for run in (h.roundspmv, h.tiledspmv):
+            y = torch.full((A.m,), 3.0, device="cuda")
+            run(1.0, y)
+            h.check_device_error()
+            ok, _ = orc.within_tol(y.cpu().numpy(), y64, mag, RTOL)
+            assert ok, run.__name__
