@@ -290,10 +290,9 @@ __device__ __forceinline__ void lb_published(const LookbackState& st, int ntiles
 // Each step reads a window of kLbWindow * 32 predecessors at once (lane l,
 // slot q: tile j - 32q - l): when every tile of a launch is in flight, few of
 // them have published an inclusive prefix yet, and a look-back that moved 32
-// tiles per memory round trip took ~16 round trips at 512 tiles (11 us for
-// a 1M-element compaction); with 256 per step it takes at most 2.  A window
-// is accepted once every tile nearer than its nearest inclusive prefix has
-// published its aggregate.
+// tiles per memory round trip needed up to 16 round trips at 512 tiles; with
+// 256 per step it needs at most 2.  A window is accepted once every tile
+// nearer than its nearest inclusive prefix has published its aggregate.
 constexpr int kLbWindow = 8;
 __device__ __forceinline__ unsigned lb_warp_lookback(const LookbackState& st,
                                                      int tile, int ntiles,
