@@ -64,6 +64,19 @@ def spmv_bytes(m, n, nnz):
     return 4 * (m + 1) + 8 * nnz + 4 * n + 4 * m
 
 
+def ref_spmv_bytes(m, nnz):
+    """The reference's own SpMV byte count, SpmvGetBytes (detail/util.h:145):
+    row pointers and column indices, then values, x read once per nonzero,
+    and y."""
+    return (m + 1 + nnz) * 4 + (2 * nnz + m) * 4
+
+
+def ref_gm1_bytes(x_nnz, bin_len):
+    """The reference's traffic model of the CSC SpMSpV, GM1 (csc-spmspv/spmspv.h:2727-2733):
+    12 bytes per x entry and 12 per product."""
+    return 12 * x_nnz + 12 * bin_len
+
+
 class Clocks:
     """nvidia-smi sampling during the timed region."""
 
@@ -717,7 +730,8 @@ def run_ours(args, world, rank, local):
         cpu = cpu_baseline(A, xs, binl) if not args.no_cpu and world == 1 else None
         sweep = [{"density": dd, "x_nnz": k, "bin_len": b, "kernel": abi.KERNEL_NAMES[c],
                   "ms_alone_flushed": float(t1), "eff_gbs_alone_flushed": eb / (t1 * 1e-3) / 1e9,
-                  "ms_in_step": float(t2)}
+                  "ms_in_step": float(t2), "bytes_compulsory": int(eb),
+                  "bytes_reference_gm1": int(ref_gm1_bytes(k, b))}
                  for (dd, _, _, k), b, c, t1, eb, t2 in zip(dx, binl, chosen, per_call, ebytes, in_step)]
         line = {
             "metric": METRIC, "value": value, "unit": "GB/s", "n_gpus": world,
@@ -738,6 +752,8 @@ def run_ours(args, world, rank, local):
                          "achieved": achieved, "peak": peak, "peak_kind": peak_kind,
                          "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
                          "bytes_per_launch": sb, "ms_per_launch": k_ms,
+                         "reference_bytes_per_launch": ref_spmv_bytes(m, nnz),
+                         "achieved_reference_bytes_gbs": ref_spmv_bytes(m, nnz) / (k_ms * 1e-3) / 1e9,
                          "ms_per_launch_median": statistics.median(kt), "ms_per_launch_min": min(kt)},
             "e2e": {"value": e2e_val, "unit": "GB/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms,
