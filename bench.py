@@ -815,7 +815,8 @@ def run_bfs_plain(torch, dev, stream, args):
     h.Destroy()
     return {"graph": "rmat scale 14, edge factor 16, seed 1, source 0",
             "ms": ms, "gteps": edges / (ms * 1e-3) / 1e9, "depth": depth,
-            "bit_exact": bool(np.array_equal(got, ref)), "edges": edges}
+            "bit_exact": bool(np.array_equal(got, ref)), "edges": edges,
+            "gteps_edges": "undirected input edges inside the source's component (Graph500)"}
 
 
 def run_bfs_batched(torch, dev, stream, args):
@@ -870,6 +871,7 @@ def run_bfs_batched(torch, dev, stream, args):
     h.Destroy()
     return {"graph": "rmat scale 22, edge factor 16, seed 3, 64 sources (seed 3)",
             "batched_ms": mb, "plain64_ms": mp, "edges": edges,
+            "gteps_edges": "undirected input edges inside each source's component, summed over the 64 (Graph500)",
             "batched_gteps": edges / (mb * 1e-3) / 1e9, "plain64_gteps": edges / (mp * 1e-3) / 1e9,
             "speedup": mp / mb, "bit_exact_vs_plain": exact,
             "bit_exact_vs_oracle": {"sources": [int(srcs[i]) for i in sampled], "ok": bool(oracle_ok)}}
