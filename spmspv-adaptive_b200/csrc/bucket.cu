@@ -21,6 +21,7 @@
 #include "sort.h"
 #include <algorithm>
 #include "common.cuh"
+#include "engine.h"
 #include "csc_lb.cuh"
 
 namespace spmx {
@@ -173,7 +174,7 @@ int bucket_geometry(int m, int buckets, int* rshift, int* nb) {
 
 template <class K>
 static void allow_smem(K kernel, int bytes) {
-  cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  kernel_smem_limit((const void*)kernel, (size_t)bytes);
 }
 
 int launch_bucket_spmspv(const CscArgs& a, const CscScratch& s, const BucketScratch& bs,
@@ -182,13 +183,11 @@ int launch_bucket_spmspv(const CscArgs& a, const CscScratch& s, const BucketScra
                          cudaStream_t st) {
   constexpr int NT = kCscLbNT, VT = kCscLbVT;
   const int hist_bytes = 4 * nb;
-  static bool attrs = false;
-  if (!attrs) {
-    allow_smem(bucket_count_kernel<NT, VT>, 4 * kBucketMax);
-    allow_smem(bucket_scatter_kernel<NT, VT>, 4 * kBucketMax);
-    allow_smem(bucket_reduce_kernel<256>, 4 * (8192 + 8192 / 32));
-    attrs = true;
-  }
+  // the limits are per function and device: cached per device, set on each
+  // device the first time it runs these kernels
+  allow_smem(bucket_count_kernel<NT, VT>, 4 * kBucketMax);
+  allow_smem(bucket_scatter_kernel<NT, VT>, 4 * kBucketMax);
+  allow_smem(bucket_reduce_kernel<256>, 4 * (8192 + 8192 / 32));
   cudaMemsetAsync(bs.gcount, 0, sizeof(int) * (size_t)nb, st);
   note_launch();
   bucket_count_kernel<NT, VT><<<grid, NT, hist_bytes, st>>>(a, s, variant, rshift, nb, bs.gcount);
